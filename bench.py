@@ -1,0 +1,443 @@
+#!/usr/bin/env python
+"""NCS throughput benchmark on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): ``stack512`` -- 200 frames of 512 x 512 float32 photo-
+electrons (worm-like-chain structure, sCMOS camera model, seeded synthetic),
+one shared gamma map, OTF-weighted 16x16 mask, alpha 0.2, L-BFGS capped at 20
+iterations, all 273,800 tiles in one persistent launch.  A step is one solve
+of the whole stack.  Inputs and outputs (210 MB each) exceed the 126 MB L2, so
+no flush is needed between steps.
+
+Prints one JSON line.  ``value`` is Mpixel/s of the whole job (all ranks) with
+the stack resident in HBM, timed with CUDA events; ``e2e`` is the same metric
+through the public ``Solver`` API from pinned host memory (H2D copy, solve,
+D2H copy every step).  Under torchrun each rank solves its own stack
+(replicas by frame, weak scaling, no collective in the data path); the time
+is the max over ranks.  ``--impl reference`` times the reference's own CPU
+path (pyCNCS ncs.c compiled by oracle/Makefile, else the oracle's C port) on
+all host cores instead.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic FP32 work of the plain solver per tile ("Roofline"):
+#   Q application by 16x16 real FFTs (forward + inverse, 2 x 2.5 N log2 N with
+#   N = 256) and the spectrum weighting                       11,264
+#   initial gradient (256 x 9) + norms                          3,328
+#   per iteration: Q application 11,264, directional dots 1,536, accepted
+#   point + gradient 2,304, norms / curvature dots 2,048, two-loop with m
+#   pairs 4 * 256 * 2 * m (16,384 at m = 8)                    33,536
+#   per line-search trial: 256 x (log1p, divide, 6 flops)        2,048
+FLOP_INIT = 11264 + 3328
+FLOP_ITER_BASE = 11264 + 1536 + 2304 + 2048
+FLOP_TWO_LOOP_PER_PAIR = 4 * 256 * 2
+FLOP_TRIAL = 2048
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def fp32_peak_tflops(sm_mhz, n_sms):
+    return n_sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ----------------------------------------------------------- CPU reference --
+
+class _quiet_stdout:
+    """The reference C prints one line per tile whose solver returns non-zero
+    (ncs.c:116-119), which a capped run does for most tiles; keep it off the
+    JSON stdout."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *a):
+        try:
+            ctypes.CDLL(None).fflush(None)
+        except Exception:
+            pass
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def cpu_reduce_frames(frames, gamma, mask_shifted, alpha, max_iters, threads):
+    """pyCNCS cReduceNoise on each frame, frames spread over `threads` host
+    threads (ctypes releases the GIL).  Returns (wall seconds, kind)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import pycncs
+    pycncs.set_overrides(max_iterations=max_iters)
+    kind = pycncs.kind()
+    g64 = numpy.ascontiguousarray(gamma, dtype=numpy.float64)
+    m64 = numpy.ascontiguousarray(mask_shifted, dtype=numpy.float64)
+    try:
+        with _quiet_stdout():
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(max_workers=threads) as ex:
+                list(ex.map(lambda fr: pycncs.cReduceNoise(fr, g64, m64, alpha), frames))
+            wall = time.perf_counter() - t0
+    finally:
+        pycncs.set_overrides()
+    return wall, kind
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_sample_frames(images_cpu, threads, budget_s=20.0):
+    """Frames for a bounded CPU sample: one per thread, at most enough for
+    ~budget_s of CPU work and never more than the stack."""
+    return min(images_cpu.shape[0], max(1, threads))
+
+
+def accuracy_gate(w, tile_cost, n_sample, seed=0):
+    """Per-tile final cost vs the FP64 Newton optimum (oracle) on a random
+    sample of tiles: fraction within 1e-4 relative, max and median gap."""
+    from oracle import numpy_ref as nr
+    images = w["images"]
+    T, H, W = images.shape
+    ox, oy = nr.tile_origins(H), nr.tile_origins(W)
+    per = len(ox) * len(oy)
+    rng = numpy.random.default_rng(seed)
+    idx = numpy.sort(rng.choice(T * per, size=min(n_sample, T * per), replace=False))
+    gam = numpy.pad(w["gamma"].cpu().numpy().astype(numpy.float64), 1, "edge")
+    data, gms = [], []
+    cache = {}
+    for t in idx:
+        f, rem = divmod(int(t), per)
+        i, j = divmod(rem, len(oy))
+        if f not in cache:
+            cache = {f: numpy.pad(images[f].cpu().numpy().astype(numpy.float64), 1, "edge")}
+        p = cache[f]
+        data.append(p[ox[i]:ox[i] + 16, oy[j]:oy[j] + 16])
+        gms.append(gam[ox[i]:ox[i] + 16, oy[j]:oy[j] + 16])
+    ms = numpy.fft.fftshift(w["mask"]).astype(numpy.float32).astype(numpy.float64)
+    _, fstar, _ = nr.newton_solve(numpy.array(data), numpy.array(gms), ms, w["alpha"])
+    gap = nr.rel_cost_gap(tile_cost[idx], fstar)
+    return {"tiles_checked": int(idx.size), "frac_within_1e-4": float((gap <= 1e-4).mean()),
+            "max_rel_gap": float(gap.max()), "median_rel_gap": float(numpy.median(gap)),
+            "referee": "FP64 damped Newton (oracle/numpy_ref.py)"}
+
+
+# --------------------------------------------------------------- arms -------
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    from ncs_b200 import sim
+    w = sim.make_stack(args.workload, T=args.frames, device="cpu", seed=1234)
+    imgs = w["images"].numpy()
+    threads = cpu_threads()
+    n = cpu_sample_frames(imgs, threads)
+    frames = [imgs[i].astype(numpy.float64) for i in range(n)]
+    ms = numpy.fft.fftshift(w["mask"])
+    for _ in range(args.warmup):
+        cpu_reduce_frames(frames, w["gamma"].numpy(), ms, w["alpha"], w["max_iters"], threads)
+    walls = []
+    kind = None
+    for _ in range(args.steps):
+        wall, kind = cpu_reduce_frames(frames, w["gamma"].numpy(), ms, w["alpha"],
+                                       w["max_iters"], threads)
+        walls.append(wall)
+    H, W = imgs.shape[1:]
+    value = n * H * W / (sum(walls) / len(walls)) / 1e6
+    sample = ("%d of %d frames (%dx%d) per step, one frame per thread, pyCNCS cReduceNoise "
+              "FP64 with libLBFGS-API max_iterations=%d" % (n, imgs.shape[0], H, W,
+                                                            w["max_iters"]))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpixel/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(walls) / len(walls), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(w, args),
+        "cpu_baseline": {"value": value, "unit": "Mpixel/s", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "Mpixel/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+METRIC = "Mpixel/s at <=1e-4 rel cost vs FP64: warm-start+TC vs plain GPU (pyCNCS ref)"
+
+
+def workload_config(w, args):
+    T, H, W = w["images"].shape
+    return {"workload": "%s: %d frames x %dx%d float32, %d WLC chains, alpha %.2f, 16x16 tiles, "
+                        "L-BFGS cap %d" % (w["name"], T, H, W, w["cfg"]["chains"], w["alpha"],
+                                           w["max_iters"]),
+            "frames": T, "height": H, "width": W, "alpha": w["alpha"],
+            "max_iters": w["max_iters"], "seed": w["seed"], "form": args.form,
+            "l2": "inputs+outputs %.0f MB > 126 MB L2, no flush" % (2 * T * H * W * 4 / 1e6),
+            "parallelism": "replicas by frame (one stack per rank)"}
+
+
+def run_ours(args, world, rank, local):
+    import ncs_b200
+    from ncs_b200 import sim
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = sim.make_stack(args.workload, T=args.frames, device=dev, seed=1234 + rank)
+    images, gamma = w["images"], w["gamma"]
+    T, H, W = images.shape
+    solver = ncs_b200.Solver(alpha=w["alpha"], max_iters=w["max_iters"], mode=args.form)
+    solver.set_otf_mask(w["mask"])
+    out = torch.empty_like(images)
+    stream = torch.cuda.current_stream(dev)
+
+    # untimed statistics run: per-tile iterations / evaluations / final cost
+    _, iters, status, cost, evals = solver.reduce_noise(images, gamma, out=out, tile_stats="all")
+    torch.cuda.synchronize()
+    iters_n = iters.double().sum().item()
+    evals_n = evals.double().sum().item()
+    n_tiles = iters.numel()
+    m = solver.params.m
+    pairs = torch.clamp(iters.double() - 1.0, min=0.0)
+    two_loop = torch.minimum(pairs, torch.full_like(pairs, float(m)))
+    flops = (n_tiles * FLOP_INIT + iters_n * FLOP_ITER_BASE
+             + FLOP_TWO_LOOP_PER_PAIR * two_loop.sum().item()
+             + FLOP_TRIAL * (evals_n - n_tiles))
+    st = status.cpu().numpy()
+
+    for _ in range(args.warmup):
+        solver.reduce_noise(images, gamma, out=out)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for k in range(args.steps):
+        solver.reduce_noise(images, gamma, out=out)
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    total_ms = max_over_ranks(total_ms, world)
+    px = sum_over_ranks(float(T * H * W), world)
+    value = px * args.steps / (total_ms / 1e3) / 1e6
+
+    # end to end through the public API from pinned host memory
+    h_in = images.cpu().pin_memory()
+    h_gamma = gamma.cpu().pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        d_in = h_in.to(dev, non_blocking=True)
+        d_g = h_gamma.to(dev, non_blocking=True)
+        res = solver.reduce_noise(d_in, d_g)
+        h_out.copy_(res, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    e2e_value = px * e2e_steps / (e2e_ms / 1e3) / 1e6
+    assert torch.equal(h_out, out.cpu()), "e2e result differs from the device-resident run"
+
+    pk, pk_src = peaks()
+    n_sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak = fp32_peak_tflops(pk.get("sm_max_mhz", 1965.0), n_sms)
+    launch_ms = statistics.mean(per_step)
+    achieved = flops / (launch_ms / 1e3) / 1e12
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        key = "%s/%s" % (args.workload, args.form)
+        if key in tj:
+            traffic = tj[key]["bytes_per_launch"]
+    alg_bytes = 8.0 * T * H * W + 4.0 * H * W
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded WLC structure + sCMOS camera model)",
+        "config": workload_config(w, args),
+        "frames_per_s": world * T * args.steps / (total_ms / 1e3),
+        "tiles": n_tiles, "mean_iters": iters_n / n_tiles, "mean_evals": evals_n / n_tiles,
+        "status": {str(k): int((st == k).sum()) for k in range(-5, 1) if (st == k).any()},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
+                     "kernel": "ncs_plain_kernel",
+                     "peak_source": "148 SMs x 128 FP32 lanes x 2 x %s sm_max_mhz (%s)"
+                                    % (pk.get("sm_max_mhz"), pk_src),
+                     "flops_per_launch": flops,
+                     "hbm": {"algorithmic_bytes": alg_bytes,
+                             "achieved_gbs": alg_bytes / (launch_ms / 1e3) / 1e9,
+                             "peak_gbs": pk.get("hbm_gbs")}},
+        "e2e": {"value": e2e_value, "unit": "Mpixel/s",
+                "h2d_bytes_per_step": int(h_in.numel() * 4 + h_gamma.numel() * 4),
+                "d2h_bytes_per_step": int(h_out.numel() * 4),
+                "api": "ncs_b200.Solver.reduce_noise, pinned host buffers"},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = cpu_threads()
+        imgs = images.cpu().numpy()
+        n = cpu_sample_frames(imgs, threads)
+        frames = [imgs[i].astype(numpy.float64) for i in range(n)]
+        wall, kind = cpu_reduce_frames(frames, gamma.cpu().numpy(), numpy.fft.fftshift(w["mask"]),
+                                       w["alpha"], w["max_iters"], threads)
+        line["cpu_baseline"] = {
+            "value": n * H * W / wall / 1e6, "unit": "Mpixel/s", "cores": threads, "kind": kind,
+            "sample": "%d of %d frames, one per thread, pyCNCS cReduceNoise FP64, "
+                      "max_iterations=%d" % (n, T, w["max_iters"])}
+        line["accuracy"] = accuracy_gate(w, cost.cpu().numpy(), args.accuracy_tiles)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="stack512")
+    ap.add_argument("--frames", type=int, default=None, help="override the frame count")
+    ap.add_argument("--form", default="plain")
+    ap.add_argument("--accuracy-tiles", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # rank 0 alone times the CPU path; no process group is needed
+        return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")),
+                             int(os.environ.get("RANK", "0")))
+    world, rank, local = dist_setup()
+    try:
+        return run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

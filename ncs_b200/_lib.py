@@ -1,0 +1,103 @@
+"""ctypes binding of libncs_b200.so (C ABI in include/ncs_b200.h).
+
+The library is the only compute path: if it is missing or fails to load the
+import raises -- there is no CPU fallback.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libncs_b200.so")
+
+NCSB_OK = 0
+NCSB_EINVAL = -1
+NCSB_ECUDA = -2
+NCSB_ENOMASK = -3
+NCSB_ESIZE = -4
+
+MODE_PLAIN = 0
+
+# Per-tile status codes (cuda/ncs.cu:61-67).
+SUCCESS = 0
+UNSTARTED = -1
+REACHED_MAXITERS = -2
+INCREASING_GRADIENT = -3
+MINIMUM_STEP = -4
+REACHED_MAXPRECISION = -5
+STATUS_NAMES = {
+    UNSTARTED: "Unstarted",
+    REACHED_MAXITERS: "Reached maximum iterations",
+    INCREASING_GRADIENT: "Increasing gradient",
+    MINIMUM_STEP: "Reached minimum step size",
+    REACHED_MAXPRECISION: "Reached machine precision",
+}
+
+
+class NcsbParams(ctypes.Structure):
+    _fields_ = [
+        ("alpha", ctypes.c_double),
+        ("max_iters", ctypes.c_int32),
+        ("m", ctypes.c_int32),
+        ("epsilon", ctypes.c_double),
+        ("c1", ctypes.c_double),
+        ("min_step", ctypes.c_double),
+        ("mode", ctypes.c_int32),
+        ("ctas_per_sm", ctypes.c_int32),
+    ]
+
+
+# Every symbol include/ncs_b200.h declares (checked by the tests).
+EXPORTS = [
+    "ncsb_default_params", "ncsb_create", "ncsb_set_params", "ncsb_destroy", "ncsb_last_error",
+    "ncsb_set_otf_mask", "ncsb_num_tiles", "ncsb_reduce_noise", "ncsb_solve_tiles",
+]
+
+_lib = None
+
+
+def load():
+    """Load and type the library (raises OSError if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError("libncs_b200.so is not built; run `python -m ncs_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    P = ctypes.POINTER
+    lib.ncsb_default_params.argtypes = [P(NcsbParams)]
+    lib.ncsb_default_params.restype = None
+    lib.ncsb_create.argtypes = [P(vp), P(NcsbParams)]
+    lib.ncsb_create.restype = ctypes.c_int
+    lib.ncsb_set_params.argtypes = [vp, P(NcsbParams)]
+    lib.ncsb_set_params.restype = ctypes.c_int
+    lib.ncsb_destroy.argtypes = [vp]
+    lib.ncsb_destroy.restype = ctypes.c_int
+    lib.ncsb_last_error.argtypes = [vp]
+    lib.ncsb_last_error.restype = ctypes.c_char_p
+    lib.ncsb_set_otf_mask.argtypes = [vp, P(ctypes.c_float)]
+    lib.ncsb_set_otf_mask.restype = ctypes.c_int
+    lib.ncsb_num_tiles.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P(i64)]
+    lib.ncsb_num_tiles.restype = ctypes.c_int
+    lib.ncsb_reduce_noise.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
+                                      ctypes.c_int, vp, vp, vp, vp, vp, vp]
+    lib.ncsb_reduce_noise.restype = ctypes.c_int
+    lib.ncsb_solve_tiles.argtypes = [vp, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]
+    lib.ncsb_solve_tiles.restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def default_params():
+    p = NcsbParams()
+    load().ncsb_default_params(ctypes.byref(p))
+    return p
+
+
+def num_tiles(n_frames, height, width):
+    n = ctypes.c_int64(0)
+    rc = load().ncsb_num_tiles(int(n_frames), int(height), int(width), ctypes.byref(n))
+    if rc != NCSB_OK:
+        raise ValueError("frames of %dx%d cannot be tiled (need >= 14 on each axis)"
+                         % (height, width))
+    return n.value

@@ -1,0 +1,155 @@
+// ncs_internal.cuh -- device-side building blocks shared by the NCS kernels.
+//
+// Tile geometry (fixed by the reference GPU path, cuda/ncs.cu:41-51): 16x16
+// tiles, 256 unknowns each.  A warp group (128 threads) owns one tile; thread
+// t holds the two pixels (r, c) and (r + 8, c) with r = t >> 4, c = t & 15.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ncsb {
+
+constexpr int kTile = 16;
+constexpr int kPix = 256;
+constexpr int kThreads = 128;  // one warp group per tile
+constexpr int kMaxM = 8;       // L-BFGS history capacity
+constexpr float kFitMin = 1.0e-6f;  // FITMIN, ncs.c:169 / ncs.cu:40
+
+// Per-tile solver status, identical values to cuda/ncs.cu:61-67.
+enum Status : int32_t {
+    kSuccess = 0,
+    kUnstarted = -1,
+    kReachedMaxIters = -2,
+    kIncreasingGradient = -3,
+    kMinimumStep = -4,
+    kReachedMaxPrecision = -5,
+};
+
+// Launch description shared by every solver form.
+struct SolveArgs {
+    int tile_mode;                 // 0: stack in / stack out, 1: tiles in / tiles out
+    const float* data;             // stack [T][H][W] or tiles [N][256]
+    const float* gamma;            // [H][W], [T][H][W] or tiles [N][256]
+    const float* u0;               // optional start, tile mode only [N][256]
+    long long gamma_frame_stride;  // stack mode: 0 (shared map) or H*W
+    float* out;                    // stack [T][H][W] or tiles [N][256]
+    int T, H, W;
+    int tiles_x, tiles_y;          // tiles along H (slow) and W (fast)
+    long long n_tiles;
+    int32_t* iters;                // optional [N]
+    int32_t* status;               // optional [N]
+    double* cost;                  // optional [N]
+    int32_t* evals;                // optional [N]: 1 + line-search trials
+    unsigned long long* queue;     // work counter, zero at launch
+    const float* msq;              // [256] M^2/256 in the kernel's spectral layout
+    float alpha, eps, c1, min_step;
+    int max_iters, m;
+};
+
+__device__ __forceinline__ int bitrev4(int v) {
+    return ((v & 1) << 3) | ((v & 2) << 1) | ((v & 4) >> 1) | ((v & 8) >> 3);
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+// Twiddles of a 16-point radix-2 transform for lane v (0..15) of a
+// half-warp: stage s (span h = 8 >> s) pairs lanes v and v ^ h; both use
+// W16^e with e = (v & (h-1)) << s, W16 = exp(-2 pi i / 16).
+struct Twiddles {
+    float2 w[4];
+};
+
+__device__ __forceinline__ Twiddles make_twiddles(int v) {
+    Twiddles t;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        int h = 8 >> s;
+        int e = (v & (h - 1)) << s;
+        float sn, cs;
+        sincospif((float)e / 8.0f, &sn, &cs);  // angle 2*pi*e/16
+        t.w[s] = make_float2(cs, -sn);
+    }
+    return t;
+}
+
+// Forward 16-point DFT across the 16 lanes of a half-warp, one complex value
+// per lane, decimation in frequency: natural-order input, output in
+// bit-reversed order (lane v holds X[bitrev4(v)]).  Unnormalised.
+__device__ __forceinline__ float2 fft16_fwd(float2 z, int v, const Twiddles& tw) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const int h = 8 >> s;
+        float2 p;
+        p.x = __shfl_xor_sync(0xffffffffu, z.x, h);
+        p.y = __shfl_xor_sync(0xffffffffu, z.y, h);
+        const bool up = (v & h) != 0;
+        const float sg = up ? -1.0f : 1.0f;
+        float2 t = make_float2(fmaf(sg, z.x, p.x), fmaf(sg, z.y, p.y));
+        z = up ? cmul(t, tw.w[s]) : t;
+    }
+    return z;
+}
+
+// Inverse of fft16_fwd up to the factor 16: bit-reversed input, natural-order
+// output, decimation in time with conjugate twiddles, i.e. the unnormalised
+// inverse DFT sum_k X[k] exp(+2 pi i k n / 16).
+__device__ __forceinline__ float2 fft16_inv(float2 z, int v, const Twiddles& tw) {
+#pragma unroll
+    for (int s = 3; s >= 0; --s) {
+        const int h = 8 >> s;
+        float2 p;
+        p.x = __shfl_xor_sync(0xffffffffu, z.x, h);
+        p.y = __shfl_xor_sync(0xffffffffu, z.y, h);
+        const bool up = (v & h) != 0;
+        const float2 hi = up ? z : p;
+        const float2 lo = up ? p : z;
+        const float2 wc = make_float2(tw.w[s].x, -tw.w[s].y);
+        const float2 t = cmul(hi, wc);
+        const float sg = up ? -1.0f : 1.0f;
+        z = make_float2(fmaf(sg, t.x, lo.x), fmaf(sg, t.y, lo.y));
+    }
+    return z;
+}
+
+// Block-wide (one warp group) sums.  Every thread receives bitwise the same
+// result (xor butterflies are order-symmetric and the four warp partials are
+// added in a fixed order), so control flow that depends on it stays uniform.
+// `buf` alternates between two slots so one barrier per reduction suffices.
+// `red` holds two fixed 16-double slots: every reduction, whatever its K,
+// writes only its own slot, so a reduction never overwrites the slot that a
+// slower thread may still be reading from the previous one.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* red, int& buf) {
+    static_assert(K >= 1 && K <= 4, "slot holds 4 warps x 4 values");
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+    double* rb = red + buf * 16;
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) rb[w * K + k] = v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = (rb[k] + rb[K + k]) + (rb[2 * K + k] + rb[3 * K + k]);
+    buf ^= 1;
+}
+
+__device__ __forceinline__ float block_sum_f(float v, float* red, int& buf) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    float* rb = red + buf * 4;
+    if ((threadIdx.x & 31) == 0) rb[threadIdx.x >> 5] = v;
+    __syncthreads();
+    v = (rb[0] + rb[1]) + (rb[2] + rb[3]);
+    buf ^= 1;
+    return v;
+}
+
+}  // namespace ncsb

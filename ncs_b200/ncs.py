@@ -1,0 +1,309 @@
+"""Python entry points of the B200 NCS solver.
+
+Two layers:
+
+* ``Solver`` -- the torch-level API.  Device tensors in, device tensors out,
+  on the caller's current CUDA stream; wraps one ``ncsb_handle``.
+* Drop-ins for the reference Python entries, same names, argument meaning and
+  error behaviour:
+    - ``NCSCUDA`` / ``reduceNoise`` / ``checkOTFMask``  <- cuda/pyCUDANCS/ncs.py:23-226
+      (a list of frames + one gamma map + a centred mask; returns a list of
+      float32 frames; per-tile failures become ``warnings.warn``)
+    - ``cReduceNoise``  <- clib/pyCNCS/ncs_c.py:250-276 (one frame, mask
+      already fftshifted; returns float64)
+  These take host (numpy) arrays, copy them to the GPU, run the same kernel
+  and copy the result back.
+
+All compute runs in libncs_b200.so; there is no CPU fallback.
+"""
+import ctypes
+import warnings
+
+import numpy
+import torch
+
+from . import _lib
+
+
+class NCSCUDAException(Exception):
+    """Raised for invalid input in strict mode (cuda/pyCUDANCS/ncs.py:23-24)."""
+
+
+def checkOTFMask(otf_mask):
+    """True when the centred mask has the Hermitian symmetry the cost needs
+    (cuda/pyCUDANCS/ncs.py:200-208, clib/pyCNCS/ncs_c.py:239-247)."""
+    otf_mask_fft = numpy.fft.ifft2(numpy.fft.fftshift(otf_mask))
+    return not (numpy.max(numpy.imag(otf_mask_fft)) > 1.0e-12)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+_MODES = {"plain": _lib.MODE_PLAIN}
+
+
+class Solver:
+    """One NCS solver handle on one CUDA device.
+
+    Parameters mirror the reference constants (cuda/ncs.cu:54-59): ``alpha``,
+    ``max_iters`` (MAXITERS), ``m`` (history size M), ``epsilon`` (stopping
+    tolerance on ||g|| / max(1, ||u||)), ``c1`` (Armijo), ``min_step``.
+    The default ``epsilon`` is libLBFGS's 1e-5 (the pyCNCS path) rather than
+    the reference kernel's 1e-4.
+    """
+
+    def __init__(self, alpha=0.2, max_iters=200, m=8, epsilon=1e-5, c1=1e-4, min_step=1e-6,
+                 mode="plain", ctas_per_sm=0, device=None):
+        self.lib = _lib.load()
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None
+                                   else torch.device(device).index or 0)
+        self.params = _lib.default_params()
+        self._handle = ctypes.c_void_p()
+        self._set(alpha=alpha, max_iters=max_iters, m=m, epsilon=epsilon, c1=c1,
+                  min_step=min_step, mode=mode, ctas_per_sm=ctas_per_sm)
+        with torch.cuda.device(self.device):
+            rc = self.lib.ncsb_create(ctypes.byref(self._handle), ctypes.byref(self.params))
+        if rc != _lib.NCSB_OK:
+            raise RuntimeError("ncsb_create failed with code %d" % rc)
+        self.mask_shifted = None
+
+    def _set(self, **kw):
+        for k, v in kw.items():
+            if k == "mode":
+                if v not in _MODES:
+                    raise ValueError("unknown mode %r" % (v,))
+                v = _MODES[v]
+            setattr(self.params, k, v)
+
+    def _check(self, rc):
+        if rc != _lib.NCSB_OK:
+            msg = self.lib.ncsb_last_error(self._handle).decode()
+            if rc == _lib.NCSB_ESIZE:
+                raise ValueError(msg)
+            raise RuntimeError("libncs_b200 error %d: %s" % (rc, msg))
+
+    def set_params(self, **kw):
+        self._set(**kw)
+        self._check(self.lib.ncsb_set_params(self._handle, ctypes.byref(self.params)))
+
+    def set_otf_mask_shifted(self, mask_shifted):
+        """16x16 mask with DC at [0, 0] (ncs.c / ncs.cu convention)."""
+        m = numpy.ascontiguousarray(numpy.asarray(mask_shifted, dtype=numpy.float32))
+        if m.shape != (16, 16):
+            raise ValueError("OTF mask must be 16 x 16")
+        self._check(self.lib.ncsb_set_otf_mask(
+            self._handle, m.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        self.mask_shifted = m.copy()
+
+    def set_otf_mask(self, otf_mask_centred):
+        """Centred mask (DC in the middle), fftshifted here (ncs.py:197)."""
+        self.set_otf_mask_shifted(numpy.fft.fftshift(numpy.asarray(otf_mask_centred)))
+
+    def _tensor(self, x, name, shape=None):
+        if not isinstance(x, torch.Tensor) or not x.is_cuda:
+            raise TypeError("%s must be a CUDA tensor" % name)
+        if x.dtype != torch.float32:
+            raise TypeError("%s must be float32" % name)
+        if x.device != self.device:
+            raise ValueError("%s is on %s, solver on %s" % (name, x.device, self.device))
+        if shape is not None and tuple(x.shape) != tuple(shape):
+            raise ValueError("%s has shape %s, expected %s" % (name, tuple(x.shape), shape))
+        return x.contiguous()
+
+    def num_tiles(self, n_frames, height, width):
+        return _lib.num_tiles(n_frames, height, width)
+
+    def reduce_noise(self, images, gamma, out=None, tile_stats=False, stream=None):
+        """Denoise a [T, H, W] float32 CUDA stack; gamma is [H, W] (shared) or
+        [T, H, W].  Returns ``out`` or, with ``tile_stats``, (out, iters,
+        status, cost) where the per-tile arrays follow (frame, row, col) order."""
+        images = self._tensor(images, "images")
+        if images.dim() == 2:
+            images = images.unsqueeze(0)
+        T, H, W = images.shape
+        gamma = self._tensor(gamma, "gamma")
+        if gamma.shape == (H, W):
+            per_frame = 0
+        elif gamma.shape == (T, H, W):
+            per_frame = 1
+        else:
+            raise ValueError("gamma must be [H, W] or [T, H, W]")
+        if out is None:
+            out = torch.empty_like(images)
+        else:
+            out = self._tensor(out, "out", (T, H, W))
+        iters = status = cost = evals = None
+        if tile_stats:
+            n = self.num_tiles(T, H, W)
+            iters = torch.empty(n, dtype=torch.int32, device=self.device)
+            status = torch.empty(n, dtype=torch.int32, device=self.device)
+            cost = torch.empty(n, dtype=torch.float64, device=self.device)
+            evals = torch.empty(n, dtype=torch.int32, device=self.device)
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_reduce_noise(
+                self._handle, _ptr(images), T, H, W, _ptr(gamma), per_frame, _ptr(out),
+                _ptr(iters), _ptr(status), _ptr(cost), _ptr(evals),
+                ctypes.c_void_p(s.cuda_stream)))
+        if tile_stats == "all":
+            return out, iters, status, cost, evals
+        if tile_stats:
+            return out, iters, status, cost
+        return out
+
+    def solve_tiles(self, data, gamma, u0=None, stream=None):
+        """Solve [N, 16, 16] tiles (gamma per tile, the layout of the reference
+        kernel cuda/ncs.cu:873-879).  Returns (u, iters, status, cost)."""
+        data = self._tensor(data, "data")
+        n = data.shape[0]
+        if tuple(data.shape[1:]) != (16, 16):
+            raise ValueError("tiles must be [N, 16, 16]")
+        gamma = self._tensor(gamma, "gamma", data.shape)
+        if u0 is not None:
+            u0 = self._tensor(u0, "u0", data.shape)
+        u = torch.empty_like(data)
+        iters = torch.empty(n, dtype=torch.int32, device=self.device)
+        status = torch.empty(n, dtype=torch.int32, device=self.device)
+        cost = torch.empty(n, dtype=torch.float64, device=self.device)
+        evals = torch.empty(n, dtype=torch.int32, device=self.device)
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_solve_tiles(
+                self._handle, _ptr(data), _ptr(gamma), _ptr(u0), n, _ptr(u), _ptr(iters),
+                _ptr(status), _ptr(cost), _ptr(evals), ctypes.c_void_p(s.cuda_stream)))
+        self.last_evals = evals
+        return u, iters, status, cost
+
+    def close(self):
+        if getattr(self, "_handle", None) and self._handle.value:
+            self.lib.ncsb_destroy(self._handle)
+            self._handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _status_report(status, iters, verbose):
+    """Warning / verbose summary of per-tile outcomes (cuda/pyCUDANCS/ncs.py:131-159)."""
+    status = numpy.asarray(status)
+    iters = numpy.asarray(iters)
+    failures = {}
+    n_fails = int(numpy.count_nonzero(status != 0))
+    if n_fails > 0:
+        n_maxp = int(numpy.count_nonzero(status == _lib.REACHED_MAXPRECISION))
+        if n_maxp != n_fails:
+            warnings.warn("Noise reduction failed on {0:d} sub-regions.".format(n_fails))
+        for i in range(-5, 0):
+            nf = int(numpy.count_nonzero(status == i))
+            if nf:
+                failures[i] = nf
+    if verbose:
+        print("Minimum iterations: {0:d}".format(int(iters.min())))
+        print("Maximum iterations: {0:d}".format(int(iters.max())))
+        print("Median iterations: {0:.3f}".format(float(numpy.median(iters))))
+        for key, n in failures.items():
+            print(n, "failures of type '" + _lib.STATUS_NAMES[key] + "'")
+        print()
+    return failures
+
+
+class NCSCUDA:
+    """Drop-in for pyCUDANCS.ncs.NCSCUDA (cuda/pyCUDANCS/ncs.py:27-197).
+
+    ``setOTFMask`` takes the centred 16x16 mask, ``setGamma`` one H x W map
+    shared by all frames, ``reduceNoise(images, alpha)`` a list of equally
+    sized frames in photo-electrons.  Extra keyword arguments go to
+    ``Solver`` (e.g. ``max_iters``, ``epsilon``)."""
+
+    def __init__(self, strict=True, **solver_kwargs):
+        self.size = 16
+        self.strict = strict
+        self.gamma = None
+        self.otf_mask = None
+        self._solver_kwargs = solver_kwargs
+        self._solver = None
+
+    def _get_solver(self, alpha):
+        if self._solver is None:
+            self._solver = Solver(alpha=float(alpha), **self._solver_kwargs)
+        else:
+            self._solver.set_params(alpha=float(alpha))
+        return self._solver
+
+    def setGamma(self, gamma):
+        """CMOS variance / gain^2 in e-^2, shared by all frames (ncs.py:175-181)."""
+        self.gamma = numpy.asarray(gamma).astype(numpy.float32)
+
+    def setOTFMask(self, otf_mask):
+        """Centred OTF mask (ncs.py:183-197)."""
+        otf_mask = numpy.asarray(otf_mask)
+        if self.strict:
+            if otf_mask.shape[0] != otf_mask.shape[1]:
+                raise NCSCUDAException("OTF must be square!")
+            if otf_mask.size != self.size * self.size:
+                raise NCSCUDAException("OTF size must match sub-region size!")
+            if not checkOTFMask(otf_mask):
+                raise NCSCUDAException("OTF does not have the expected symmetry!")
+        self.otf_mask = numpy.fft.fftshift(otf_mask).astype(numpy.float32)
+
+    def reduceNoise(self, images, alpha, verbose=False):
+        """Denoise a list of frames (ncs.py:35-173); returns a list of float32 frames."""
+        if self.otf_mask is None or self.gamma is None:
+            raise NCSCUDAException("setOTFMask() and setGamma() must be called first")
+        images = [numpy.asarray(im) for im in images]
+        if len(images) == 0:
+            return []
+        im0_shape = images[0].shape
+        for im in images:
+            if im.shape != im0_shape:
+                raise NCSCUDAException("All images must be the same size!")
+        if self.gamma.shape != im0_shape:
+            raise NCSCUDAException("gamma must have the same shape as the images!")
+        solver = self._get_solver(alpha)
+        solver.set_otf_mask_shifted(self.otf_mask)
+        host = torch.from_numpy(numpy.stack(images).astype(numpy.float32)).pin_memory()
+        ghost = torch.from_numpy(self.gamma).pin_memory()
+        dev = solver.device
+        x = host.to(dev, non_blocking=True)
+        g = ghost.to(dev, non_blocking=True)
+        out, iters, status, _ = solver.reduce_noise(x, g, tile_stats=True)
+        result = out.cpu().numpy()
+        if verbose:
+            print("Processed {0:d} sub-regions.".format(iters.numel()))
+        _status_report(status.cpu().numpy(), iters.cpu().numpy(), verbose)
+        return [result[i] for i in range(result.shape[0])]
+
+
+def reduceNoise(images, gamma, otf_mask, alpha, strict=True, verbose=False, **solver_kwargs):
+    """Drop-in for pyCUDANCS.ncs.reduceNoise (cuda/pyCUDANCS/ncs.py:211-226)."""
+    ncs = NCSCUDA(strict=strict, **solver_kwargs)
+    ncs.setOTFMask(otf_mask)
+    ncs.setGamma(gamma)
+    return ncs.reduceNoise(images, alpha, verbose=verbose)
+
+
+def cReduceNoise(image, gamma, otf_mask, alpha, strict=True, **solver_kwargs):
+    """GPU drop-in for pyCNCS.ncs_c.cReduceNoise (clib/pyCNCS/ncs_c.py:250-276).
+
+    ``otf_mask`` is already fftshifted (DC at [0, 0]), as the reference C call
+    expects.  Returns a float64 frame like the reference."""
+    otf_mask = numpy.asarray(otf_mask)
+    if strict:
+        if otf_mask.shape[0] != otf_mask.shape[1]:
+            raise NCSCUDAException("OTF must be square!")
+        if (otf_mask.shape[0] % 2) != 0:
+            raise NCSCUDAException("Sub region size must be divisible by 2!")
+    if otf_mask.shape != (16, 16):
+        raise NCSCUDAException("Only 16 x 16 sub-regions are supported on the GPU.")
+    solver = Solver(alpha=float(alpha), **solver_kwargs)
+    solver.set_otf_mask_shifted(otf_mask)
+    x = torch.from_numpy(numpy.ascontiguousarray(image, dtype=numpy.float32)).to(solver.device)
+    g = torch.from_numpy(numpy.ascontiguousarray(gamma, dtype=numpy.float32)).to(solver.device)
+    out = solver.reduce_noise(x, g)
+    res = out[0].cpu().numpy().astype(numpy.float64)
+    solver.close()
+    return res

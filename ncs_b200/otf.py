@@ -1,0 +1,56 @@
+"""OTF masks for the NCS noise term (16 x 16, returned CENTRED, DC at [8, 8];
+``numpy.fft.fftshift`` gives the shifted form the solver takes).
+
+* ``otf_weighted_mask`` -- 1 - normalised incoherent OTF of a circular pupil
+  inside the cutoff 2 NA / lambda, 1 outside: the high-pass mask of the
+  synthetic workloads (the OTF-weighted idea of pyNCS ``genfilter``, with the
+  textbook diffraction-limited OTF instead of a raised cosine).
+* ``genfilter`` -- the reference's raised-cosine masks, restated from
+  python3-6/pyNCS/denoisetools.py:227-261 (types pureN / adjustable /
+  OTFweighted), with ``genkspace`` from :96-101.
+"""
+import numpy
+
+
+def genkspace(R, pixelsize):
+    """|k| grid of an R x R tile in cycles per unit of pixelsize, centred
+    (denoisetools.py:96-101)."""
+    X, Y = numpy.meshgrid(numpy.arange(-R / 2, R / 2, 1), numpy.arange(-R / 2, R / 2, 1))
+    return numpy.sqrt(X ** 2 + Y ** 2) / (R * pixelsize)
+
+
+def otf_weighted_mask(R=16, pixelsize=0.1, NA=1.4, wavelength=0.7):
+    """1 - OTF(|k| / kc) for |k| < kc = 2 NA / lambda, 1 outside, with the
+    circular-pupil incoherent OTF (2/pi)(acos(r) - r sqrt(1 - r^2)).
+    Lengths in micrometres.  Returns the centred mask (float64)."""
+    kr = genkspace(R, pixelsize)
+    kc = 2.0 * NA / wavelength
+    rho = numpy.clip(kr / kc, 0.0, 1.0)
+    otf = (2.0 / numpy.pi) * (numpy.arccos(rho) - rho * numpy.sqrt(1.0 - rho ** 2))
+    return numpy.where(kr < kc, 1.0 - otf, 1.0)
+
+
+def genfilter(R, pixelsize, NA, Lambda, Type="OTFweighted", w=1, h=0.7):
+    """Raised-cosine high-pass of pyNCS (denoisetools.py:227-261); centred."""
+    kr = genkspace(R, pixelsize)
+    kmax = 1.0 / numpy.sqrt(2.0) / pixelsize
+    if Type == "pureN":
+        beta = 0.2
+        T = (1 - beta) * Lambda / 4 / NA
+    elif Type == "adjustable":
+        w0 = w * NA / Lambda
+        beta = numpy.pi / 2 * (kmax / w0 - 1) / (numpy.arccos(1 - 2 * h) + numpy.pi / 2 * (kmax / w0 - 1))
+        T = (1 - beta) / w0 / 2
+    elif Type == "OTFweighted":
+        beta = 1.0
+        T = Lambda / 4 / NA / 1.4
+    else:
+        raise ValueError("unknown filter type %r" % (Type,))
+    rc = 0.5 * (1 + numpy.cos(numpy.pi * T / beta * (kr - (1 - beta) / 2 / T)))
+    rc[kr < (1 - beta) / 2 / T] = 1
+    rc[kr > (1 + beta) / 2 / T] = 0
+    return 1 - rc
+
+
+def shifted(mask_centred):
+    return numpy.fft.fftshift(numpy.asarray(mask_centred))

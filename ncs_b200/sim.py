@@ -1,0 +1,118 @@
+"""Seeded synthetic sCMOS stacks with the shapes and statistics of the named
+NCS workloads (the reference's own simulation inputs -- calibration .mat
+maps -- are not shipped, so these stand in for them).
+
+Physics (all lengths in micrometres):
+  * structure: worm-like chains, persistence length 2, contour length
+    U(5, 10), tangent angle diffusing so that <cos> decays as exp(-s/Lp);
+    emitters every 0.02 along each chain, ``photons`` each;
+  * optics: Gaussian PSF sigma = 0.21 lambda / NA (lambda 0.7, NA 1.4 ->
+    0.105 = 1.05 px at 0.1 px size), integrated over each pixel;
+  * background ``bg`` photons / px, independent Poisson draw per frame;
+  * camera (per pixel): offset ~ N(100, 2) ADU, gain ~ N(2, 0.2) ADU/e-,
+    read variance ~ Exponential(mean 60 ADU^2); optional hot pixels whose
+    variance is x50.  ADU = gain * photons + sqrt(var) N(0,1) + offset;
+  * NCS inputs as python3-6/pyNCS/denoisetools.py:205-225: d = (ADU -
+    offset) / gain with d <= 0 set to 1e-6, gamma = var / gain^2.
+The ideal image and camera maps are drawn with numpy PCG64 (CPU, small);
+frames are drawn with a seeded torch generator on the target device.
+"""
+import math
+
+import numpy
+import torch
+
+from .otf import otf_weighted_mask
+
+WORKLOADS = {
+    # 1 frame 256x256, 12 chains, L-BFGS cap 15
+    "frame256": dict(T=1, H=256, W=256, chains=12, photons=100.0, bg=10.0, hot=0.0,
+                     alpha=0.2, max_iters=15),
+    # 200 frames 512x512, shared gamma map, cap 20, all tiles in one launch
+    "stack512": dict(T=200, H=512, W=512, chains=12, photons=100.0, bg=10.0, hot=0.0,
+                     alpha=0.2, max_iters=20),
+    # 100 frames 2048x2048, 60 chains, 0.5% hot pixels, run to the stopping rule
+    "sensor2048": dict(T=100, H=2048, W=2048, chains=60, photons=100.0, bg=10.0, hot=0.005,
+                       alpha=0.2, max_iters=200),
+}
+
+
+def wlc_emitters(n_chains, field, rng, lp=2.0, length=(5.0, 10.0), spacing=0.02):
+    """Emitter positions (x, y) of n_chains 2-D worm-like chains in a square field."""
+    out = []
+    for _ in range(n_chains):
+        L = rng.uniform(*length)
+        n = max(int(L / spacing), 2)
+        th0 = rng.uniform(0.0, 2.0 * math.pi)
+        dth = rng.normal(0.0, math.sqrt(2.0 * spacing / lp), size=n)
+        th = th0 + numpy.cumsum(dth)
+        x = rng.uniform(0.0, field) + numpy.cumsum(spacing * numpy.cos(th))
+        y = rng.uniform(0.0, field) + numpy.cumsum(spacing * numpy.sin(th))
+        out.append(numpy.stack([x, y], axis=1))
+    return numpy.concatenate(out, axis=0)
+
+
+def render(emitters_px, H, W, sigma_px, photons, bg, half=5):
+    """bg + photons * pixel-integrated Gaussian PSF at each emitter (px units,
+    pixel i spans [i, i+1))."""
+    from scipy.special import erf
+    img = numpy.full((H, W), float(bg))
+    s2 = math.sqrt(2.0) * sigma_px
+    for x, y in emitters_px:  # x along W (columns), y along H (rows)
+        cx, cy = int(math.floor(x)), int(math.floor(y))
+        cols = numpy.arange(cx - half, cx + half + 1)
+        rows = numpy.arange(cy - half, cy + half + 1)
+        px = 0.5 * (erf((cols + 1 - x) / s2) - erf((cols - x) / s2))
+        py = 0.5 * (erf((rows + 1 - y) / s2) - erf((rows - y) / s2))
+        rm = (rows >= 0) & (rows < H)
+        cm = (cols >= 0) & (cols < W)
+        if rm.any() and cm.any():
+            img[numpy.ix_(rows[rm], cols[cm])] += photons * numpy.outer(py[rm], px[cm])
+    return img
+
+
+def camera_maps(H, W, rng, hot=0.0):
+    offset = rng.normal(100.0, 2.0, size=(H, W))
+    gain = rng.normal(2.0, 0.2, size=(H, W))
+    var = rng.exponential(60.0, size=(H, W))
+    if hot > 0:
+        mask = rng.uniform(size=(H, W)) < hot
+        var[mask] *= 50.0
+    return offset, gain, var
+
+
+def make_stack(name="stack512", T=None, device="cuda", seed=1234, pixel=0.1, NA=1.4,
+               wavelength=0.7):
+    """Build a named workload.  Returns a dict with ``images`` [T,H,W] and
+    ``gamma`` [H,W] (float32 torch tensors on ``device``), ``mask`` (centred
+    16x16 numpy), ``alpha``, ``max_iters`` and the generating parameters."""
+    cfg = dict(WORKLOADS[name])
+    if T is not None:
+        cfg["T"] = int(T)
+    rng = numpy.random.default_rng(seed)
+    H, W = cfg["H"], cfg["W"]
+    field = max(H, W) * pixel
+    em = wlc_emitters(cfg["chains"], field, rng) / pixel
+    sigma_px = 0.21 * wavelength / NA / pixel
+    ideal = render(em, H, W, sigma_px, cfg["photons"], cfg["bg"])
+    offset, gain, var = camera_maps(H, W, rng, cfg["hot"])
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 1)
+    t_ideal = torch.as_tensor(ideal, dtype=torch.float32, device=dev)
+    t_gain = torch.as_tensor(gain, dtype=torch.float32, device=dev)
+    t_off = torch.as_tensor(offset, dtype=torch.float32, device=dev)
+    t_sd = torch.as_tensor(numpy.sqrt(var), dtype=torch.float32, device=dev)
+    images = torch.empty((cfg["T"], H, W), dtype=torch.float32, device=dev)
+    chunk = max(1, (1 << 26) // (H * W))
+    for f0 in range(0, cfg["T"], chunk):
+        n = min(chunk, cfg["T"] - f0)
+        lam = t_ideal.expand(n, H, W).contiguous()
+        phot = torch.poisson(lam, generator=g)
+        adu = phot * t_gain + t_sd * torch.randn((n, H, W), generator=g, device=dev) + t_off
+        d = (adu - t_off) / t_gain
+        images[f0:f0 + n] = torch.where(d <= 0, torch.full_like(d, 1e-6), d)
+    gamma = torch.as_tensor(var / gain ** 2, dtype=torch.float32, device=dev)
+    mask = otf_weighted_mask(16, pixel, NA, wavelength)
+    return dict(images=images, gamma=gamma, mask=mask, alpha=cfg["alpha"],
+                max_iters=cfg["max_iters"], ideal=ideal, name=name, seed=seed, cfg=cfg)

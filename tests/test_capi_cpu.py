@@ -1,0 +1,62 @@
+"""CPU tests of the C ABI library: it loads, exports every symbol the header
+declares, and its host-only functions agree with the oracle.  No device
+compute is called here."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from ncs_b200 import _lib, build
+    build.build()
+    return _lib.load()
+
+
+def declared_symbols():
+    hdr = open(os.path.join(ROOT, "include", "ncs_b200.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    return sorted(set(re.findall(r"\b(ncsb_[a-z_0-9]+)\s*\(", hdr)))
+
+
+def test_exports_every_declared_symbol(lib):
+    from ncs_b200 import _lib
+    syms = declared_symbols()
+    assert set(syms) == set(_lib.EXPORTS)
+    for s in syms:
+        assert hasattr(lib, s), s
+
+
+def test_default_params(lib):
+    from ncs_b200 import _lib
+    p = _lib.default_params()
+    assert (p.alpha, p.max_iters, p.m, p.epsilon, p.c1, p.min_step, p.mode) == \
+        (0.2, 200, 8, 1e-5, 1e-4, 1e-6, 0)
+
+
+def test_num_tiles_matches_oracle(lib):
+    from ncs_b200 import _lib
+    from oracle import numpy_ref as nr
+    for T, H, W in [(1, 256, 256), (200, 512, 512), (100, 2048, 2048), (3, 14, 31), (2, 45, 37)]:
+        assert _lib.num_tiles(T, H, W) == T * len(nr.tile_origins(H)) * len(nr.tile_origins(W))
+    assert _lib.num_tiles(1, 256, 256) == 361
+    assert _lib.num_tiles(200, 512, 512) == 273800
+    assert _lib.num_tiles(100, 2048, 2048) == 2160900
+    with pytest.raises(ValueError):
+        _lib.num_tiles(1, 13, 40)
+
+
+def test_null_handle_is_rejected(lib):
+    from ncs_b200 import _lib
+    assert lib.ncsb_set_otf_mask(None, None) == _lib.NCSB_EINVAL
+    assert lib.ncsb_destroy(None) == _lib.NCSB_EINVAL
+    assert lib.ncsb_reduce_noise(None, None, 1, 16, 16, None, 0, None, None, None, None, None,
+                                 None) == _lib.NCSB_EINVAL
+    assert lib.ncsb_last_error(None) == b"null handle"
+    n = ctypes.c_int64()
+    assert lib.ncsb_num_tiles(1, 16, 16, None) == _lib.NCSB_EINVAL
+    assert lib.ncsb_num_tiles(-1, 16, 16, ctypes.byref(n)) == _lib.NCSB_EINVAL

@@ -1,0 +1,204 @@
+"""GPU parity tests of the plain solver through the C ABI (libncs_b200.so).
+
+Models: cuda/pyCUDANCS/test/test_solver.py (tiles vs the Python mirror and
+vs the C solver), cuda/pyCUDANCS/test/test_im.py (144 odd-sized crops vs
+pyCNCS cReduceNoise), plus exact checks the reference does not have (device
+stitching vs host stitching, FP64 optimum, status codes, determinism).
+Tolerances are stated per test.
+"""
+import numpy
+import pytest
+import torch
+
+from conftest import create_otf_mask_shifted, random_otf_mask
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ncs(cuda_ok):
+    import ncs_b200
+    return ncs_b200
+
+
+def tiles_seed1(n, rng=None):
+    """data U(10,20), gamma U(2,4) -- cuda/pyCUDANCS/test/test_solver.py:79-84."""
+    numpy.random.seed(1)
+    data = numpy.random.uniform(10.0, 20.0, size=(n, 16, 16)).astype(numpy.float32)
+    gamma = numpy.random.uniform(2.0, 4.0, size=(n, 16, 16)).astype(numpy.float32)
+    return data, gamma
+
+
+def test_tiles_vs_fp64_optimum_and_reference(ncs, oracle_libs):
+    from oracle import numpy_ref as nr
+    n, alpha = 64, 0.1
+    data, gamma = tiles_seed1(n)
+    ms = create_otf_mask_shifted()
+    s = ncs.Solver(alpha=alpha, epsilon=1e-6, max_iters=500)
+    s.set_otf_mask_shifted(ms)
+    u, iters, status, cost = s.solve_tiles(torch.from_numpy(data).cuda(),
+                                           torch.from_numpy(gamma).cuda())
+    u = u.cpu().numpy().astype(numpy.float64)
+    status = status.cpu().numpy()
+    assert (status == 0).all(), status
+    ustar, fstar, _ = nr.newton_solve(data, gamma, ms.astype(numpy.float64), alpha)
+    f_gpu = nr.cost(u, data.astype(numpy.float64), gamma.astype(numpy.float64),
+                    ms.astype(numpy.float64), alpha)
+    # per tile: final cost within 1e-6 relative of the FP64 optimum
+    assert nr.rel_cost_gap(f_gpu, fstar).max() <= 1e-6
+    # per pixel: within 1e-3 relative of the optimum
+    assert (numpy.abs(u - ustar) / numpy.maximum(numpy.abs(ustar), 1.0)).max() <= 1e-3
+    # the kernel's own FP64 cost report agrees with numpy at its u
+    assert numpy.allclose(cost.cpu().numpy(), f_gpu, rtol=1e-7, atol=1e-6)
+    # vs the pyCNCS C solver (compiled reference when available, else the port)
+    for i in range(n):
+        uref, ret, fref = oracle_libs.solve_tile(data[i].astype(numpy.float64),
+                                                 gamma[i].astype(numpy.float64),
+                                                 ms.astype(numpy.float64), alpha)
+        # reference criterion (test_solver.py:116-118) and the north-star one
+        assert numpy.abs(u[i] - uref).max() / numpy.abs(uref).max() < 1e-2
+        assert nr.rel_cost_gap(f_gpu[i], fref) <= 1e-4
+        assert (numpy.abs(u[i] - uref) / numpy.maximum(numpy.abs(uref), 1.0)).max() <= 1e-3
+
+
+def test_matches_pycncs_on_photon_like_tiles(ncs, oracle_libs):
+    """GPU vs the pyCNCS C path on bright photon-like tiles (alpha 0.2).
+
+    At both solvers' default stopping rule (epsilon 1e-5 on ||g||/max(1,||u||))
+    the final costs agree within 1e-4 relative per tile.  Per-pixel parity
+    (<= 1e-3 relative) is checked with both solvers converged to epsilon 1e-6:
+    at 1e-5 pyCNCS itself stops up to ~2e-3 relative from the exact optimum
+    on tiles of a few hundred photons, so no solver could match it closer.
+    """
+    from oracle import numpy_ref as nr
+    n, alpha = 32, 0.2
+    rng = numpy.random.default_rng(7)
+    data = rng.uniform(5.0, 300.0, size=(n, 16, 16)).astype(numpy.float32)
+    gamma = rng.exponential(15.0, size=(n, 16, 16)).astype(numpy.float32) + 0.5
+    ms = create_otf_mask_shifted()
+    d64, g64, m64 = (x.astype(numpy.float64) for x in (data, gamma, ms))
+    for eps, check_pixels in ((1e-5, False), (1e-6, True)):
+        s = ncs.Solver(alpha=alpha, epsilon=eps, max_iters=1000)
+        s.set_otf_mask_shifted(ms)
+        u, iters, status, cost = s.solve_tiles(torch.from_numpy(data).cuda(),
+                                               torch.from_numpy(gamma).cuda())
+        assert (status.cpu().numpy() == 0).all()
+        u = u.cpu().numpy().astype(numpy.float64)
+        oracle_libs.set_overrides(epsilon=eps)
+        try:
+            for i in range(n):
+                uref, ret, fref = oracle_libs.solve_tile(d64[i], g64[i], m64, alpha)
+                fg = nr.cost(u[i], d64[i], g64[i], m64, alpha)
+                assert nr.rel_cost_gap(fg, fref) <= 1e-4
+                if check_pixels:
+                    rel = numpy.abs(u[i] - uref) / numpy.maximum(numpy.abs(uref), 1.0)
+                    assert rel.max() <= 1e-3
+        finally:
+            oracle_libs.set_overrides()
+
+
+@pytest.mark.parametrize("shape", [(2, 45, 37), (1, 14, 14), (3, 16, 30), (1, 64, 64)])
+def test_stack_mode_equals_host_tiling(ncs, shape):
+    """Device segmentation + owner-rule stitching is bit-identical to host
+    tiling (numpy.pad 'edge', ncs_c.py:296-319) + tile solve + row-major
+    overwrite stitching (ncs.c:121-130)."""
+    from oracle import numpy_ref as nr
+    rng = numpy.random.default_rng(3)
+    T, H, W = shape
+    images = rng.uniform(1.0, 50.0, size=shape).astype(numpy.float32)
+    gamma = rng.uniform(1.0, 20.0, size=(H, W)).astype(numpy.float32)
+    s = ncs.Solver(alpha=0.2, max_iters=30)
+    s.set_otf_mask_shifted(create_otf_mask_shifted())
+    out, iters, status, cost = s.reduce_noise(torch.from_numpy(images).cuda(),
+                                              torch.from_numpy(gamma).cuda(), tile_stats=True)
+    td, tg, meta = nr.segment(images, gamma)
+    assert td.shape[0] == s.num_tiles(T, H, W) == iters.numel()
+    u, it2, st2, c2 = s.solve_tiles(torch.from_numpy(td.astype(numpy.float32)).cuda(),
+                                    torch.from_numpy(tg.astype(numpy.float32)).cuda())
+    ref = nr.stitch(u.cpu().numpy().astype(numpy.float64), meta, shape).astype(numpy.float32)
+    assert numpy.array_equal(out.cpu().numpy(), ref)
+    assert numpy.array_equal(iters.cpu().numpy(), it2.cpu().numpy())
+    assert numpy.array_equal(status.cpu().numpy(), st2.cpu().numpy())
+
+
+def test_crops_vs_pycncs(ncs, oracle_libs):
+    """cuda/pyCUDANCS/test/test_im.py:16-44: 144 crops of a 30x30 frame,
+    alpha 0.02, random symmetric mask, atol 0.02 against cReduceNoise."""
+    rng = numpy.random.default_rng(1)
+    gamma = rng.uniform(2.0, 4.0, size=(30, 30))
+    image = rng.uniform(0.01, 10.0, size=(30, 30))
+    otfmask = random_otf_mask(16, rng)
+    shifted = numpy.fft.fftshift(otfmask)
+    nc = ncs.NCSCUDA()
+    nc.setOTFMask(otfmask)
+    worst = 0.0
+    for ix in range(12):
+        for iy in range(12):
+            im, gm = image[ix:, iy:], gamma[ix:, iy:]
+            ref = oracle_libs.cReduceNoise(im, gm, shifted, 0.02)
+            nc.setGamma(gm)
+            got = nc.reduceNoise([im], 0.02)[0]
+            worst = max(worst, float(numpy.abs(got - ref).max()))
+            assert numpy.allclose(ref, got, atol=0.02)
+    assert worst < 0.02
+
+
+def test_status_codes_and_caps(ncs):
+    data, gamma = tiles_seed1(8)
+    s = ncs.Solver(alpha=0.1, max_iters=0)
+    s.set_otf_mask_shifted(create_otf_mask_shifted())
+    d = torch.from_numpy(data).cuda()
+    g = torch.from_numpy(gamma).cuda()
+    u, iters, status, _ = s.solve_tiles(d, g)
+    assert (status.cpu().numpy() == -2).all()        # REACHED_MAXITERS
+    assert (iters.cpu().numpy() == 0).all()
+    assert torch.equal(u, d)                          # untouched start point
+    s.set_params(max_iters=3)
+    u, iters, status, _ = s.solve_tiles(d, g)
+    assert (iters.cpu().numpy() <= 3).all()
+    # a tile with a NaN pixel ends in bounded time with a failure status,
+    # the other tiles are unaffected
+    bad = d.clone()
+    bad[2, 5, 5] = float("nan")
+    s.set_params(max_iters=200)
+    u1, _, st1, _ = s.solve_tiles(d, g)
+    u2, _, st2, _ = s.solve_tiles(bad, g)
+    st2 = st2.cpu().numpy()
+    assert st2[2] != 0
+    keep = [i for i in range(8) if i != 2]
+    assert torch.equal(u1[keep], u2[keep])
+
+
+def test_warm_start_input_and_determinism(ncs):
+    data, gamma = tiles_seed1(16)
+    s = ncs.Solver(alpha=0.1, epsilon=1e-6)
+    s.set_otf_mask_shifted(create_otf_mask_shifted())
+    d = torch.from_numpy(data).cuda()
+    g = torch.from_numpy(gamma).cuda()
+    u1, it1, _, _ = s.solve_tiles(d, g)
+    u2, it2, _, _ = s.solve_tiles(d, g)
+    assert torch.equal(u1, u2) and torch.equal(it1, it2)   # shared-memory race canary
+    # starting at the solution converges immediately
+    u3, it3, st3, _ = s.solve_tiles(d, g, u0=u1)
+    assert (it3.cpu().numpy() <= 1).all()
+    assert (st3.cpu().numpy() == 0).all()
+
+
+def test_drop_in_errors(ncs):
+    nc = ncs.NCSCUDA()
+    with pytest.raises(ncs.NCSCUDAException):
+        nc.setOTFMask(numpy.ones((16, 8)))
+    with pytest.raises(ncs.NCSCUDAException):
+        nc.setOTFMask(numpy.ones((8, 8)))
+    asym = numpy.zeros((16, 16))
+    asym[3, 4] = 1.0
+    with pytest.raises(ncs.NCSCUDAException):
+        nc.setOTFMask(asym)
+    nc.setOTFMask(numpy.fft.fftshift(create_otf_mask_shifted()))
+    nc.setGamma(numpy.ones((20, 20)))
+    with pytest.raises(ncs.NCSCUDAException):
+        nc.reduceNoise([numpy.ones((20, 20)), numpy.ones((21, 20))], 0.1)
+    with pytest.raises(ValueError):
+        s = ncs.Solver()
+        s.set_otf_mask_shifted(create_otf_mask_shifted())
+        s.reduce_noise(torch.ones(1, 10, 10, device="cuda"), torch.ones(10, 10, device="cuda"))

@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math_constants.h>
 #include <stdint.h>
 
 namespace ncsb {
@@ -15,6 +16,7 @@ constexpr int kPix = 256;
 constexpr int kThreads = 128;  // one warp group per tile
 constexpr int kMaxM = 8;       // L-BFGS history capacity
 constexpr float kFitMin = 1.0e-6f;  // FITMIN, ncs.c:169 / ncs.cu:40
+constexpr float kBarrierFrac = 0.01f;  // line-search trials keep u+gamma >= 1% of its value
 
 // Per-tile solver status, identical values to cuda/ncs.cu:61-67.
 enum Status : int32_t {

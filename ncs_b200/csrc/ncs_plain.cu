@@ -198,7 +198,16 @@ __global__ void __launch_bounds__(kThreads, 8) ncs_plain_kernel(const SolveArgs 
                     else l0 = logf(fmaxf(n0, kFitMin)) - logf(fmaxf(a0, kFitMin));
                     if (a1 >= kFitMin && n1 >= kFitMin) l1 = log1pf(tp1 / a1);
                     else l1 = logf(fmaxf(n1, kFitMin)) - logf(fmaxf(a1, kFitMin));
-                    double dl[1] = {((double)tp0 - (double)c0 * l0) + ((double)tp1 - (double)c1 * l1)};
+                    // Fraction to the log barrier: a trial that takes a pixel below 1 % of
+                    // its u + gamma is infeasible (cost +inf).  Without it the FITMIN
+                    // clamp makes points past the barrier look cheaper and Armijo-only
+                    // backtracking accepts them (the reference's Moré–Thuente search
+                    // rejects them through its curvature test).
+                    const bool cross = (a0 >= kFitMin && n0 < kBarrierFrac * a0) ||
+                                       (a1 >= kFitMin && n1 < kBarrierFrac * a1);
+                    double dl[1] = {cross ? CUDART_INF
+                                          : ((double)tp0 - (double)c0 * l0) +
+                                                ((double)tp1 - (double)c1 * l1)};
                     block_sum<1>(dl, sm.redd, bufd);
                     ++evals;
                     const double td = (double)t;

@@ -202,3 +202,24 @@ def test_drop_in_errors(ncs):
         s = ncs.Solver()
         s.set_otf_mask_shifted(create_otf_mask_shifted())
         s.reduce_noise(torch.ones(1, 10, 10, device="cuda"), torch.ones(10, 10, device="cuda"))
+
+
+def test_accuracy_gate_on_synthetic_frames(ncs):
+    """stack512-style frames with the workload cap (20 iterations): every
+    sampled tile's final cost within 1e-4 relative of the FP64 optimum, and
+    no line-search failures (the fraction-to-barrier rule keeps trials out of
+    the FITMIN-clamped region)."""
+    from ncs_b200 import sim
+    from oracle import numpy_ref as nr
+    w = sim.make_stack("stack512", T=2, device="cuda", seed=77)
+    s = ncs.Solver(alpha=w["alpha"], max_iters=w["max_iters"])
+    s.set_otf_mask(w["mask"])
+    out, iters, status, cost = s.reduce_noise(w["images"], w["gamma"], tile_stats=True)
+    st = status.cpu().numpy()
+    assert set(numpy.unique(st)) <= {0, -2}, numpy.unique(st, return_counts=True)
+    td, tg, _ = nr.segment(w["images"].cpu().numpy(), w["gamma"].cpu().numpy())
+    sel = numpy.arange(0, td.shape[0], 5)
+    ms = numpy.fft.fftshift(w["mask"]).astype(numpy.float32).astype(numpy.float64)
+    _, fs, _ = nr.newton_solve(td[sel], tg[sel], ms, w["alpha"])
+    gap = nr.rel_cost_gap(cost.cpu().numpy()[sel], fs)
+    assert gap.max() <= 1e-4, gap.max()

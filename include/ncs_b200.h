@@ -42,6 +42,10 @@ extern "C" {
 #define NCSB_ECUDA (-2)    /* a CUDA runtime call failed */
 #define NCSB_ENOMASK (-3)  /* ncsb_set_otf_mask() has not been called */
 #define NCSB_ESIZE (-4)    /* image smaller than a tile interior on an axis */
+#define NCSB_ESCRATCH (-5) /* request needs more than the static scratch holds */
+
+/* Capacity of the static device scratch of ncsb_reduce_noise_noalloc. */
+#define NCSB_NOALLOC_SCRATCH_BYTES 4096
 
 /* Per-tile solver status (same values as cuda/ncs.cu:61-67). */
 #define NCSB_SUCCESS 0
@@ -121,6 +125,39 @@ int ncsb_reduce_noise(ncsb_handle *h, const float *images, int n_frames, int hei
 int ncsb_solve_tiles(ncsb_handle *h, const float *data_in, const float *gamma_in,
                      const float *u0, int64_t n_tiles, float *data_out, int32_t *iters,
                      int32_t *status, double *cost, int32_t *evals, void *stream);
+
+/*
+ * ncsb_reduce_noise without a handle and without allocating device memory.
+ * No counterpart in the reference: it exists for callers that may not call
+ * cudaMalloc while they run -- a plug-in in an acquisition or image-server
+ * process whose host application owns the GPU memory budget through its own
+ * pool, or a real-time pipeline that forbids device allocation after start-up
+ * because cudaMalloc can synchronise the device and stall the camera stream.
+ * Such callers cannot use ncsb_create, which allocates the work counter and
+ * the mask table.
+ *
+ * Same arguments and results as ncsb_reduce_noise, plus the solver
+ * parameters and the 16x16 shifted OTF mask (host memory) that a handle would
+ * hold.  The work counter and the mask table live instead in one file-scope
+ * __device__ array of NCSB_NOALLOC_SCRATCH_BYTES (4 KiB), held by every GPU
+ * that loads the library until the process exits; this call uses 1280 bytes
+ * of it whatever the stack size, and a request that would need more than the
+ * capacity is rejected with NCSB_ESCRATCH.  The call allocates nothing: no
+ * cudaMalloc, cudaFree or allocating library routine.
+ *
+ * The first call on a device does a one-time set-up (it looks up the
+ * array's device address with cudaGetSymbolAddress and caches the launch
+ * geometry) and should come before any stream capture.  Every call shares the
+ * array and re-initialises it on its own stream (mask table copy, counter
+ * reset) before its launch, so calls that overlap on the GPU -- on two
+ * streams or from two host threads -- race and must be serialised by the
+ * caller.
+ */
+int ncsb_reduce_noise_noalloc(const ncsb_params *p, const float *mask_shifted_host,
+                              const float *images, int n_frames, int height, int width,
+                              const float *gamma, int gamma_per_frame, float *out,
+                              int32_t *tile_iters, int32_t *tile_status, double *tile_cost,
+                              int32_t *tile_evals, void *stream);
 
 #ifdef __cplusplus
 }

@@ -14,6 +14,7 @@ NCSB_EINVAL = -1
 NCSB_ECUDA = -2
 NCSB_ENOMASK = -3
 NCSB_ESIZE = -4
+NCSB_ESCRATCH = -5
 
 MODE_PLAIN = 0
 
@@ -50,6 +51,7 @@ class NcsbParams(ctypes.Structure):
 EXPORTS = [
     "ncsb_default_params", "ncsb_create", "ncsb_set_params", "ncsb_destroy", "ncsb_last_error",
     "ncsb_set_otf_mask", "ncsb_num_tiles", "ncsb_reduce_noise", "ncsb_solve_tiles",
+    "ncsb_reduce_noise_noalloc",
 ]
 
 _lib = None
@@ -61,7 +63,7 @@ def load():
     if _lib is not None:
         return _lib
     if not os.path.exists(LIB_PATH):
-        raise OSError("libncs_b200.so is not built; run `python -m ncs_b200.build`")
+        raise OSError("libncs_b200.so is not built; run `python ncs_b200/build.py`")
     lib = ctypes.CDLL(LIB_PATH)
     vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
     P = ctypes.POINTER
@@ -84,6 +86,10 @@ def load():
     lib.ncsb_reduce_noise.restype = ctypes.c_int
     lib.ncsb_solve_tiles.argtypes = [vp, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]
     lib.ncsb_solve_tiles.restype = ctypes.c_int
+    lib.ncsb_reduce_noise_noalloc.argtypes = [P(NcsbParams), P(ctypes.c_float), vp, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp,
+                                              vp, vp, vp, vp, vp]
+    lib.ncsb_reduce_noise_noalloc.restype = ctypes.c_int
     _lib = lib
     return lib
 

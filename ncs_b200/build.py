@@ -1,6 +1,8 @@
 """Build libncs_b200.so in-tree with nvcc for sm_100a (B200).
 
-Usage: ``python -m ncs_b200.build`` (also called by ``__graft_entry__.build``).
+Usage: ``python ncs_b200/build.py [--force] [-v]`` (also called by
+``__graft_entry__.build``).  Run it as a script: importing the package loads
+the library, which must exist first.
 The library is a plain C-ABI shared object (include/ncs_b200.h) loaded with
 ctypes; it links only the CUDA runtime.
 """
@@ -12,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libncs_b200.so")
-SOURCES = ["ncs_capi.cu", "ncs_plain.cu"]
+SOURCES = ["ncs_capi.cu", "ncs_plain.cu", "ncs_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

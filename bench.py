@@ -383,7 +383,7 @@ def run_ours(args, world, rank, local):
         "status": {str(k): int((st == k).sum()) for k in range(-5, 1) if (st == k).any()},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
-                     "kernel": "ncs_plain_kernel",
+                     "kernel": "ncs_warp_kernel" if args.form == "plain" else "ncs_plain_kernel",
                      "peak_source": "148 SMs x 128 FP32 lanes x 2 x %s sm_max_mhz (%s)"
                                     % (pk.get("sm_max_mhz"), pk_src),
                      "flops_per_launch": flops,

@@ -17,6 +17,7 @@ NCSB_ESIZE = -4
 NCSB_ESCRATCH = -5
 
 MODE_PLAIN = 0
+MODE_PLAIN_WG = 1
 
 # Per-tile status codes (cuda/ncs.cu:61-67).
 SUCCESS = 0

@@ -14,6 +14,8 @@
 namespace ncsb {
 cudaError_t launch_plain(const SolveArgs& args, int grid, cudaStream_t stream);
 int plain_max_ctas_per_sm();
+cudaError_t launch_warp_blocks(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
+int warp_max_ctas_per_sm(int m, int blocks);
 }  // namespace ncsb
 
 struct ncsb_handle {
@@ -45,7 +47,7 @@ int check_params(const ncsb_params* p, std::string* why) {
     if (!(p->epsilon >= 0.0)) { *why = "epsilon must be >= 0"; return NCSB_EINVAL; }
     if (!(p->c1 > 0.0 && p->c1 < 1.0)) { *why = "c1 must be in (0, 1)"; return NCSB_EINVAL; }
     if (!(p->min_step > 0.0)) { *why = "min_step must be > 0"; return NCSB_EINVAL; }
-    if (p->mode != NCSB_MODE_PLAIN) { *why = "unsupported mode"; return NCSB_EINVAL; }
+    if (p->mode != NCSB_MODE_PLAIN && p->mode != NCSB_MODE_PLAIN_WG) { *why = "unsupported mode"; return NCSB_EINVAL; }
     if (p->ctas_per_sm < 0) { *why = "ctas_per_sm must be >= 0"; return NCSB_EINVAL; }
     return NCSB_OK;
 }
@@ -62,8 +64,6 @@ int tiles_along(int n) {
     return count;
 }
 
-int bitrev4(int v) { return ((v & 1) << 3) | ((v & 2) << 1) | ((v & 4) >> 1) | ((v & 8) >> 3); }
-
 int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(h->d_queue, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemsetAsync(queue)");
@@ -75,11 +75,18 @@ int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s) {
     a.min_step = (float)h->p.min_step;
     a.max_iters = h->p.max_iters;
     a.m = h->p.m;
-    int per_sm = h->p.ctas_per_sm > 0 ? h->p.ctas_per_sm : ncsb::plain_max_ctas_per_sm();
+    const bool wg = h->p.mode == NCSB_MODE_PLAIN_WG;
+    int per_sm = h->p.ctas_per_sm > 0
+                     ? h->p.ctas_per_sm
+                     : (wg ? ncsb::plain_max_ctas_per_sm() : ncsb::warp_max_ctas_per_sm(a.m, 0));
+    // warp-per-tile CTAs hold 4 tiles at a time
+    const long long tiles_per_cta = wg ? 1 : 4;
     long long grid = (long long)per_sm * h->num_sms;
-    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid > (a.n_tiles + tiles_per_cta - 1) / tiles_per_cta)
+        grid = (a.n_tiles + tiles_per_cta - 1) / tiles_per_cta;
     if (grid < 1) grid = 1;
-    e = ncsb::launch_plain(a, (int)grid, s);
+    e = wg ? ncsb::launch_plain(a, (int)grid, s)
+           : ncsb::launch_warp_blocks(a, (int)grid, h->p.ctas_per_sm, s);
     if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
     return NCSB_OK;
 }
@@ -92,7 +99,7 @@ void ncsb_default_params(ncsb_params* p) {
     if (!p) return;
     p->alpha = 0.2;
     p->max_iters = 200;
-    p->m = 8;
+    p->m = 4;
     p->epsilon = 1e-5;
     p->c1 = 1e-4;
     p->min_step = 1e-6;
@@ -156,14 +163,11 @@ int ncsb_set_otf_mask(ncsb_handle* h, const float* mask) {
             if (!std::isfinite(a)) return fail(h, NCSB_EINVAL, "mask has a non-finite value");
             m2[i][j] = 0.5 * (a * a + b * b);
         }
-    // Kernel layout: thread t = g*16 + l owns spectral positions
-    // (bitrev(l), g) and (bitrev(l), g + 8), stored at [2t] and [2t + 1].
+    // Natural order [kr][kc], scaled by 1/256; each kernel permutes it into
+    // its own spectral layout when a CTA starts.
     float tab[256];
-    for (int t = 0; t < 128; ++t) {
-        const int g = t >> 4, l = t & 15, kr = bitrev4(l);
-        tab[2 * t] = (float)(m2[kr][g] / 256.0);
-        tab[2 * t + 1] = (float)(m2[kr][g + 8] / 256.0);
-    }
+    for (int i = 0; i < 16; ++i)
+        for (int j = 0; j < 16; ++j) tab[i * 16 + j] = (float)(m2[i][j] / 256.0);
     cudaError_t e = cudaMemcpy(h->d_msq, tab, sizeof(tab), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpy(mask)");
     h->has_mask = true;

@@ -44,7 +44,7 @@ struct SolveArgs {
     double* cost;                  // optional [N]
     int32_t* evals;                // optional [N]: 1 + line-search trials
     unsigned long long* queue;     // work counter, zero at launch
-    const float* msq;              // [256] M^2/256 in the kernel's spectral layout
+    const float* msq;              // [256] M^2/256, natural order [kr][kc], symmetrised
     float alpha, eps, c1, min_step;
     int max_iters, m;
 };
@@ -141,6 +141,23 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* red, int& buf)
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = (rb[k] + rb[K + k]) + (rb[2 * K + k] + rb[3 * K + k]);
     buf ^= 1;
+}
+
+// Warp-wide sums of 32 values at once: on return lane v holds the sum over
+// the warp of v[lane].  Each halving step exchanges half of the remaining
+// vector (16, 8, 4, 2, 1 values): 31 shuffles instead of 32 x 5.
+__device__ __forceinline__ float warp_transpose_sum32(float (&v)[32], int lane) {
+#pragma unroll
+    for (int h = 16; h >= 1; h >>= 1) {
+        const bool up = (lane & h) != 0;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            const float send = up ? v[i] : v[i + h];
+            const float keep = up ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+        }
+    }
+    return v[0];
 }
 
 __device__ __forceinline__ float block_sum_f(float v, float* red, int& buf) {

@@ -23,6 +23,8 @@
 namespace ncsb {
 cudaError_t launch_plain(const SolveArgs& args, int grid, cudaStream_t stream);
 int plain_max_ctas_per_sm();
+cudaError_t launch_warp(const SolveArgs& args, int grid, cudaStream_t stream);
+int warp_max_ctas_per_sm(int m);
 }  // namespace ncsb
 
 namespace {
@@ -84,12 +86,11 @@ int tiles_along(int n) {
     return count;
 }
 
-int bitrev4(int v) { return ((v & 1) << 3) | ((v & 2) << 1) | ((v & 4) >> 1) | ((v & 8) >> 3); }
-
 bool params_ok(const ncsb_params* p) {
     return p && std::isfinite(p->alpha) && p->alpha >= 0.0 && p->max_iters >= 0 && p->m >= 1 &&
            p->m <= ncsb::kMaxM && p->epsilon >= 0.0 && p->c1 > 0.0 && p->c1 < 1.0 &&
-           p->min_step > 0.0 && p->mode == NCSB_MODE_PLAIN && p->ctas_per_sm >= 0;
+           p->min_step > 0.0 && (p->mode == NCSB_MODE_PLAIN || p->mode == NCSB_MODE_PLAIN_WG) &&
+           p->ctas_per_sm >= 0;
 }
 
 }  // namespace
@@ -110,17 +111,15 @@ extern "C" int ncsb_reduce_noise_noalloc(const ncsb_params* p, const float* mask
     int rc = setup_current_device(&dev);
     if (rc != NCSB_OK) return rc;
 
-    // M^2 symmetrised over k -> -k, scaled by 1/256 and permuted to the
-    // kernel's spectral layout (the table ncsb_set_otf_mask builds).
+    // M^2 symmetrised over k -> -k and scaled by 1/256, natural order (the
+    // table ncsb_set_otf_mask builds).
     float table[ncsb::kPix];
-    for (int t = 0; t < 128; ++t) {
-        const int g = t >> 4, l = t & 15, kr = bitrev4(l);
-        for (int h = 0; h < 2; ++h) {
-            const int kc = g + 8 * h;
+    for (int kr = 0; kr < 16; ++kr) {
+        for (int kc = 0; kc < 16; ++kc) {
             const double a = mask_shifted_host[kr * 16 + kc];
             const double b = mask_shifted_host[((16 - kr) & 15) * 16 + ((16 - kc) & 15)];
             if (!std::isfinite(a) || !std::isfinite(b)) return NCSB_EINVAL;
-            table[2 * t + h] = (float)(0.5 * (a * a + b * b) / 256.0);
+            table[kr * 16 + kc] = (float)(0.5 * (a * a + b * b) / 256.0);
         }
     }
     cudaStream_t s = (cudaStream_t)stream;
@@ -156,9 +155,14 @@ extern "C" int ncsb_reduce_noise_noalloc(const ncsb_params* p, const float* mask
     a.min_step = (float)p->min_step;
     a.max_iters = p->max_iters;
     a.m = p->m;
-    const int per_sm = p->ctas_per_sm > 0 ? p->ctas_per_sm : dev->ctas_per_sm;
+    const bool wg = p->mode == NCSB_MODE_PLAIN_WG;
+    const int per_sm = p->ctas_per_sm > 0 ? p->ctas_per_sm
+                                          : (wg ? dev->ctas_per_sm : ncsb::warp_max_ctas_per_sm(a.m));
+    const long long tiles_per_cta = wg ? 1 : 4;
     long long grid = (long long)per_sm * dev->num_sms;
-    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid > (a.n_tiles + tiles_per_cta - 1) / tiles_per_cta)
+        grid = (a.n_tiles + tiles_per_cta - 1) / tiles_per_cta;
     if (grid < 1) grid = 1;
-    return ncsb::launch_plain(a, (int)grid, s) == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
+    const cudaError_t e = wg ? ncsb::launch_plain(a, (int)grid, s) : ncsb::launch_warp(a, (int)grid, s);
+    return e == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
 }

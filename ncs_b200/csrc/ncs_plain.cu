@@ -106,7 +106,9 @@ __global__ void __launch_bounds__(kThreads, 8) ncs_plain_kernel(const SolveArgs 
     const int tid = threadIdx.x;
     const int r = tid >> 4, c = tid & 15;
     const Twiddles tw = make_twiddles(c);
-    const float msq0 = a.msq[2 * tid], msq1 = a.msq[2 * tid + 1];
+    // M^2/256 at the spectral positions (bitrev(c), r) and (bitrev(c), r + 8)
+    // this thread owns in the column pass
+    const float msq0 = a.msq[bitrev4(c) * 16 + r], msq1 = a.msq[bitrev4(c) * 16 + r + 8];
     const float alpha = a.alpha;
     const int mcap = a.m < 1 ? 1 : (a.m > kMaxM ? kMaxM : a.m);
     int bufd = 0, buff = 0;

@@ -1,0 +1,737 @@
+// ncs_warp.cu -- the plain (FP32 SIMT) persistent NCS solver, one warp per
+// 16x16 tile.  This is the default form (NCSB_MODE_PLAIN).
+//
+// It minimises, per tile, the NCS cost
+//     f(u) = sum_i [u_i - c_i log(max(u_i + gamma_i, 1e-6))] + alpha u^T Q u,
+//     c_i = d_i + gamma_i,  Q = (1/256) F^H diag(M^2) F
+// (clib/pyCNCS/ncs.c:185-299, cuda/ncs.cu:635-817) by L-BFGS with up to 8
+// correction pairs and Armijo backtracking (ncs.cu:997-1087), with the
+// reference GPU kernel's stopping rules and status codes (ncs.cu:824-852,
+// :1097-1127, :61-67).  The algorithm is that of ncs_plain.cu (one Q
+// application per iteration, FP64 cost-difference Armijo test, fraction-to-
+// barrier rule); what changes is the mapping onto the machine:
+//
+//  * One warp owns a tile and each lane holds 8 pixels, so reductions are
+//    warp shuffles only -- no block barrier anywhere in the solve -- and most
+//    FFT butterflies are lane-local arithmetic.  A 128-thread CTA holds 4
+//    independent warps that pull tiles from the global atomic queue one at a
+//    time.  (The warp-group-per-tile kernel of ncs_plain.cu spends ~7,000
+//    warp instructions per tile-iteration, mostly in cross-thread traffic;
+//    measured and kept for comparison as NCSB_MODE_PLAIN_WG.)
+//  * Pixel layout: lane L holds rows P = L >> 2 and P + 8 at columns
+//    Qd + 4j (Qd = L & 3, j = 0..3), packed as the complex numbers
+//    x[P][c] + i x[P+8][c] -- two real rows per complex transform.
+//  * Q x by FFT: 16-point row transforms = lane-local radix-4 step, twiddle,
+//    and a 4-point transform across the 4 lanes of a row pair (two shuffle
+//    stages with trivial twiddles); one shared-memory transpose; column
+//    transforms with 2 lanes per column frequency (the two packed rows are
+//    separated lane-locally from X[k] and X[-k], the 16-point column DFT is
+//    split into even/odd 8-point DFTs, one per lane); multiply by M^2/256 in
+//    that spectral layout; the same steps inverted.
+//  * The search direction uses the compact L-BFGS representation (Byrd,
+//    Nocedal & Schnabel 1994): all dot products of the new gradient with the
+//    stored pairs in one 32-value transposed warp reduction, R and Y'Y from
+//    differences of consecutive dot products, the k x k triangular solves on
+//    lanes 0..k-1.  Same H g as the two-loop recursion of ncs.cu:1129-1198.
+//  * log1p in the line search: 2 atanh(x / (2 + x)) by its odd power series
+//    for |x| <= 1/2 (relative error ~1e-7 where the Armijo test needs it),
+//    the hardware log2 otherwise.
+#include "ncs_internal.cuh"
+
+namespace ncsb {
+
+namespace {
+
+constexpr int kWarps = 4;
+constexpr int kWarpCtaThreads = 32 * kWarps;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr float kS2 = 0.70710678118654752f;  // sqrt(1/2)
+
+// Per-warp shared memory (the history arrays follow it, sized by m).
+struct WarpSmem {
+    float2 fb[16][17];    // FFT transpose buffer
+    float R[kMaxM][kMaxM];   // s_i'y_j by slot (upper triangle in age order is used)
+    float YY[kMaxM][kMaxM];  // y_i'y_j by slot
+    float rinv[kMaxM];       // 1 / s_i'y_i by slot
+};
+
+constexpr size_t kTableBytes = 256 * sizeof(float);
+
+__host__ __device__ constexpr size_t warp_bytes(int m) {
+    return ((sizeof(WarpSmem) + 15) / 16) * 16 + 2 * (size_t)m * 32 * 2 * sizeof(float4);
+}
+
+__device__ __forceinline__ int bitrev3(int i) {
+    return ((i & 1) << 2) | (i & 2) | ((i & 4) >> 2);
+}
+
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 mul_i(float2 a) { return make_float2(-a.y, a.x); }      // i a
+__device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }     // -i a
+__device__ __forceinline__ float2 conjmul(float2 a, float2 w) {                            // a conj(w)
+    return make_float2(fmaf(a.x, w.x, a.y * w.y), fmaf(a.y, w.x, -a.x * w.y));
+}
+__device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
+    return make_float2(__shfl_xor_sync(kFull, v.x, m), __shfl_xor_sync(kFull, v.y, m));
+}
+
+// W16^p = exp(-2 pi i p / 16), p = 0..7
+__device__ __forceinline__ float2 w16(int p) {
+    const float c[8] = {1.0f, 0.92387953251128674f, kS2, 0.38268343236508978f,
+                        0.0f, -0.38268343236508978f, -kS2, -0.92387953251128674f};
+    const float s[8] = {0.0f, 0.38268343236508978f, kS2, 0.92387953251128674f,
+                        1.0f, 0.92387953251128674f, kS2, 0.38268343236508978f};
+    return make_float2(c[p], -s[p]);
+}
+
+// In-place 8-point DFT, decimation in frequency: natural order in, output
+// position i holds frequency bitrev3(i).  Unnormalised.
+__device__ __forceinline__ void fft8_fwd(float2 (&e)[8]) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const float2 a = e[r] + e[r + 4], b = e[r] - e[r + 4];
+        e[r] = a;
+        if (r == 0) e[r + 4] = b;
+        else if (r == 1) e[r + 4] = make_float2(kS2 * (b.x + b.y), kS2 * (b.y - b.x));
+        else if (r == 2) e[r + 4] = mul_mi(b);
+        else e[r + 4] = make_float2(kS2 * (b.y - b.x), -kS2 * (b.x + b.y));
+    }
+#pragma unroll
+    for (int base = 0; base < 8; base += 4) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const float2 a = e[base + r] + e[base + r + 2], b = e[base + r] - e[base + r + 2];
+            e[base + r] = a;
+            e[base + r + 2] = r == 0 ? b : mul_mi(b);
+        }
+    }
+#pragma unroll
+    for (int base = 0; base < 8; base += 2) {
+        const float2 a = e[base] + e[base + 1], b = e[base] - e[base + 1];
+        e[base] = a;
+        e[base + 1] = b;
+    }
+}
+
+// Inverse of fft8_fwd up to the factor 8: bit-reversed in, natural out,
+// conjugate twiddles (unnormalised inverse DFT).
+__device__ __forceinline__ void fft8_inv(float2 (&e)[8]) {
+#pragma unroll
+    for (int base = 0; base < 8; base += 2) {
+        const float2 a = e[base], b = e[base + 1];
+        e[base] = a + b;
+        e[base + 1] = a - b;
+    }
+#pragma unroll
+    for (int base = 0; base < 8; base += 4) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const float2 t = r == 0 ? e[base + r + 2] : mul_i(e[base + r + 2]);
+            const float2 a = e[base + r];
+            e[base + r] = a + t;
+            e[base + r + 2] = a - t;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const float2 b = e[r + 4];
+        float2 t;
+        if (r == 0) t = b;
+        else if (r == 1) t = make_float2(kS2 * (b.x - b.y), kS2 * (b.x + b.y));
+        else if (r == 2) t = mul_i(b);
+        else t = make_float2(-kS2 * (b.x + b.y), kS2 * (b.x - b.y));
+        const float2 a = e[r];
+        e[r] = a + t;
+        e[r + 4] = a - t;
+    }
+}
+
+struct LaneGeo {
+    int lane, P, Qd, KC, H, k0;
+    float2 tw1, tw2, tw3;  // W16^(Qd*k1), k1 = 1..3
+    float sA, sB, sH;      // butterfly signs of this lane
+};
+
+__device__ __forceinline__ LaneGeo lane_geo(int lane) {
+    LaneGeo g;
+    g.lane = lane;
+    g.P = lane >> 2;
+    g.Qd = lane & 3;
+    g.KC = lane >> 1;
+    g.H = lane & 1;
+    g.k0 = 4 * ((g.Qd & 1) * 2 + (g.Qd >> 1));  // 4 * bitrev2(Qd)
+    float sn, cs;
+    sincospif((float)(g.Qd * 1) / 8.0f, &sn, &cs);
+    g.tw1 = make_float2(cs, -sn);
+    sincospif((float)(g.Qd * 2) / 8.0f, &sn, &cs);
+    g.tw2 = make_float2(cs, -sn);
+    sincospif((float)(g.Qd * 3) / 8.0f, &sn, &cs);
+    g.tw3 = make_float2(cs, -sn);
+    g.sA = g.Qd < 2 ? 1.0f : -1.0f;
+    g.sB = (g.Qd & 1) ? -1.0f : 1.0f;
+    g.sH = g.H ? -1.0f : 1.0f;
+    return g;
+}
+
+// y = Q x for the 8 pixels of this lane (x[2j] = row P, x[2j+1] = row P+8,
+// column Qd + 4j).  mt = this lane's 8 mask values.  *nc_part (optional)
+// receives this lane's share of x^T Q x.
+__device__ __forceinline__ void warp_apply_q(const float (&x)[8], float (&y)[8], WarpSmem& ws,
+                                             const float* mt, const LaneGeo& L, float* nc_part) {
+    // ---- rows: 4-point DFT over j in the lane, twiddle, 4-point DFT across lanes
+    float2 V[4];
+    {
+        const float2 z0 = make_float2(x[0], x[1]), z1 = make_float2(x[2], x[3]);
+        const float2 z2 = make_float2(x[4], x[5]), z3 = make_float2(x[6], x[7]);
+        const float2 s02 = z0 + z2, d02 = z0 - z2, s13 = z1 + z3, d13 = z1 - z3;
+        V[0] = s02 + s13;
+        V[2] = cmul(s02 - s13, L.tw2);
+        V[1] = cmul(d02 + mul_mi(d13), L.tw1);
+        V[3] = cmul(d02 + mul_i(d13), L.tw3);
+    }
+    const bool q3 = L.Qd == 3;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 p = shfl_xor2(V[k], 2);
+        float2 t = make_float2(fmaf(L.sA, V[k].x, p.x), fmaf(L.sA, V[k].y, p.y));
+        V[k] = q3 ? mul_mi(t) : t;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 p = shfl_xor2(V[k], 1);
+        V[k] = make_float2(fmaf(L.sB, V[k].x, p.x), fmaf(L.sB, V[k].y, p.y));
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ws.fb[L.P][L.k0 + k] = V[k];
+    __syncwarp();
+
+    // ---- columns: lane (KC, H) separates the two packed rows of every row
+    // pair from X[KC] and X[-KC], forms the even (H = 0) or odd (H = 1) half of
+    // the 16-point column DFT and transforms it with an 8-point DFT.
+    float2 e[8];
+    const int kneg = (16 - L.KC) & 15;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const float2 Z = ws.fb[p][L.KC], Zm = ws.fb[p][kneg];
+        const float sx = Z.x + Zm.x, dx = Z.x - Zm.x, sy = Z.y + Zm.y, dy = Z.y - Zm.y;
+        float2 ev = make_float2(0.5f * fmaf(L.sH, sy, sx), 0.5f * fmaf(-L.sH, dx, dy));
+        const float2 w = w16(p);
+        e[p] = L.H ? cmul(ev, w) : ev;
+    }
+    fft8_fwd(e);
+    const float4 m0 = *reinterpret_cast<const float4*>(mt);
+    const float4 m1 = *reinterpret_cast<const float4*>(mt + 4);
+    const float mk[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+    if (nc_part) {
+        float s = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) s = fmaf(fmaf(e[i].x, e[i].x, e[i].y * e[i].y), mk[i], s);
+        *nc_part = s;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) e[i] = make_float2(e[i].x * mk[i], e[i].y * mk[i]);
+    fft8_inv(e);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const float2 w = w16(r);
+        e[r] = L.H ? conjmul(e[r], w) : e[r];
+    }
+    float2 out[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const float2 q = shfl_xor2(e[r], 1);
+        // H = 0: rows r = e + q ; H = 1: rows r + 8 = q - e
+        out[r] = make_float2(fmaf(L.sH, e[r].x, q.x), fmaf(L.sH, e[r].y, q.y));
+    }
+    __syncwarp();  // every lane has read the row spectra
+#pragma unroll
+    for (int r = 0; r < 8; ++r) ws.fb[r + 8 * L.H][L.KC] = out[r];
+    __syncwarp();
+
+    // ---- inverse rows: pack the two real output rows, inverse transforms
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 a = ws.fb[L.P][L.k0 + k], b = ws.fb[L.P + 8][L.k0 + k];
+        V[k] = make_float2(a.x - b.y, a.y + b.x);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 p = shfl_xor2(V[k], 1);
+        V[k] = make_float2(fmaf(L.sB, V[k].x, p.x), fmaf(L.sB, V[k].y, p.y));
+    }
+    const bool lower = L.Qd < 2, odd = (L.Qd & 1) != 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 p = shfl_xor2(V[k], 2);
+        const float2 src = lower ? p : V[k];
+        const float2 b = odd ? mul_i(src) : src;
+        const float2 other = lower ? V[k] : p;
+        V[k] = make_float2(fmaf(L.sA, b.x, other.x), fmaf(L.sA, b.y, other.y));
+    }
+    V[1] = conjmul(V[1], L.tw1);
+    V[2] = conjmul(V[2], L.tw2);
+    V[3] = conjmul(V[3], L.tw3);
+    {
+        const float2 s02 = V[0] + V[2], d02 = V[0] - V[2], s13 = V[1] + V[3], d13 = V[1] - V[3];
+        const float2 z0 = s02 + s13, z2 = s02 - s13;
+        const float2 z1 = d02 + mul_i(d13), z3 = d02 + mul_mi(d13);
+        y[0] = z0.x; y[1] = z0.y; y[2] = z1.x; y[3] = z1.y;
+        y[4] = z2.x; y[5] = z2.y; y[6] = z3.x; y[7] = z3.y;
+    }
+}
+
+// log1p(x) for x > -1: 2 atanh(y), y = x / (2 + x), by the odd series
+// 2y (1 + y^2/3 + ... + y^10/11) when |x| <= 1/2 (|y| <= 1/5, truncation
+// < 1e-9 relative); otherwise log(1 + x) from the hardware log2, whose
+// absolute error is small against |log(1 + x)| >= 0.4 there.
+__device__ __forceinline__ float log1p_ls(float x) {
+    const float y = __fdividef(x, 2.0f + x);
+    const float y2 = y * y;
+    float s = fmaf(y2, 1.0f / 11.0f, 1.0f / 9.0f);
+    s = fmaf(y2, s, 1.0f / 7.0f);
+    s = fmaf(y2, s, 1.0f / 5.0f);
+    s = fmaf(y2, s, 1.0f / 3.0f);
+    s = fmaf(y2, s, 1.0f);
+    const float small = 2.0f * y * s;
+    return fabsf(x) <= 0.5f ? small : __logf(1.0f + x);
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int tile_origin(int i, int n) {
+    const int o = 14 * i, last = n + 2 - kTile;
+    return o < last ? o : last;
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+__device__ __forceinline__ void load8(const float4* h, float (&x)[8]) {
+    const float4 a = h[0], b = h[1];
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+
+__device__ __forceinline__ void store8(float4* h, const float (&x)[8]) {
+    h[0] = make_float4(x[0], x[1], x[2], x[3]);
+    h[1] = make_float4(x[4], x[5], x[6], x[7]);
+}
+
+}  // namespace
+
+// MinBlocks CTAs per SM: the register budget (128 threads each) the
+// compiler must meet; the launcher picks the variant shared memory allows.
+template <int MinBlocks>
+__global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_warp_kernel(const SolveArgs a) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    const int mcap = a.m < 1 ? 1 : (a.m > kMaxM ? kMaxM : a.m);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float* mtab = reinterpret_cast<float*>(dsm);
+    unsigned char* wbase = dsm + kTableBytes + (size_t)wid * warp_bytes(mcap);
+    WarpSmem& ws = *reinterpret_cast<WarpSmem*>(wbase);
+    float4* hs = reinterpret_cast<float4*>(wbase + ((sizeof(WarpSmem) + 15) / 16) * 16);
+    float4* hy = hs + (size_t)mcap * 64;
+
+    // Mask table in the column-pass layout: lane (KC, H), entry i holds
+    // M^2/256 at row frequency 2 bitrev3(i) + H, column frequency KC.
+    for (int idx = threadIdx.x; idx < 256; idx += blockDim.x) {
+        const int L = idx >> 3, i = idx & 7;
+        mtab[idx] = a.msq[(2 * bitrev3(i) + (L & 1)) * 16 + (L >> 1)];
+    }
+    __syncthreads();
+    const float* mt = mtab + lane * 8;
+    const LaneGeo G = lane_geo(lane);
+    const float alpha = a.alpha, two_alpha = 2.0f * a.alpha;
+
+    for (;;) {
+        unsigned long long tk = 0;
+        if (lane == 0) tk = atomicAdd(a.queue, 1ull);
+        const long long tile = (long long)__shfl_sync(kFull, tk, 0);
+        if (tile >= a.n_tiles) break;
+
+        // ---- gather the tile (segmentation, ncs.c:66-113) ---------------------
+        float d[8], gm[8], u[8];
+        int f = 0, ox = 0, oy = 0, own_r = 0, own_c = 0;
+        if (a.tile_mode) {
+            const long long base = tile * kPix;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int off = (G.P + 8 * s) * kTile + G.Qd + 4 * j;
+                    d[2 * j + s] = __ldg(a.data + base + off);
+                    gm[2 * j + s] = __ldg(a.gamma + base + off);
+                    u[2 * j + s] = a.u0 ? __ldg(a.u0 + base + off) : d[2 * j + s];
+                }
+        } else {
+            const long long per_frame = (long long)a.tiles_x * a.tiles_y;
+            f = (int)(tile / per_frame);
+            const int rem = (int)(tile - (long long)f * per_frame);
+            const int ti = rem / a.tiles_y, tj = rem - (rem / a.tiles_y) * a.tiles_y;
+            ox = tile_origin(ti, a.H);
+            oy = tile_origin(tj, a.W);
+            own_r = (ti + 1 < a.tiles_x ? tile_origin(ti + 1, a.H) : ox + 14) - ox;
+            own_c = (tj + 1 < a.tiles_y ? tile_origin(tj + 1, a.W) : oy + 14) - oy;
+            const float* img = a.data + (long long)f * a.H * a.W;
+            const float* gmap = a.gamma + (long long)f * a.gamma_frame_stride;
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const long long row = clampi(ox + G.P + 8 * s - 1, 0, a.H - 1);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int col = clampi(oy + G.Qd + 4 * j - 1, 0, a.W - 1);
+                    d[2 * j + s] = __ldg(img + row * a.W + col);
+                    gm[2 * j + s] = __ldg(gmap + row * a.W + col);
+                    u[2 * j + s] = d[2 * j + s];
+                }
+            }
+        }
+        float c[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) c[i] = d[i] + gm[i];
+
+        // ---- initial point ----------------------------------------------------
+        float v[8], g[8];
+        warp_apply_q(u, v, ws, mt, G, nullptr);
+        float uu = 0.0f, gg = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            g[i] = 1.0f - __fdividef(c[i], fmaxf(u[i] + gm[i], kFitMin)) + two_alpha * v[i];
+            uu = fmaf(u[i], u[i], uu);
+            gg = fmaf(g[i], g[i], gg);
+        }
+        uu = warp_sum_f(uu);
+        gg = warp_sum_f(gg);
+        int status = kUnstarted, iters = 0, evals = 1;
+        if (sqrtf(gg) <= a.eps * fmaxf(sqrtf(uu), 1.0f)) status = kSuccess;
+        float p[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) p[i] = -g[i];
+        float step = rsqrtf(gg);  // first step 1/||g|| (ncs.cu:980-984)
+        int k = 0, head = 0;
+        float theta = 1.0f, aold = 0.0f, bold = 0.0f;
+
+        while (status == kUnstarted) {
+            if (iters >= a.max_iters) { status = kReachedMaxIters; break; }
+            float w[8];
+            warp_apply_q(p, w, ws, mt, G, nullptr);
+            float gp = 0.0f, pv = 0.0f, pw = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                gp = fmaf(g[i], p[i], gp);
+                pv = fmaf(p[i], v[i], pv);
+                pw = fmaf(p[i], w[i], pw);
+            }
+            const double gd = warp_sum_d((double)gp);
+            const double dpv = warp_sum_d((double)pv), dpw = warp_sum_d((double)pw);
+            if (gd > 0.0) { status = kIncreasingGradient; break; }
+
+            // Armijo backtracking on the exact cost difference, FP64 across lanes
+            float t = step;
+            bool ok = false;
+            for (int trial = 0; trial < 64; ++trial) {
+                float term = 0.0f;
+                bool cross = false;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float ai = u[i] + gm[i];
+                    const float tp = t * p[i];
+                    const float ni = ai + tp;
+                    float l;
+                    if (ai >= kFitMin && ni >= kFitMin) l = log1p_ls(__fdividef(tp, ai));
+                    else l = __logf(fmaxf(ni, kFitMin)) - __logf(fmaxf(ai, kFitMin));
+                    cross |= (ai >= kFitMin) && (ni < kBarrierFrac * ai);
+                    term += fmaf(-c[i], l, tp);
+                }
+                // fraction to the log barrier (see ncs_plain.cu): infeasible trial
+                const bool any_cross = __any_sync(kFull, cross);
+                const double dl = warp_sum_d((double)term);
+                ++evals;
+                const double td = (double)t;
+                const double delta = any_cross ? CUDART_INF
+                                               : dl + (double)alpha * (2.0 * td * dpv + td * td * dpw);
+                if (delta <= (double)a.c1 * td * gd) { ok = true; break; }
+                t *= 0.5f;
+                if (!(t >= a.min_step)) break;  // also stops on NaN
+            }
+            if (!ok) { status = kMinimumStep; break; }
+
+            // Accept the step; pair s = u_new - u, y = g_new - g.
+            float s[8], y[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float un = fmaf(t, p[i], u[i]);
+                v[i] = fmaf(t, w[i], v[i]);
+                const float gn = 1.0f - __fdividef(c[i], fmaxf(un + gm[i], kFitMin)) + two_alpha * v[i];
+                s[i] = un - u[i];
+                y[i] = gn - g[i];
+                u[i] = un;
+                g[i] = gn;
+            }
+            // One transposed reduction: [0,8) s_x'g, [8,16) y_x'g for stored slots,
+            // 16 s'g, 17 y'g, 18 s'y, 19 y'y of the new pair, 20 ||u||^2,
+            // 21 ||g||^2, 22 pixels moved.
+            float vals[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) vals[i] = 0.0f;
+#pragma unroll
+            for (int x = 0; x < kMaxM; ++x) {
+                if (x < k) {
+                    float hv[8];
+                    load8(hs + x * 64 + lane * 2, hv);
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc = fmaf(hv[i], g[i], acc);
+                    vals[x] = acc;
+                    load8(hy + x * 64 + lane * 2, hv);
+                    acc = 0.0f;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc = fmaf(hv[i], g[i], acc);
+                    vals[8 + x] = acc;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                vals[16] = fmaf(s[i], g[i], vals[16]);
+                vals[17] = fmaf(y[i], g[i], vals[17]);
+                vals[18] = fmaf(s[i], y[i], vals[18]);
+                vals[19] = fmaf(y[i], y[i], vals[19]);
+                vals[20] = fmaf(u[i], u[i], vals[20]);
+                vals[21] = fmaf(g[i], g[i], vals[21]);
+                vals[22] += (s[i] != 0.0f) ? 1.0f : 0.0f;
+            }
+            const float tot = warp_transpose_sum32(vals, lane);  // lane v: total of value v
+            const float T16 = __shfl_sync(kFull, tot, 16), T17 = __shfl_sync(kFull, tot, 17);
+            const float sy = __shfl_sync(kFull, tot, 18), yy = __shfl_sync(kFull, tot, 19);
+            const float un2 = __shfl_sync(kFull, tot, 20), gn2 = __shfl_sync(kFull, tot, 21);
+            const float moved = __shfl_sync(kFull, tot, 22);
+            const float bnew = __shfl_sync(kFull, tot, 8 + (lane & 7));
+            ++iters;
+            if (sqrtf(gn2) <= a.eps * fmaxf(sqrtf(un2), 1.0f)) { status = kSuccess; break; }
+            if (moved == 0.0f) { status = kReachedMaxPrecision; break; }
+
+            // R_xq = s_x'y_new, (Y'Y)_xq = y_x'y_new from consecutive dot products
+            {
+                const float rx = tot - aold, tx = bnew - bold;
+                aold = tot;  // lanes 0..7: s_x'g of slot x
+                bold = bnew;
+                if (sy > 0.0f && yy > 0.0f) {
+                    const int q = k < mcap ? k : head;  // fresh slot, or evict the oldest
+                    store8(hs + q * 64 + lane * 2, s);
+                    store8(hy + q * 64 + lane * 2, y);
+                    if (lane < k && lane != q) {
+                        ws.R[lane][q] = rx;
+                        ws.YY[lane][q] = tx;
+                        ws.YY[q][lane] = tx;
+                    }
+                    if (lane == q) {
+                        ws.R[q][q] = sy;
+                        ws.rinv[q] = 1.0f / sy;
+                        ws.YY[q][q] = yy;
+                        aold = T16;
+                        bold = T17;
+                    }
+                    if (k < mcap) ++k;
+                    else head = head + 1 == mcap ? 0 : head + 1;
+                    theta = sy / yy;
+                }
+            }
+            __syncwarp();
+
+            // p = -H g, compact form: H g = theta g + S p1 - theta Y z with
+            // z = R^-1 S'g, p1 = R^-T ((D + theta Y'Y) z - theta Y'g); lane j = age j.
+            const int j = lane;
+            int sj = head + (j & (kMaxM - 1));
+            if (sj >= mcap) sj -= mcap;
+            const float a_slot = __shfl_sync(kFull, aold, sj);
+            const float b_slot = __shfl_sync(kFull, bold, sj);
+            float zj = 0.0f, p1j = 0.0f, aj = 0.0f, bj = 0.0f;
+            if (k > 0) {
+                const bool mine = j < k;
+                aj = mine ? a_slot : 0.0f;
+                bj = mine ? b_slot : 0.0f;
+                const float rinv_j = mine ? ws.rinv[sj] : 0.0f;
+                float acc = aj;
+#pragma unroll
+                for (int l = kMaxM - 1; l >= 0; --l) {
+                    if (l < k) {
+                        const float zl = __shfl_sync(kFull, acc * rinv_j, l);
+                        int sl = head + l;
+                        if (sl >= mcap) sl -= mcap;
+                        if (j == l) zj = zl;
+                        if (j < l) acc = fmaf(-ws.R[sj][sl], zl, acc);
+                    }
+                }
+                float wsum = 0.0f;
+#pragma unroll
+                for (int l = 0; l < kMaxM; ++l) {
+                    if (l < k) {
+                        const float zl = __shfl_sync(kFull, zj, l);
+                        int sl = head + l;
+                        if (sl >= mcap) sl -= mcap;
+                        if (mine) wsum = fmaf(ws.YY[sj][sl], zl, wsum);
+                    }
+                }
+                acc = mine ? fmaf(ws.R[sj][sj], zj, theta * (wsum - bj)) : 0.0f;
+#pragma unroll
+                for (int l = 0; l < kMaxM; ++l) {
+                    if (l < k) {
+                        const float pl = __shfl_sync(kFull, acc * rinv_j, l);
+                        int sl = head + l;
+                        if (sl >= mcap) sl -= mcap;
+                        if (j == l) p1j = pl;
+                        if (j > l && mine) acc = fmaf(-ws.R[sl][sj], pl, acc);
+                    }
+                }
+            }
+            // g'p from the small quantities; a non-descent direction (rounding)
+            // restarts from steepest descent instead of failing
+            const float gdl = warp_sum_f(j < k ? fmaf(-p1j, aj, theta * zj * bj) : 0.0f);
+            if (k > 0 && !(fmaf(-theta, gn2, gdl) < 0.0f)) {
+                k = 0;
+                head = 0;
+                theta = 1.0f;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) p[i] = -theta * g[i];
+#pragma unroll
+            for (int l = 0; l < kMaxM; ++l) {
+                if (l < k) {
+                    const float cs = __shfl_sync(kFull, -p1j, l);
+                    const float cy = __shfl_sync(kFull, theta * zj, l);
+                    int sl = head + l;
+                    if (sl >= mcap) sl -= mcap;
+                    float hv[8];
+                    load8(hs + sl * 64 + lane * 2, hv);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) p[i] = fmaf(cs, hv[i], p[i]);
+                    load8(hy + sl * 64 + lane * 2, hv);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) p[i] = fmaf(cy, hv[i], p[i]);
+                }
+            }
+            step = k > 0 ? 1.0f : rsqrtf(gn2);
+        }
+
+        // ---- outputs -----------------------------------------------------------
+        if (a.cost) {
+            double e0 = 0.0, e1 = 0.0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                e0 += (double)u[i] - (double)c[i] * log(fmax((double)u[i] + gm[i], 1.0e-6));
+                e1 += (double)u[i] * v[i];
+            }
+            e0 = warp_sum_d(e0);
+            e1 = warp_sum_d(e1);
+            if (lane == 0) a.cost[tile] = e0 + (double)alpha * e1;
+        }
+        if (lane == 0) {
+            if (a.iters) a.iters[tile] = iters;
+            if (a.status) a.status[tile] = status;
+            if (a.evals) a.evals[tile] = evals;
+        }
+        if (a.tile_mode) {
+            const long long base = tile * kPix;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                    a.out[base + (G.P + 8 * s) * kTile + G.Qd + 4 * j] = u[2 * j + s];
+        } else {
+            float* o = a.out + (long long)f * a.H * a.W;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int cc = G.Qd + 4 * j;
+                if (cc < 1 || cc > own_c) continue;
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int rr = G.P + 8 * s;
+                    if (rr >= 1 && rr <= own_r)
+                        o[(long long)(ox + rr - 1) * a.W + oy + cc - 1] = u[2 * j + s];
+                }
+            }
+        }
+    }
+}
+
+size_t warp_smem_bytes(int m) {
+    const int mc = m < 1 ? 1 : (m > kMaxM ? kMaxM : m);
+    return kTableBytes + (size_t)kWarps * warp_bytes(mc);
+}
+
+namespace {
+
+using KernelFn = void (*)(SolveArgs);
+
+KernelFn warp_variant(int blocks) {
+    switch (blocks <= 3 ? 3 : (blocks >= 6 ? 6 : blocks)) {
+        case 3: return ncs_warp_kernel<3>;
+        case 4: return ncs_warp_kernel<4>;
+        case 5: return ncs_warp_kernel<5>;
+        default: return ncs_warp_kernel<6>;
+    }
+}
+
+// CTAs per SM that shared memory allows for history size m.
+int blocks_by_smem(int m) {
+    int dev = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+        cudaSuccess)
+        per_sm = 228 * 1024;
+    const size_t need = warp_smem_bytes(m) + 1024;  // + per-CTA reservation
+    return (int)(per_sm / need);
+}
+
+}  // namespace
+
+// Default variant: as many CTAs as shared memory allows, at most 4 -- the
+// 5- and 6-CTA register budgets (96 / 80) spill and measured slower.
+int default_blocks(int m) {
+    const int b = blocks_by_smem(m);
+    return b < 4 ? b : 4;
+}
+
+// Launch with `blocks` CTAs per SM in mind (0 = default_blocks).
+cudaError_t launch_warp_blocks(const SolveArgs& args, int grid, int blocks, cudaStream_t stream) {
+    const size_t smem = warp_smem_bytes(args.m);
+    const KernelFn fn = warp_variant(blocks > 0 ? blocks : default_blocks(args.m));
+    cudaError_t e =
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    fn<<<grid, kWarpCtaThreads, smem, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_warp(const SolveArgs& args, int grid, cudaStream_t stream) {
+    return launch_warp_blocks(args, grid, 0, stream);
+}
+
+// Resident CTAs per SM of the variant launch_warp_blocks(.., blocks) uses.
+int warp_max_ctas_per_sm(int m, int blocks) {
+    const size_t smem = warp_smem_bytes(m);
+    const KernelFn fn = warp_variant(blocks > 0 ? blocks : default_blocks(m));
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kWarpCtaThreads, smem) != cudaSuccess)
+        return 1;
+    return n > 0 ? n : 1;
+}
+
+int warp_max_ctas_per_sm(int m) { return warp_max_ctas_per_sm(m, 0); }
+
+}  // namespace ncsb

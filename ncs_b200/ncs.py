@@ -40,7 +40,7 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
 
 
-_MODES = {"plain": _lib.MODE_PLAIN}
+_MODES = {"plain": _lib.MODE_PLAIN, "plain_wg": _lib.MODE_PLAIN_WG}
 
 
 class Solver:
@@ -53,7 +53,7 @@ class Solver:
     the reference kernel's 1e-4.
     """
 
-    def __init__(self, alpha=0.2, max_iters=200, m=8, epsilon=1e-5, c1=1e-4, min_step=1e-6,
+    def __init__(self, alpha=0.2, max_iters=200, m=4, epsilon=1e-5, c1=1e-4, min_step=1e-6,
                  mode="plain", ctas_per_sm=0, device=None):
         self.lib = _lib.load()
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None

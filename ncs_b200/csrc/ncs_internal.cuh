@@ -160,6 +160,25 @@ __device__ __forceinline__ float warp_transpose_sum32(float (&v)[32], int lane) 
     return v[0];
 }
 
+// Same for N = 16 or 32 values: lane v ends with the warp total of value
+// v & (N - 1) (the two half-warps are combined last when N = 16).
+template <int N>
+__device__ __forceinline__ float warp_transpose_sum(float (&v)[N], int lane) {
+    static_assert(N == 16 || N == 32, "16 or 32 values");
+#pragma unroll
+    for (int h = N / 2; h >= 1; h >>= 1) {
+        const bool up = (lane & h) != 0;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            const float send = up ? v[i] : v[i + h];
+            const float keep = up ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+        }
+    }
+    if (N == 16) v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
+    return v[0];
+}
+
 __device__ __forceinline__ float block_sum_f(float v, float* red, int& buf) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

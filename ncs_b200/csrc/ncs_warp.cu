@@ -333,10 +333,15 @@ __device__ __forceinline__ void store8(float4* h, const float (&x)[8]) {
 
 // MinBlocks CTAs per SM: the register budget (128 threads each) the
 // compiler must meet; the launcher picks the variant shared memory allows.
-template <int MinBlocks>
+// MaxM: compiled history capacity (m <= MaxM); a capacity of 4 halves the
+// unrolled history loops and the transposed reduction of the default m = 4.
+template <int MinBlocks, int MaxM>
 __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_warp_kernel(const SolveArgs a) {
+    static_assert(MaxM == 4 || MaxM == 8, "history capacity");
+    constexpr int NV = (2 * MaxM + 7 <= 16) ? 16 : 32;  // values in the transposed reduction
+    constexpr int IA = 0, IB = MaxM, IN = 2 * MaxM;     // slot dots, then the new pair's
     extern __shared__ __align__(16) unsigned char dsm[];
-    const int mcap = a.m < 1 ? 1 : (a.m > kMaxM ? kMaxM : a.m);
+    const int mcap = a.m < 1 ? 1 : (a.m > MaxM ? MaxM : a.m);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* mtab = reinterpret_cast<float*>(dsm);
     unsigned char* wbase = dsm + kTableBytes + (size_t)wid * warp_bytes(mcap);
@@ -402,31 +407,43 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_warp_kernel(co
 #pragma unroll
         for (int i = 0; i < 8; ++i) c[i] = d[i] + gm[i];
 
-        // ---- initial point ----------------------------------------------------
-        float v[8], g[8];
-        warp_apply_q(u, v, ws, mt, G, nullptr);
-        float uu = 0.0f, gg = 0.0f;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            g[i] = 1.0f - __fdividef(c[i], fmaxf(u[i] + gm[i], kFitMin)) + two_alpha * v[i];
-            uu = fmaf(u[i], u[i], uu);
-            gg = fmaf(g[i], g[i], gg);
-        }
-        uu = warp_sum_f(uu);
-        gg = warp_sum_f(gg);
+        // ---- L-BFGS --------------------------------------------------------------
+        // The first pass of the loop applies Q to u (v = Qu, initial gradient);
+        // later passes apply it to the direction.  One call site keeps the FFT
+        // code once in the instruction stream.
+        float v[8], g[8], p[8];
         int status = kUnstarted, iters = 0, evals = 1;
-        if (sqrtf(gg) <= a.eps * fmaxf(sqrtf(uu), 1.0f)) status = kSuccess;
-        float p[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) p[i] = -g[i];
-        float step = rsqrtf(gg);  // first step 1/||g|| (ncs.cu:980-984)
+        bool first = true;
+        float step = 0.0f;
         int k = 0, head = 0;
         float theta = 1.0f, aold = 0.0f, bold = 0.0f;
 
-        while (status == kUnstarted) {
-            if (iters >= a.max_iters) { status = kReachedMaxIters; break; }
+        for (;;) {
+            if (!first && iters >= a.max_iters) { status = kReachedMaxIters; break; }
             float w[8];
-            warp_apply_q(p, w, ws, mt, G, nullptr);
+            {
+                float xq[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) xq[i] = first ? u[i] : p[i];
+                warp_apply_q(xq, w, ws, mt, G, nullptr);
+            }
+            if (first) {
+                first = false;
+                float uu = 0.0f, gg = 0.0f;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    v[i] = w[i];
+                    g[i] = 1.0f - __fdividef(c[i], fmaxf(u[i] + gm[i], kFitMin)) + two_alpha * v[i];
+                    uu = fmaf(u[i], u[i], uu);
+                    gg = fmaf(g[i], g[i], gg);
+                    p[i] = -g[i];
+                }
+                uu = warp_sum_f(uu);
+                gg = warp_sum_f(gg);
+                if (sqrtf(gg) <= a.eps * fmaxf(sqrtf(uu), 1.0f)) { status = kSuccess; break; }
+                step = rsqrtf(gg);  // first step 1/||g|| (ncs.cu:980-984)
+                continue;
+            }
             float gp = 0.0f, pv = 0.0f, pw = 0.0f;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
@@ -480,44 +497,43 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_warp_kernel(co
                 u[i] = un;
                 g[i] = gn;
             }
-            // One transposed reduction: [0,8) s_x'g, [8,16) y_x'g for stored slots,
-            // 16 s'g, 17 y'g, 18 s'y, 19 y'y of the new pair, 20 ||u||^2,
-            // 21 ||g||^2, 22 pixels moved.
-            float vals[32];
+            // One transposed reduction: s_x'g and y_x'g for the stored slots x, then
+            // for the new pair s'g, y'g, s'y, y'y, and ||u||^2, ||g||^2, pixels moved.
+            float vals[NV];
 #pragma unroll
-            for (int i = 0; i < 32; ++i) vals[i] = 0.0f;
+            for (int i = 0; i < NV; ++i) vals[i] = 0.0f;
 #pragma unroll
-            for (int x = 0; x < kMaxM; ++x) {
+            for (int x = 0; x < MaxM; ++x) {
                 if (x < k) {
                     float hv[8];
                     load8(hs + x * 64 + lane * 2, hv);
                     float acc = 0.0f;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) acc = fmaf(hv[i], g[i], acc);
-                    vals[x] = acc;
+                    vals[IA + x] = acc;
                     load8(hy + x * 64 + lane * 2, hv);
                     acc = 0.0f;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) acc = fmaf(hv[i], g[i], acc);
-                    vals[8 + x] = acc;
+                    vals[IB + x] = acc;
                 }
             }
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                vals[16] = fmaf(s[i], g[i], vals[16]);
-                vals[17] = fmaf(y[i], g[i], vals[17]);
-                vals[18] = fmaf(s[i], y[i], vals[18]);
-                vals[19] = fmaf(y[i], y[i], vals[19]);
-                vals[20] = fmaf(u[i], u[i], vals[20]);
-                vals[21] = fmaf(g[i], g[i], vals[21]);
-                vals[22] += (s[i] != 0.0f) ? 1.0f : 0.0f;
+                vals[IN + 0] = fmaf(s[i], g[i], vals[IN + 0]);
+                vals[IN + 1] = fmaf(y[i], g[i], vals[IN + 1]);
+                vals[IN + 2] = fmaf(s[i], y[i], vals[IN + 2]);
+                vals[IN + 3] = fmaf(y[i], y[i], vals[IN + 3]);
+                vals[IN + 4] = fmaf(u[i], u[i], vals[IN + 4]);
+                vals[IN + 5] = fmaf(g[i], g[i], vals[IN + 5]);
+                vals[IN + 6] += (s[i] != 0.0f) ? 1.0f : 0.0f;
             }
-            const float tot = warp_transpose_sum32(vals, lane);  // lane v: total of value v
-            const float T16 = __shfl_sync(kFull, tot, 16), T17 = __shfl_sync(kFull, tot, 17);
-            const float sy = __shfl_sync(kFull, tot, 18), yy = __shfl_sync(kFull, tot, 19);
-            const float un2 = __shfl_sync(kFull, tot, 20), gn2 = __shfl_sync(kFull, tot, 21);
-            const float moved = __shfl_sync(kFull, tot, 22);
-            const float bnew = __shfl_sync(kFull, tot, 8 + (lane & 7));
+            const float tot = warp_transpose_sum<NV>(vals, lane);  // lane v: total of value v
+            const float T16 = __shfl_sync(kFull, tot, IN + 0), T17 = __shfl_sync(kFull, tot, IN + 1);
+            const float sy = __shfl_sync(kFull, tot, IN + 2), yy = __shfl_sync(kFull, tot, IN + 3);
+            const float un2 = __shfl_sync(kFull, tot, IN + 4), gn2 = __shfl_sync(kFull, tot, IN + 5);
+            const float moved = __shfl_sync(kFull, tot, IN + 6);
+            const float bnew = __shfl_sync(kFull, tot, IB + (lane & (MaxM - 1)));
             ++iters;
             if (sqrtf(gn2) <= a.eps * fmaxf(sqrtf(un2), 1.0f)) { status = kSuccess; break; }
             if (moved == 0.0f) { status = kReachedMaxPrecision; break; }
@@ -553,7 +569,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_warp_kernel(co
             // p = -H g, compact form: H g = theta g + S p1 - theta Y z with
             // z = R^-1 S'g, p1 = R^-T ((D + theta Y'Y) z - theta Y'g); lane j = age j.
             const int j = lane;
-            int sj = head + (j & (kMaxM - 1));
+            int sj = head + (j & (MaxM - 1));
             if (sj >= mcap) sj -= mcap;
             const float a_slot = __shfl_sync(kFull, aold, sj);
             const float b_slot = __shfl_sync(kFull, bold, sj);
@@ -565,7 +581,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_warp_kernel(co
                 const float rinv_j = mine ? ws.rinv[sj] : 0.0f;
                 float acc = aj;
 #pragma unroll
-                for (int l = kMaxM - 1; l >= 0; --l) {
+                for (int l = MaxM - 1; l >= 0; --l) {
                     if (l < k) {
                         const float zl = __shfl_sync(kFull, acc * rinv_j, l);
                         int sl = head + l;
@@ -576,7 +592,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_warp_kernel(co
                 }
                 float wsum = 0.0f;
 #pragma unroll
-                for (int l = 0; l < kMaxM; ++l) {
+                for (int l = 0; l < MaxM; ++l) {
                     if (l < k) {
                         const float zl = __shfl_sync(kFull, zj, l);
                         int sl = head + l;
@@ -586,7 +602,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_warp_kernel(co
                 }
                 acc = mine ? fmaf(ws.R[sj][sj], zj, theta * (wsum - bj)) : 0.0f;
 #pragma unroll
-                for (int l = 0; l < kMaxM; ++l) {
+                for (int l = 0; l < MaxM; ++l) {
                     if (l < k) {
                         const float pl = __shfl_sync(kFull, acc * rinv_j, l);
                         int sl = head + l;
@@ -607,7 +623,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_warp_kernel(co
 #pragma unroll
             for (int i = 0; i < 8; ++i) p[i] = -theta * g[i];
 #pragma unroll
-            for (int l = 0; l < kMaxM; ++l) {
+            for (int l = 0; l < MaxM; ++l) {
                 if (l < k) {
                     const float cs = __shfl_sync(kFull, -p1j, l);
                     const float cy = __shfl_sync(kFull, theta * zj, l);
@@ -675,13 +691,18 @@ namespace {
 
 using KernelFn = void (*)(SolveArgs);
 
-KernelFn warp_variant(int blocks) {
+template <int MaxM>
+KernelFn warp_variant_m(int blocks) {
     switch (blocks <= 3 ? 3 : (blocks >= 6 ? 6 : blocks)) {
-        case 3: return ncs_warp_kernel<3>;
-        case 4: return ncs_warp_kernel<4>;
-        case 5: return ncs_warp_kernel<5>;
-        default: return ncs_warp_kernel<6>;
+        case 3: return ncs_warp_kernel<3, MaxM>;
+        case 4: return ncs_warp_kernel<4, MaxM>;
+        case 5: return ncs_warp_kernel<5, MaxM>;
+        default: return ncs_warp_kernel<6, MaxM>;
     }
+}
+
+KernelFn warp_variant(int blocks, int m) {
+    return m <= 4 ? warp_variant_m<4>(blocks) : warp_variant_m<8>(blocks);
 }
 
 // CTAs per SM that shared memory allows for history size m.
@@ -707,7 +728,7 @@ int default_blocks(int m) {
 // Launch with `blocks` CTAs per SM in mind (0 = default_blocks).
 cudaError_t launch_warp_blocks(const SolveArgs& args, int grid, int blocks, cudaStream_t stream) {
     const size_t smem = warp_smem_bytes(args.m);
-    const KernelFn fn = warp_variant(blocks > 0 ? blocks : default_blocks(args.m));
+    const KernelFn fn = warp_variant(blocks > 0 ? blocks : default_blocks(args.m), args.m);
     cudaError_t e =
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -722,7 +743,7 @@ cudaError_t launch_warp(const SolveArgs& args, int grid, cudaStream_t stream) {
 // Resident CTAs per SM of the variant launch_warp_blocks(.., blocks) uses.
 int warp_max_ctas_per_sm(int m, int blocks) {
     const size_t smem = warp_smem_bytes(m);
-    const KernelFn fn = warp_variant(blocks > 0 ? blocks : default_blocks(m));
+    const KernelFn fn = warp_variant(blocks > 0 ? blocks : default_blocks(m), m);
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return 1;

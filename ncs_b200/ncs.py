@@ -152,6 +152,79 @@ class Solver:
             return out, iters, status, cost
         return out
 
+    def reduce_noise_host(self, images, gamma, out=None, chunk_frames=None, n_streams=3):
+        """Host stack in, host stack out, with the copies hidden behind the solve.
+
+        ``images`` [T, H, W] and ``gamma`` [H, W] or [T, H, W] are float32 CPU
+        tensors (pinned memory lets the copies run asynchronously; numpy arrays
+        are accepted and pinned here).  The frames are cut into chunks; chunk i
+        is copied in, solved and copied out on stream i % n_streams, each
+        stream with its own solver handle (its own work counter), so one
+        chunk's host-device copies overlap another chunk's solve.  Returns the
+        pinned [T, H, W] result after all streams finish."""
+        def pinned(x):
+            t = x if isinstance(x, torch.Tensor) else torch.from_numpy(numpy.asarray(x))
+            if t.dtype != torch.float32:
+                t = t.float()
+            t = t.contiguous()
+            return t if t.is_pinned() else t.pin_memory()
+        h_in = pinned(images)
+        if h_in.dim() == 2:
+            h_in = h_in.unsqueeze(0)
+        T, H, W = h_in.shape
+        h_g = pinned(gamma)
+        per_frame = h_g.dim() == 3
+        if out is None:
+            out = torch.empty((T, H, W), dtype=torch.float32).pin_memory()
+        if T == 0:
+            return out
+        if chunk_frames is None:
+            chunk_frames = max(1, -(-T // 8))
+        chunk_frames = max(1, min(int(chunk_frames), T))
+        n_streams = max(1, int(n_streams))
+        pipe = getattr(self, "_pipe", None)
+        if pipe is None or len(pipe) != n_streams:
+            pipe = [Solver(device=self.device) for _ in range(n_streams)]
+            self._pipe = pipe
+        for sv in pipe:
+            sv.params = _lib.NcsbParams.from_buffer_copy(self.params)
+            sv._check(sv.lib.ncsb_set_params(sv._handle, ctypes.byref(sv.params)))
+            if self.mask_shifted is None:
+                raise RuntimeError("set an OTF mask first")
+            if sv.mask_shifted is None or not numpy.array_equal(sv.mask_shifted, self.mask_shifted):
+                sv.set_otf_mask_shifted(self.mask_shifted)
+        cur = torch.cuda.current_stream(self.device)
+        streams = [torch.cuda.Stream(device=self.device) for _ in range(n_streams)]
+        with torch.cuda.device(self.device):
+            d_g = None if per_frame else h_g.to(self.device, non_blocking=True)
+            ready = torch.cuda.Event()
+            ready.record(cur)
+            bufs = []
+            for st in streams:
+                st.wait_event(ready)
+                with torch.cuda.stream(st):
+                    bufs.append((torch.empty((chunk_frames, H, W), dtype=torch.float32,
+                                             device=self.device),
+                                 torch.empty((chunk_frames, H, W), dtype=torch.float32,
+                                             device=self.device),
+                                 torch.empty((chunk_frames, H, W), dtype=torch.float32,
+                                             device=self.device) if per_frame else None))
+            for i, f0 in enumerate(range(0, T, chunk_frames)):
+                n = min(chunk_frames, T - f0)
+                k = i % n_streams
+                st, (d_in, d_out, d_gf) = streams[k], bufs[k]
+                with torch.cuda.stream(st):
+                    d_in[:n].copy_(h_in[f0:f0 + n], non_blocking=True)
+                    g = d_g
+                    if per_frame:
+                        d_gf[:n].copy_(h_g[f0:f0 + n], non_blocking=True)
+                        g = d_gf[:n]
+                    pipe[k].reduce_noise(d_in[:n], g, out=d_out[:n], stream=st)
+                    out[f0:f0 + n].copy_(d_out[:n], non_blocking=True)
+            for st in streams:
+                st.synchronize()
+        return out
+
     def solve_tiles(self, data, gamma, u0=None, stream=None):
         """Solve [N, 16, 16] tiles (gamma per tile, the layout of the reference
         kernel cuda/ncs.cu:873-879).  Returns (u, iters, status, cost)."""

@@ -36,19 +36,25 @@ import torch
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic FP32 work of the plain solver per tile ("Roofline"):
-#   Q application by 16x16 real FFTs (forward + inverse, 2 x 2.5 N log2 N with
-#   N = 256) and the spectrum weighting                       11,264
-#   initial gradient (256 x 9) + norms                          3,328
-#   per iteration: Q application 11,264, directional dots 1,536, accepted
-#   point + gradient 2,304, norms / curvature dots 2,048, L-BFGS direction
-#   with k stored pairs 4 * 256 * 2 * k (2k dot products with the new
-#   gradient, 2k axpys into the direction)
-#   per line-search trial: 256 x (log1p, divide, 6 flops)        2,048
+# Algorithmic FP32 work per tile ("Roofline").  A real 16x16
+# 2-D FFT is counted as 2.5 N log2 N = 5,120 flops (N = 256).
+#   start (both forms): Q u by a forward + inverse FFT and the spectrum
+#     weighting (11,264), gradient and norms (3,328)              14,592
+#   per line-search trial: 256 x (log1p, divide, 6 flops)          2,048
+# plain form (scalar initial matrix), per iteration: Q p (11,264),
+#   directional dots (1,536), accepted point + gradient (2,304), norms and
+#   curvature dots (2,048), plus 2,048 per stored pair (2 dots, 2 axpys)
+# spectral form, per iteration: one forward + two inverse FFTs and two
+#   spectrum weightings (17,408), directional dots (1,536), accepted point
+#   + gradient + curvature (2,816), norms and lambda (2,048), plus 2,560 per
+#   stored pair (2 dots, 3 axpys)
 FLOP_INIT = 11264 + 3328
-FLOP_ITER_BASE = 11264 + 1536 + 2304 + 2048
-FLOP_TWO_LOOP_PER_PAIR = 4 * 256 * 2
 FLOP_TRIAL = 2048
+FLOP_ITER_BASE = {"plain": 11264 + 1536 + 2304 + 2048, "plain_wg": 11264 + 1536 + 2304 + 2048,
+                  "spectral": 17408 + 1536 + 2816 + 2048}
+FLOP_PER_PAIR = {"plain": 4 * 256 * 2, "plain_wg": 4 * 256 * 2, "spectral": 5 * 256 * 2}
+KERNEL = {"plain": "ncs_warp_kernel", "plain_wg": "ncs_plain_kernel",
+          "spectral": "ncs_spectral_kernel"}
 
 
 def peaks():
@@ -311,10 +317,12 @@ def run_ours(args, world, rank, local):
     evals_n = evals.double().sum().item()
     n_tiles = iters.numel()
     m = solver.params.m
-    pairs = torch.clamp(iters.double() - 1.0, min=0.0)
-    two_loop = torch.minimum(pairs, torch.full_like(pairs, float(m)))
-    flops = (n_tiles * FLOP_INIT + iters_n * FLOP_ITER_BASE
-             + FLOP_TWO_LOOP_PER_PAIR * two_loop.sum().item()
+    # pairs stored when iteration i starts: min(i, m) for i = 0 .. iters-1
+    it = iters.double()
+    mm = float(m)
+    pairs = torch.where(it <= mm, it * (it - 1.0) / 2.0, mm * (mm - 1.0) / 2.0 + (it - mm) * mm)
+    flops = (n_tiles * FLOP_INIT + iters_n * FLOP_ITER_BASE[args.form]
+             + FLOP_PER_PAIR[args.form] * pairs.sum().item()
              + FLOP_TRIAL * (evals_n - n_tiles))
     st = status.cpu().numpy()
 
@@ -360,6 +368,32 @@ def run_ours(args, world, rank, local):
     e2e_value = px * e2e_steps / (e2e_ms / 1e3) / 1e6
     assert torch.equal(h_out, out.cpu()), "e2e result differs from the device-resident run"
 
+    # the plain GPU form (the reference's L-BFGS: scalar initial matrix,
+    # Armijo backtracking, one warp per tile) on the same stack, for the
+    # "vs plain GPU" part of the metric
+    plain = None
+    if not args.no_compare_plain and args.form != "plain":
+        ps = ncs_b200.Solver(alpha=w["alpha"], max_iters=w["max_iters"], mode="plain", m=4)
+        ps.set_otf_mask(w["mask"])
+        _, p_it, p_st, p_cost = ps.reduce_noise(images, gamma, out=out, tile_stats=True)
+        ps.reduce_noise(images, gamma, out=out)
+        barrier(world)
+        torch.cuda.synchronize()
+        pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nps = max(1, min(args.steps, 3))
+        pe0.record(stream)
+        for _ in range(nps):
+            ps.reduce_noise(images, gamma, out=out)
+        pe1.record(stream)
+        torch.cuda.synchronize()
+        p_ms = max_over_ranks(pe0.elapsed_time(pe1), world) / nps
+        plain = {"form": "plain (m=4)", "ms_per_step": p_ms,
+                 "value": px / (p_ms / 1e3) / 1e6, "mean_iters": p_it.double().mean().item(),
+                 "capped_tiles": int((p_st == -2).sum().item()),
+                 "speedup_of_form": p_ms / (total_ms / args.steps)}
+        p_cost_np = p_cost.cpu().numpy()
+        ps.close()
+
     pk, pk_src = peaks()
     n_sms = torch.cuda.get_device_properties(dev).multi_processor_count
     fp32_peak = fp32_peak_tflops(pk.get("sm_max_mhz", 1965.0), n_sms)
@@ -385,7 +419,7 @@ def run_ours(args, world, rank, local):
         "status": {str(k): int((st == k).sum()) for k in range(-5, 1) if (st == k).any()},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
-                     "kernel": "ncs_warp_kernel" if args.form == "plain" else "ncs_plain_kernel",
+                     "kernel": KERNEL[args.form],
                      "peak_source": "148 SMs x 128 FP32 lanes x 2 x %s sm_max_mhz (%s)"
                                     % (pk.get("sm_max_mhz"), pk_src),
                      "flops_per_launch": flops,
@@ -400,6 +434,8 @@ def run_ours(args, world, rank, local):
         "gpu_launches": args.steps,
         "clocks": clk,
     }
+    if plain is not None:
+        line["plain_gpu"] = plain
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         imgs = images.cpu().numpy()
@@ -412,6 +448,8 @@ def run_ours(args, world, rank, local):
             "sample": "%d of %d frames, one per thread, pyCNCS cReduceNoise FP64, "
                       "max_iterations=%d" % (n, T, w["max_iters"])}
         line["accuracy"] = accuracy_gate(w, cost.cpu().numpy(), args.accuracy_tiles)
+        if plain is not None:
+            line["plain_gpu"]["accuracy"] = accuracy_gate(w, p_cost_np, args.accuracy_tiles)
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -425,7 +463,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="stack512")
     ap.add_argument("--frames", type=int, default=None, help="override the frame count")
-    ap.add_argument("--form", default="plain")
+    ap.add_argument("--form", default="spectral", choices=sorted(KERNEL))
+    ap.add_argument("--no-compare-plain", action="store_true",
+                    help="skip timing the plain form on the same stack")
     ap.add_argument("--accuracy-tiles", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

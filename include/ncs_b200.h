@@ -58,6 +58,8 @@ extern "C" {
 /* Solver forms. */
 #define NCSB_MODE_PLAIN 0     /* FP32 SIMT, one warp per tile, in-register/smem FFT */
 #define NCSB_MODE_PLAIN_WG 1  /* FP32 SIMT, one warp group per tile (comparison form) */
+#define NCSB_MODE_SPECTRAL 2  /* FP32 SIMT, one warp per tile, L-BFGS with the spectral
+                                 initial inverse Hessian (lambda I + 2 alpha Q)^-1; m <= 4 */
 
 /* Tile geometry is fixed: 16x16 tiles, 14x14 interiors, stride 14. */
 #define NCSB_TILE 16
@@ -65,9 +67,10 @@ extern "C" {
 typedef struct {
     double alpha;      /* NCS alpha (ncs.c:352, ncs.cu:959) */
     int32_t max_iters; /* L-BFGS iteration cap (ncs.cu MAXITERS = 200) */
-    int32_t m;         /* history pairs, 1..8 (ncs.cu M = 8; libLBFGS m = 6; default 4:
-                          NCS tiles need the same iterations for m = 3..8, measured,
-                          and each iteration costs less with fewer pairs) */
+    int32_t m;         /* history pairs, 1..8, at most 4 in the spectral form (ncs.cu M = 8;
+                          libLBFGS m = 6; default 2: NCS tiles need the same number of
+                          iterations for every m measured, 1..8 in the plain form and
+                          1..4 in the spectral one, and fewer pairs cost less) */
     double epsilon;    /* stop when ||g|| <= epsilon * max(1, ||u||)
                           (ncs.cu EPSILON = 1e-4; libLBFGS epsilon = 1e-5) */
     double c1;         /* Armijo constant (ncs.cu C_1 = 1e-4) */
@@ -78,8 +81,8 @@ typedef struct {
 
 typedef struct ncsb_handle ncsb_handle;
 
-/* Fill *p with the defaults: alpha 0.2, max_iters 200, m 4, epsilon 1e-5,
- * c1 1e-4, min_step 1e-6, plain mode, auto grid. */
+/* Fill *p with the defaults: alpha 0.2, max_iters 200, m 2, epsilon 1e-5,
+ * c1 1e-4, min_step 1e-6, spectral form, auto grid. */
 void ncsb_default_params(ncsb_params *p);
 
 /* Create a handle on the current CUDA device; allocates its small device

@@ -18,6 +18,7 @@ NCSB_ESCRATCH = -5
 
 MODE_PLAIN = 0
 MODE_PLAIN_WG = 1
+MODE_SPECTRAL = 2
 
 # Per-tile status codes (cuda/ncs.cu:61-67).
 SUCCESS = 0

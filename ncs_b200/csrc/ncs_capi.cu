@@ -16,6 +16,8 @@ cudaError_t launch_plain(const SolveArgs& args, int grid, cudaStream_t stream);
 int plain_max_ctas_per_sm();
 cudaError_t launch_warp_blocks(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
 int warp_max_ctas_per_sm(int m, int blocks);
+cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
+int spectral_max_ctas_per_sm(int m, int blocks);
 }  // namespace ncsb
 
 struct ncsb_handle {
@@ -47,7 +49,7 @@ int check_params(const ncsb_params* p, std::string* why) {
     if (!(p->epsilon >= 0.0)) { *why = "epsilon must be >= 0"; return NCSB_EINVAL; }
     if (!(p->c1 > 0.0 && p->c1 < 1.0)) { *why = "c1 must be in (0, 1)"; return NCSB_EINVAL; }
     if (!(p->min_step > 0.0)) { *why = "min_step must be > 0"; return NCSB_EINVAL; }
-    if (p->mode != NCSB_MODE_PLAIN && p->mode != NCSB_MODE_PLAIN_WG) { *why = "unsupported mode"; return NCSB_EINVAL; }
+    if (p->mode != NCSB_MODE_PLAIN && p->mode != NCSB_MODE_PLAIN_WG && p->mode != NCSB_MODE_SPECTRAL) { *why = "unsupported mode"; return NCSB_EINVAL; }
     if (p->ctas_per_sm < 0) { *why = "ctas_per_sm must be >= 0"; return NCSB_EINVAL; }
     return NCSB_OK;
 }
@@ -76,9 +78,12 @@ int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s) {
     a.max_iters = h->p.max_iters;
     a.m = h->p.m;
     const bool wg = h->p.mode == NCSB_MODE_PLAIN_WG;
+    const bool spec = h->p.mode == NCSB_MODE_SPECTRAL;
     int per_sm = h->p.ctas_per_sm > 0
                      ? h->p.ctas_per_sm
-                     : (wg ? ncsb::plain_max_ctas_per_sm() : ncsb::warp_max_ctas_per_sm(a.m, 0));
+                     : (wg ? ncsb::plain_max_ctas_per_sm()
+                           : (spec ? ncsb::spectral_max_ctas_per_sm(a.m, 0)
+                                   : ncsb::warp_max_ctas_per_sm(a.m, 0)));
     // warp-per-tile CTAs hold 4 tiles at a time
     const long long tiles_per_cta = wg ? 1 : 4;
     long long grid = (long long)per_sm * h->num_sms;
@@ -86,7 +91,8 @@ int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s) {
         grid = (a.n_tiles + tiles_per_cta - 1) / tiles_per_cta;
     if (grid < 1) grid = 1;
     e = wg ? ncsb::launch_plain(a, (int)grid, s)
-           : ncsb::launch_warp_blocks(a, (int)grid, h->p.ctas_per_sm, s);
+           : (spec ? ncsb::launch_spectral(a, (int)grid, h->p.ctas_per_sm, s)
+                   : ncsb::launch_warp_blocks(a, (int)grid, h->p.ctas_per_sm, s));
     if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
     return NCSB_OK;
 }
@@ -99,11 +105,11 @@ void ncsb_default_params(ncsb_params* p) {
     if (!p) return;
     p->alpha = 0.2;
     p->max_iters = 200;
-    p->m = 4;
+    p->m = 2;
     p->epsilon = 1e-5;
     p->c1 = 1e-4;
     p->min_step = 1e-6;
-    p->mode = NCSB_MODE_PLAIN;
+    p->mode = NCSB_MODE_SPECTRAL;
     p->ctas_per_sm = 0;
 }
 

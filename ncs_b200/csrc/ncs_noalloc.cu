@@ -25,6 +25,8 @@ cudaError_t launch_plain(const SolveArgs& args, int grid, cudaStream_t stream);
 int plain_max_ctas_per_sm();
 cudaError_t launch_warp(const SolveArgs& args, int grid, cudaStream_t stream);
 int warp_max_ctas_per_sm(int m);
+cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
+int spectral_max_ctas_per_sm(int m, int blocks);
 }  // namespace ncsb
 
 namespace {
@@ -89,7 +91,9 @@ int tiles_along(int n) {
 bool params_ok(const ncsb_params* p) {
     return p && std::isfinite(p->alpha) && p->alpha >= 0.0 && p->max_iters >= 0 && p->m >= 1 &&
            p->m <= ncsb::kMaxM && p->epsilon >= 0.0 && p->c1 > 0.0 && p->c1 < 1.0 &&
-           p->min_step > 0.0 && (p->mode == NCSB_MODE_PLAIN || p->mode == NCSB_MODE_PLAIN_WG) &&
+           p->min_step > 0.0 &&
+           (p->mode == NCSB_MODE_PLAIN || p->mode == NCSB_MODE_PLAIN_WG ||
+            p->mode == NCSB_MODE_SPECTRAL) &&
            p->ctas_per_sm >= 0;
 }
 
@@ -156,13 +160,19 @@ extern "C" int ncsb_reduce_noise_noalloc(const ncsb_params* p, const float* mask
     a.max_iters = p->max_iters;
     a.m = p->m;
     const bool wg = p->mode == NCSB_MODE_PLAIN_WG;
-    const int per_sm = p->ctas_per_sm > 0 ? p->ctas_per_sm
-                                          : (wg ? dev->ctas_per_sm : ncsb::warp_max_ctas_per_sm(a.m));
+    const bool spec = p->mode == NCSB_MODE_SPECTRAL;
+    const int per_sm = p->ctas_per_sm > 0
+                           ? p->ctas_per_sm
+                           : (wg ? dev->ctas_per_sm
+                                 : (spec ? ncsb::spectral_max_ctas_per_sm(a.m, 0)
+                                         : ncsb::warp_max_ctas_per_sm(a.m)));
     const long long tiles_per_cta = wg ? 1 : 4;
     long long grid = (long long)per_sm * dev->num_sms;
     if (grid > (a.n_tiles + tiles_per_cta - 1) / tiles_per_cta)
         grid = (a.n_tiles + tiles_per_cta - 1) / tiles_per_cta;
     if (grid < 1) grid = 1;
-    const cudaError_t e = wg ? ncsb::launch_plain(a, (int)grid, s) : ncsb::launch_warp(a, (int)grid, s);
+    const cudaError_t e = wg     ? ncsb::launch_plain(a, (int)grid, s)
+                          : spec ? ncsb::launch_spectral(a, (int)grid, p->ctas_per_sm, s)
+                                 : ncsb::launch_warp(a, (int)grid, s);
     return e == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
 }

@@ -1,0 +1,319 @@
+// ncs_warp_common.cuh -- device helpers of the warp-per-tile NCS solvers
+// (ncs_warp.cu, ncs_spectral.cu): lane geometry, the 16x16 FFT pieces,
+// warp reductions, the line-search log1p and tile gather helpers.
+//
+// Lane L of a warp holds rows P = L >> 2 and P + 8 at columns Qd + 4j
+// (Qd = L & 3, j = 0..3) of its tile, packed as x[P][c] + i x[P+8][c].
+#pragma once
+
+#include "ncs_internal.cuh"
+
+namespace ncsb {
+namespace warp {
+
+
+constexpr int kWarps = 4;
+constexpr int kWarpCtaThreads = 32 * kWarps;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr float kS2 = 0.70710678118654752f;  // sqrt(1/2)
+
+// Per-warp shared memory (the history arrays follow it, sized by m).
+struct WarpSmem {
+    float2 fb[16][17];    // FFT transpose buffer
+    float R[kMaxM][kMaxM];   // s_i'y_j by slot (upper triangle in age order is used)
+    float YY[kMaxM][kMaxM];  // y_i'y_j by slot
+    float rinv[kMaxM];       // 1 / s_i'y_i by slot
+};
+
+constexpr size_t kTableBytes = 256 * sizeof(float);
+
+__host__ __device__ constexpr size_t warp_bytes(int m) {
+    return ((sizeof(WarpSmem) + 15) / 16) * 16 + 2 * (size_t)m * 32 * 2 * sizeof(float4);
+}
+
+__device__ __forceinline__ int bitrev3(int i) {
+    return ((i & 1) << 2) | (i & 2) | ((i & 4) >> 2);
+}
+
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 mul_i(float2 a) { return make_float2(-a.y, a.x); }      // i a
+__device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }     // -i a
+__device__ __forceinline__ float2 conjmul(float2 a, float2 w) {                            // a conj(w)
+    return make_float2(fmaf(a.x, w.x, a.y * w.y), fmaf(a.y, w.x, -a.x * w.y));
+}
+__device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
+    return make_float2(__shfl_xor_sync(kFull, v.x, m), __shfl_xor_sync(kFull, v.y, m));
+}
+
+// W16^p = exp(-2 pi i p / 16), p = 0..7
+__device__ __forceinline__ float2 w16(int p) {
+    const float c[8] = {1.0f, 0.92387953251128674f, kS2, 0.38268343236508978f,
+                        0.0f, -0.38268343236508978f, -kS2, -0.92387953251128674f};
+    const float s[8] = {0.0f, 0.38268343236508978f, kS2, 0.92387953251128674f,
+                        1.0f, 0.92387953251128674f, kS2, 0.38268343236508978f};
+    return make_float2(c[p], -s[p]);
+}
+
+// In-place 8-point DFT, decimation in frequency: natural order in, output
+// position i holds frequency bitrev3(i).  Unnormalised.
+__device__ __forceinline__ void fft8_fwd(float2 (&e)[8]) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const float2 a = e[r] + e[r + 4], b = e[r] - e[r + 4];
+        e[r] = a;
+        if (r == 0) e[r + 4] = b;
+        else if (r == 1) e[r + 4] = make_float2(kS2 * (b.x + b.y), kS2 * (b.y - b.x));
+        else if (r == 2) e[r + 4] = mul_mi(b);
+        else e[r + 4] = make_float2(kS2 * (b.y - b.x), -kS2 * (b.x + b.y));
+    }
+#pragma unroll
+    for (int base = 0; base < 8; base += 4) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const float2 a = e[base + r] + e[base + r + 2], b = e[base + r] - e[base + r + 2];
+            e[base + r] = a;
+            e[base + r + 2] = r == 0 ? b : mul_mi(b);
+        }
+    }
+#pragma unroll
+    for (int base = 0; base < 8; base += 2) {
+        const float2 a = e[base] + e[base + 1], b = e[base] - e[base + 1];
+        e[base] = a;
+        e[base + 1] = b;
+    }
+}
+
+// Inverse of fft8_fwd up to the factor 8: bit-reversed in, natural out,
+// conjugate twiddles (unnormalised inverse DFT).
+__device__ __forceinline__ void fft8_inv(float2 (&e)[8]) {
+#pragma unroll
+    for (int base = 0; base < 8; base += 2) {
+        const float2 a = e[base], b = e[base + 1];
+        e[base] = a + b;
+        e[base + 1] = a - b;
+    }
+#pragma unroll
+    for (int base = 0; base < 8; base += 4) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const float2 t = r == 0 ? e[base + r + 2] : mul_i(e[base + r + 2]);
+            const float2 a = e[base + r];
+            e[base + r] = a + t;
+            e[base + r + 2] = a - t;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const float2 b = e[r + 4];
+        float2 t;
+        if (r == 0) t = b;
+        else if (r == 1) t = make_float2(kS2 * (b.x - b.y), kS2 * (b.x + b.y));
+        else if (r == 2) t = mul_i(b);
+        else t = make_float2(-kS2 * (b.x + b.y), kS2 * (b.x - b.y));
+        const float2 a = e[r];
+        e[r] = a + t;
+        e[r + 4] = a - t;
+    }
+}
+
+struct LaneGeo {
+    int lane, P, Qd, KC, H, k0;
+    float2 tw1, tw2, tw3;  // W16^(Qd*k1), k1 = 1..3
+    float sA, sB, sH;      // butterfly signs of this lane
+};
+
+__device__ __forceinline__ LaneGeo lane_geo(int lane) {
+    LaneGeo g;
+    g.lane = lane;
+    g.P = lane >> 2;
+    g.Qd = lane & 3;
+    g.KC = lane >> 1;
+    g.H = lane & 1;
+    g.k0 = 4 * ((g.Qd & 1) * 2 + (g.Qd >> 1));  // 4 * bitrev2(Qd)
+    float sn, cs;
+    sincospif((float)(g.Qd * 1) / 8.0f, &sn, &cs);
+    g.tw1 = make_float2(cs, -sn);
+    sincospif((float)(g.Qd * 2) / 8.0f, &sn, &cs);
+    g.tw2 = make_float2(cs, -sn);
+    sincospif((float)(g.Qd * 3) / 8.0f, &sn, &cs);
+    g.tw3 = make_float2(cs, -sn);
+    g.sA = g.Qd < 2 ? 1.0f : -1.0f;
+    g.sB = (g.Qd & 1) ? -1.0f : 1.0f;
+    g.sH = g.H ? -1.0f : 1.0f;
+    return g;
+}
+
+// Forward half of the 16x16 transform: lane (KC = L>>1, H = L&1) ends with
+// the spectrum X[2 bitrev3(i) + H][KC] of its 8 pixels' tile in e[i]
+// (unnormalised).  Input: x[2j] = row P, x[2j+1] = row P+8, column Qd + 4j.
+__device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8], WarpSmem& ws,
+                                             const LaneGeo& L) {
+    // rows: 4-point DFT over j in the lane, twiddle, 4-point DFT across lanes
+    float2 V[4];
+    {
+        const float2 z0 = make_float2(x[0], x[1]), z1 = make_float2(x[2], x[3]);
+        const float2 z2 = make_float2(x[4], x[5]), z3 = make_float2(x[6], x[7]);
+        const float2 s02 = z0 + z2, d02 = z0 - z2, s13 = z1 + z3, d13 = z1 - z3;
+        V[0] = s02 + s13;
+        V[2] = cmul(s02 - s13, L.tw2);
+        V[1] = cmul(d02 + mul_mi(d13), L.tw1);
+        V[3] = cmul(d02 + mul_i(d13), L.tw3);
+    }
+    const bool q3 = L.Qd == 3;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 p = shfl_xor2(V[k], 2);
+        float2 t = make_float2(fmaf(L.sA, V[k].x, p.x), fmaf(L.sA, V[k].y, p.y));
+        V[k] = q3 ? mul_mi(t) : t;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 p = shfl_xor2(V[k], 1);
+        V[k] = make_float2(fmaf(L.sB, V[k].x, p.x), fmaf(L.sB, V[k].y, p.y));
+    }
+    __syncwarp();  // previous users of the transpose buffer are done
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ws.fb[L.P][L.k0 + k] = V[k];
+    __syncwarp();
+
+    // columns: lane (KC, H) separates the two packed rows of every row pair
+    // from X[KC] and X[-KC], forms the even (H = 0) or odd (H = 1) half of the
+    // 16-point column DFT and transforms it with an 8-point DFT.
+    const int kneg = (16 - L.KC) & 15;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const float2 Z = ws.fb[p][L.KC], Zm = ws.fb[p][kneg];
+        const float sx = Z.x + Zm.x, dx = Z.x - Zm.x, sy = Z.y + Zm.y, dy = Z.y - Zm.y;
+        float2 ev = make_float2(0.5f * fmaf(L.sH, sy, sx), 0.5f * fmaf(-L.sH, dx, dy));
+        const float2 w = w16(p);
+        e[p] = L.H ? cmul(ev, w) : ev;
+    }
+    fft8_fwd(e);
+}
+
+// Inverse half: from a spectrum in the layout warp_fft_fwd leaves, the real
+// tile back in this lane's 8 pixels (unnormalised inverse: x 256).
+__device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float (&y)[8], WarpSmem& ws,
+                                             const LaneGeo& L) {
+    fft8_inv(e);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const float2 w = w16(r);
+        e[r] = L.H ? conjmul(e[r], w) : e[r];
+    }
+    float2 out[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const float2 q = shfl_xor2(e[r], 1);
+        // H = 0: rows r = e + q ; H = 1: rows r + 8 = q - e
+        out[r] = make_float2(fmaf(L.sH, e[r].x, q.x), fmaf(L.sH, e[r].y, q.y));
+    }
+    __syncwarp();  // every lane has read the row spectra
+#pragma unroll
+    for (int r = 0; r < 8; ++r) ws.fb[r + 8 * L.H][L.KC] = out[r];
+    __syncwarp();
+
+    // inverse rows: pack the two real output rows, inverse transforms
+    float2 V[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 a = ws.fb[L.P][L.k0 + k], b = ws.fb[L.P + 8][L.k0 + k];
+        V[k] = make_float2(a.x - b.y, a.y + b.x);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 p = shfl_xor2(V[k], 1);
+        V[k] = make_float2(fmaf(L.sB, V[k].x, p.x), fmaf(L.sB, V[k].y, p.y));
+    }
+    const bool lower = L.Qd < 2, odd = (L.Qd & 1) != 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 p = shfl_xor2(V[k], 2);
+        const float2 src = lower ? p : V[k];
+        const float2 b = odd ? mul_i(src) : src;
+        const float2 other = lower ? V[k] : p;
+        V[k] = make_float2(fmaf(L.sA, b.x, other.x), fmaf(L.sA, b.y, other.y));
+    }
+    V[1] = conjmul(V[1], L.tw1);
+    V[2] = conjmul(V[2], L.tw2);
+    V[3] = conjmul(V[3], L.tw3);
+    {
+        const float2 s02 = V[0] + V[2], d02 = V[0] - V[2], s13 = V[1] + V[3], d13 = V[1] - V[3];
+        const float2 z0 = s02 + s13, z2 = s02 - s13;
+        const float2 z1 = d02 + mul_i(d13), z3 = d02 + mul_mi(d13);
+        y[0] = z0.x; y[1] = z0.y; y[2] = z1.x; y[3] = z1.y;
+        y[4] = z2.x; y[5] = z2.y; y[6] = z3.x; y[7] = z3.y;
+    }
+}
+
+// y = Q x for the 8 pixels of this lane; mt = this lane's 8 values of
+// M^2/256 in the column-pass layout.
+__device__ __forceinline__ void warp_apply_q(const float (&x)[8], float (&y)[8], WarpSmem& ws,
+                                             const float* mt, const LaneGeo& L, float* nc_part) {
+    float2 e[8];
+    warp_fft_fwd(x, e, ws, L);
+    const float4 m0 = *reinterpret_cast<const float4*>(mt);
+    const float4 m1 = *reinterpret_cast<const float4*>(mt + 4);
+    const float mk[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+    if (nc_part) {
+        float s = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) s = fmaf(fmaf(e[i].x, e[i].x, e[i].y * e[i].y), mk[i], s);
+        *nc_part = s;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) e[i] = make_float2(e[i].x * mk[i], e[i].y * mk[i]);
+    warp_fft_inv(e, y, ws, L);
+}
+
+// log1p(x) for x > -1: 2 atanh(y), y = x / (2 + x), by the odd series
+// 2y (1 + y^2/3 + ... + y^10/11) when |x| <= 1/2 (|y| <= 1/5, truncation
+// < 1e-9 relative); otherwise log(1 + x) from the hardware log2, whose
+// absolute error is small against |log(1 + x)| >= 0.4 there.
+__device__ __forceinline__ float log1p_ls(float x) {
+    const float y = __fdividef(x, 2.0f + x);
+    const float y2 = y * y;
+    float s = fmaf(y2, 1.0f / 11.0f, 1.0f / 9.0f);
+    s = fmaf(y2, s, 1.0f / 7.0f);
+    s = fmaf(y2, s, 1.0f / 5.0f);
+    s = fmaf(y2, s, 1.0f / 3.0f);
+    s = fmaf(y2, s, 1.0f);
+    const float small = 2.0f * y * s;
+    return fabsf(x) <= 0.5f ? small : __logf(1.0f + x);
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int tile_origin(int i, int n) {
+    const int o = 14 * i, last = n + 2 - kTile;
+    return o < last ? o : last;
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+__device__ __forceinline__ void load8(const float4* h, float (&x)[8]) {
+    const float4 a = h[0], b = h[1];
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+
+__device__ __forceinline__ void store8(float4* h, const float (&x)[8]) {
+    h[0] = make_float4(x[0], x[1], x[2], x[3]);
+    h[1] = make_float4(x[4], x[5], x[6], x[7]);
+}
+
+}  // namespace warp
+}  // namespace ncsb

@@ -40,7 +40,8 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
 
 
-_MODES = {"plain": _lib.MODE_PLAIN, "plain_wg": _lib.MODE_PLAIN_WG}
+_MODES = {"plain": _lib.MODE_PLAIN, "plain_wg": _lib.MODE_PLAIN_WG,
+          "spectral": _lib.MODE_SPECTRAL}
 
 
 class Solver:
@@ -50,11 +51,14 @@ class Solver:
     ``max_iters`` (MAXITERS), ``m`` (history size M), ``epsilon`` (stopping
     tolerance on ||g|| / max(1, ||u||)), ``c1`` (Armijo), ``min_step``.
     The default ``epsilon`` is libLBFGS's 1e-5 (the pyCNCS path) rather than
-    the reference kernel's 1e-4.
+    the reference kernel's 1e-4.  ``mode``: "spectral" (default; L-BFGS with
+    the spectral initial inverse Hessian), "plain" (the reference's L-BFGS
+    with a scalar initial matrix, one warp per tile) or "plain_wg" (one warp
+    group per tile).
     """
 
-    def __init__(self, alpha=0.2, max_iters=200, m=4, epsilon=1e-5, c1=1e-4, min_step=1e-6,
-                 mode="plain", ctas_per_sm=0, device=None):
+    def __init__(self, alpha=0.2, max_iters=200, m=2, epsilon=1e-5, c1=1e-4, min_step=1e-6,
+                 mode="spectral", ctas_per_sm=0, device=None):
         self.lib = _lib.load()
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None
                                    else torch.device(device).index or 0)

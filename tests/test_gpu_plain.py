@@ -21,6 +21,13 @@ def ncs(cuda_ok):
     return ncs_b200
 
 
+# every solver form: spectral (default), plain (reference-like L-BFGS, one
+# warp per tile) and plain_wg (one warp group per tile)
+@pytest.fixture(params=["spectral", "plain", "plain_wg"])
+def mode(request):
+    return request.param
+
+
 def tiles_seed1(n, rng=None):
     """data U(10,20), gamma U(2,4) -- cuda/pyCUDANCS/test/test_solver.py:79-84."""
     numpy.random.seed(1)
@@ -29,12 +36,12 @@ def tiles_seed1(n, rng=None):
     return data, gamma
 
 
-def test_tiles_vs_fp64_optimum_and_reference(ncs, oracle_libs):
+def test_tiles_vs_fp64_optimum_and_reference(ncs, oracle_libs, mode):
     from oracle import numpy_ref as nr
     n, alpha = 64, 0.1
     data, gamma = tiles_seed1(n)
     ms = create_otf_mask_shifted()
-    s = ncs.Solver(alpha=alpha, epsilon=1e-6, max_iters=500)
+    s = ncs.Solver(alpha=alpha, epsilon=1e-6, max_iters=500, mode=mode)
     s.set_otf_mask_shifted(ms)
     u, iters, status, cost = s.solve_tiles(torch.from_numpy(data).cuda(),
                                            torch.from_numpy(gamma).cuda())
@@ -61,7 +68,7 @@ def test_tiles_vs_fp64_optimum_and_reference(ncs, oracle_libs):
         assert (numpy.abs(u[i] - uref) / numpy.maximum(numpy.abs(uref), 1.0)).max() <= 1e-3
 
 
-def test_matches_pycncs_on_photon_like_tiles(ncs, oracle_libs):
+def test_matches_pycncs_on_photon_like_tiles(ncs, oracle_libs, mode):
     """GPU vs the pyCNCS C path on bright photon-like tiles (alpha 0.2).
 
     At both solvers' default stopping rule (epsilon 1e-5 on ||g||/max(1,||u||))
@@ -78,7 +85,7 @@ def test_matches_pycncs_on_photon_like_tiles(ncs, oracle_libs):
     ms = create_otf_mask_shifted()
     d64, g64, m64 = (x.astype(numpy.float64) for x in (data, gamma, ms))
     for eps, check_pixels in ((1e-5, False), (1e-6, True)):
-        s = ncs.Solver(alpha=alpha, epsilon=eps, max_iters=1000)
+        s = ncs.Solver(alpha=alpha, epsilon=eps, max_iters=1000, mode=mode)
         s.set_otf_mask_shifted(ms)
         u, iters, status, cost = s.solve_tiles(torch.from_numpy(data).cuda(),
                                                torch.from_numpy(gamma).cuda())
@@ -98,7 +105,7 @@ def test_matches_pycncs_on_photon_like_tiles(ncs, oracle_libs):
 
 
 @pytest.mark.parametrize("shape", [(2, 45, 37), (1, 14, 14), (3, 16, 30), (1, 64, 64)])
-def test_stack_mode_equals_host_tiling(ncs, shape):
+def test_stack_mode_equals_host_tiling(ncs, shape, mode):
     """Device segmentation + owner-rule stitching is bit-identical to host
     tiling (numpy.pad 'edge', ncs_c.py:296-319) + tile solve + row-major
     overwrite stitching (ncs.c:121-130)."""
@@ -107,7 +114,7 @@ def test_stack_mode_equals_host_tiling(ncs, shape):
     T, H, W = shape
     images = rng.uniform(1.0, 50.0, size=shape).astype(numpy.float32)
     gamma = rng.uniform(1.0, 20.0, size=(H, W)).astype(numpy.float32)
-    s = ncs.Solver(alpha=0.2, max_iters=30)
+    s = ncs.Solver(alpha=0.2, max_iters=30, mode=mode)
     s.set_otf_mask_shifted(create_otf_mask_shifted())
     out, iters, status, cost = s.reduce_noise(torch.from_numpy(images).cuda(),
                                               torch.from_numpy(gamma).cuda(), tile_stats=True)
@@ -121,7 +128,7 @@ def test_stack_mode_equals_host_tiling(ncs, shape):
     assert numpy.array_equal(status.cpu().numpy(), st2.cpu().numpy())
 
 
-def test_crops_vs_pycncs(ncs, oracle_libs):
+def test_crops_vs_pycncs(ncs, oracle_libs, mode):
     """cuda/pyCUDANCS/test/test_im.py:16-44: 144 crops of a 30x30 frame,
     alpha 0.02, random symmetric mask, atol 0.02 against cReduceNoise."""
     rng = numpy.random.default_rng(1)
@@ -129,7 +136,7 @@ def test_crops_vs_pycncs(ncs, oracle_libs):
     image = rng.uniform(0.01, 10.0, size=(30, 30))
     otfmask = random_otf_mask(16, rng)
     shifted = numpy.fft.fftshift(otfmask)
-    nc = ncs.NCSCUDA()
+    nc = ncs.NCSCUDA(mode=mode)
     nc.setOTFMask(otfmask)
     worst = 0.0
     for ix in range(12):
@@ -143,9 +150,9 @@ def test_crops_vs_pycncs(ncs, oracle_libs):
     assert worst < 0.02
 
 
-def test_status_codes_and_caps(ncs):
+def test_status_codes_and_caps(ncs, mode):
     data, gamma = tiles_seed1(8)
-    s = ncs.Solver(alpha=0.1, max_iters=0)
+    s = ncs.Solver(alpha=0.1, max_iters=0, mode=mode)
     s.set_otf_mask_shifted(create_otf_mask_shifted())
     d = torch.from_numpy(data).cuda()
     g = torch.from_numpy(gamma).cuda()
@@ -169,9 +176,9 @@ def test_status_codes_and_caps(ncs):
     assert torch.equal(u1[keep], u2[keep])
 
 
-def test_warm_start_input_and_determinism(ncs):
+def test_warm_start_input_and_determinism(ncs, mode):
     data, gamma = tiles_seed1(16)
-    s = ncs.Solver(alpha=0.1, epsilon=1e-6)
+    s = ncs.Solver(alpha=0.1, epsilon=1e-6, mode=mode)
     s.set_otf_mask_shifted(create_otf_mask_shifted())
     d = torch.from_numpy(data).cuda()
     g = torch.from_numpy(gamma).cuda()
@@ -204,7 +211,7 @@ def test_drop_in_errors(ncs):
         s.reduce_noise(torch.ones(1, 10, 10, device="cuda"), torch.ones(10, 10, device="cuda"))
 
 
-def test_accuracy_gate_on_synthetic_frames(ncs):
+def test_accuracy_gate_on_synthetic_frames(ncs, mode):
     """stack512-style frames with the workload cap (20 iterations): every
     sampled tile's final cost within 1e-4 relative of the FP64 optimum, and
     no line-search failures (the fraction-to-barrier rule keeps trials out of
@@ -212,7 +219,7 @@ def test_accuracy_gate_on_synthetic_frames(ncs):
     from ncs_b200 import sim
     from oracle import numpy_ref as nr
     w = sim.make_stack("stack512", T=2, device="cuda", seed=77)
-    s = ncs.Solver(alpha=w["alpha"], max_iters=w["max_iters"])
+    s = ncs.Solver(alpha=w["alpha"], max_iters=w["max_iters"], mode=mode)
     s.set_otf_mask(w["mask"])
     out, iters, status, cost = s.reduce_noise(w["images"], w["gamma"], tile_stats=True)
     st = status.cpu().numpy()
@@ -225,7 +232,7 @@ def test_accuracy_gate_on_synthetic_frames(ncs):
     assert gap.max() <= 1e-4, gap.max()
 
 
-def test_host_pipeline_equals_device_solve(ncs):
+def test_host_pipeline_equals_device_solve(ncs, mode):
     """Solver.reduce_noise_host (chunks over 3 streams, one handle each) gives
     bit-identical frames to the device-resident solve, for shared and
     per-frame gamma and for a chunk size that does not divide the stack."""
@@ -234,7 +241,7 @@ def test_host_pipeline_equals_device_solve(ncs):
     images = rng.uniform(1.0, 90.0, size=(T, H, W)).astype(numpy.float32)
     gamma = rng.uniform(1.0, 20.0, size=(H, W)).astype(numpy.float32)
     gframes = rng.uniform(1.0, 20.0, size=(T, H, W)).astype(numpy.float32)
-    s = ncs.Solver(alpha=0.2, max_iters=25)
+    s = ncs.Solver(alpha=0.2, max_iters=25, mode=mode)
     s.set_otf_mask_shifted(create_otf_mask_shifted())
     for g in (gamma, gframes):
         ref = s.reduce_noise(torch.from_numpy(images).cuda(), torch.from_numpy(g).cuda()).cpu()

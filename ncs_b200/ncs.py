@@ -186,33 +186,40 @@ class Solver:
             chunk_frames = max(1, -(-T // 8))
         chunk_frames = max(1, min(int(chunk_frames), T))
         n_streams = max(1, int(n_streams))
+        if self.mask_shifted is None:
+            raise RuntimeError("set an OTF mask first")
+        # Streams, handles and device chunk buffers persist across calls, so a
+        # repeated call allocates nothing (new streams would defeat the caching
+        # allocator, which keeps blocks per stream).
         pipe = getattr(self, "_pipe", None)
-        if pipe is None or len(pipe) != n_streams:
-            pipe = [Solver(device=self.device) for _ in range(n_streams)]
+        if pipe is None or len(pipe["solvers"]) != n_streams:
+            pipe = {"solvers": [Solver(device=self.device) for _ in range(n_streams)],
+                    "streams": [torch.cuda.Stream(device=self.device) for _ in range(n_streams)],
+                    "bufs": None, "key": None}
             self._pipe = pipe
-        for sv in pipe:
+        for sv in pipe["solvers"]:
             sv.params = _lib.NcsbParams.from_buffer_copy(self.params)
             sv._check(sv.lib.ncsb_set_params(sv._handle, ctypes.byref(sv.params)))
-            if self.mask_shifted is None:
-                raise RuntimeError("set an OTF mask first")
             if sv.mask_shifted is None or not numpy.array_equal(sv.mask_shifted, self.mask_shifted):
                 sv.set_otf_mask_shifted(self.mask_shifted)
+        solvers, streams = pipe["solvers"], pipe["streams"]
+        key = (chunk_frames, H, W, per_frame)
         cur = torch.cuda.current_stream(self.device)
-        streams = [torch.cuda.Stream(device=self.device) for _ in range(n_streams)]
         with torch.cuda.device(self.device):
+            if pipe["key"] != key:
+                pipe["bufs"] = [
+                    (torch.empty((chunk_frames, H, W), dtype=torch.float32, device=self.device),
+                     torch.empty((chunk_frames, H, W), dtype=torch.float32, device=self.device),
+                     torch.empty((chunk_frames, H, W), dtype=torch.float32, device=self.device)
+                     if per_frame else None)
+                    for _ in streams]
+                pipe["key"] = key
+            bufs = pipe["bufs"]
             d_g = None if per_frame else h_g.to(self.device, non_blocking=True)
             ready = torch.cuda.Event()
             ready.record(cur)
-            bufs = []
             for st in streams:
                 st.wait_event(ready)
-                with torch.cuda.stream(st):
-                    bufs.append((torch.empty((chunk_frames, H, W), dtype=torch.float32,
-                                             device=self.device),
-                                 torch.empty((chunk_frames, H, W), dtype=torch.float32,
-                                             device=self.device),
-                                 torch.empty((chunk_frames, H, W), dtype=torch.float32,
-                                             device=self.device) if per_frame else None))
             for i, f0 in enumerate(range(0, T, chunk_frames)):
                 n = min(chunk_frames, T - f0)
                 k = i % n_streams
@@ -223,10 +230,19 @@ class Solver:
                     if per_frame:
                         d_gf[:n].copy_(h_g[f0:f0 + n], non_blocking=True)
                         g = d_gf[:n]
-                    pipe[k].reduce_noise(d_in[:n], g, out=d_out[:n], stream=st)
+                    solvers[k].reduce_noise(d_in[:n], g, out=d_out[:n], stream=st)
                     out[f0:f0 + n].copy_(d_out[:n], non_blocking=True)
+            done = []
+            for st in streams:
+                ev = torch.cuda.Event()
+                ev.record(st)
+                done.append(ev)
+            for ev in done:
+                cur.wait_event(ev)  # the caller's stream orders after the whole pipeline
             for st in streams:
                 st.synchronize()
+            if d_g is not None:
+                d_g.record_stream(cur)
         return out
 
     def solve_tiles(self, data, gamma, u0=None, stream=None):

@@ -53,6 +53,9 @@ FLOP_TRIAL = 2048
 FLOP_ITER_BASE = {"plain": 11264 + 1536 + 2304 + 2048, "plain_wg": 11264 + 1536 + 2304 + 2048,
                   "spectral": 17408 + 1536 + 2816 + 2048}
 FLOP_PER_PAIR = {"plain": 4 * 256 * 2, "plain_wg": 4 * 256 * 2, "spectral": 5 * 256 * 2}
+# multiply-adds x 2 of the warm-start network per 16x16 tile:
+# 256 px x 9 taps x (2*32 + 32*32 + 32*32 + 32*1)
+INFER_FLOP_PER_TILE = 2 * 256 * 9 * (2 * 32 + 32 * 32 + 32 * 32 + 32 * 1)
 KERNEL = {"plain": "ncs_warp_kernel", "plain_wg": "ncs_plain_kernel",
           "spectral": "ncs_spectral_kernel"}
 
@@ -368,31 +371,74 @@ def run_ours(args, world, rank, local):
     e2e_value = px * e2e_steps / (e2e_ms / 1e3) / 1e6
     assert torch.equal(h_out, out.cpu()), "e2e result differs from the device-resident run"
 
-    # the plain GPU form (the reference's L-BFGS: scalar initial matrix,
-    # Armijo backtracking, one warp per tile) on the same stack, for the
-    # "vs plain GPU" part of the metric
-    plain = None
-    if not args.no_compare_plain and args.form != "plain":
-        ps = ncs_b200.Solver(alpha=w["alpha"], max_iters=w["max_iters"], mode="plain", m=4)
-        ps.set_otf_mask(w["mask"])
-        _, p_it, p_st, p_cost = ps.reduce_noise(images, gamma, out=out, tile_stats=True)
-        ps.reduce_noise(images, gamma, out=out)
+    # the plain GPU forms (the reference's L-BFGS: scalar initial matrix,
+    # Armijo backtracking) on the same stack, for the "vs plain GPU" part of
+    # the metric: one warp group per tile (the reference kernel's layout) and
+    # one warp per tile (the faster plain kernel)
+    plain = {}
+    if not args.no_compare_plain and args.form == "spectral":
+        for pform in ("plain_wg", "plain"):
+            ps = ncs_b200.Solver(alpha=w["alpha"], max_iters=w["max_iters"], mode=pform, m=4)
+            ps.set_otf_mask(w["mask"])
+            _, p_it, p_st, p_cost = ps.reduce_noise(images, gamma, out=out, tile_stats=True)
+            ps.reduce_noise(images, gamma, out=out)
+            barrier(world)
+            torch.cuda.synchronize()
+            pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            nps = max(1, min(args.steps, 3))
+            pe0.record(stream)
+            for _ in range(nps):
+                ps.reduce_noise(images, gamma, out=out)
+            pe1.record(stream)
+            torch.cuda.synchronize()
+            p_ms = max_over_ranks(pe0.elapsed_time(pe1), world) / nps
+            plain[pform] = {"form": "%s (m=4)" % pform, "kernel": KERNEL[pform],
+                            "ms_per_step": p_ms,
+                            "value": px / (p_ms / 1e3) / 1e6,
+                            "mean_iters": p_it.double().mean().item(),
+                            "capped_tiles": int((p_st == -2).sum().item()),
+                            "speedup_of_form": p_ms / (total_ms / args.steps),
+                            "_cost": p_cost.cpu().numpy()}
+            ps.close()
+
+    # learned warm start: network inference on the stack, then the spectral
+    # solve from its proposals (fallback to the photon image per tile)
+    warm = None
+    from ncs_b200 import warmstart
+    if not args.no_warm_start and args.form == "spectral" and os.path.exists(
+            warmstart.DEFAULT_WEIGHTS):
+        net = warmstart.WarmStartNet.load()
+        u0 = net.propose_stack(images, gamma)
+        _, w_it, w_st, w_cost, w_ev, w_fb = solver.reduce_noise_from(images, gamma, u0, out=out)
         barrier(world)
         torch.cuda.synchronize()
-        pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        nps = max(1, min(args.steps, 3))
-        pe0.record(stream)
-        for _ in range(nps):
-            ps.reduce_noise(images, gamma, out=out)
-        pe1.record(stream)
+        nws = max(1, min(args.steps, 3))
+        we = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nws + 1)]
+        we[0].record(stream)
+        for k in range(nws):
+            net.propose_stack(images, gamma, out=u0)
+            we[2 * k + 1].record(stream)
+            solver.reduce_noise_from(images, gamma, u0, out=out)
+            we[2 * k + 2].record(stream)
         torch.cuda.synchronize()
-        p_ms = max_over_ranks(pe0.elapsed_time(pe1), world) / nps
-        plain = {"form": "plain (m=4)", "ms_per_step": p_ms,
-                 "value": px / (p_ms / 1e3) / 1e6, "mean_iters": p_it.double().mean().item(),
-                 "capped_tiles": int((p_st == -2).sum().item()),
-                 "speedup_of_form": p_ms / (total_ms / args.steps)}
-        p_cost_np = p_cost.cpu().numpy()
-        ps.close()
+        inf_ms = sum(we[2 * k].elapsed_time(we[2 * k + 1]) for k in range(nws)) / nws
+        sol_ms = sum(we[2 * k + 1].elapsed_time(we[2 * k + 2]) for k in range(nws)) / nws
+        tot_ms = max_over_ranks(we[0].elapsed_time(we[-1]), world) / nws
+        inf_flops = n_tiles * INFER_FLOP_PER_TILE
+        warm = {"network": "4 x conv3x3 2-32-32-32-1, ReLU, %d FP32 params"
+                           % warmstart.N_PARAMS,
+                "kernels": "ncsb::net::infer (FP32 SIMT), ncs_spectral_kernel<.., Warm>",
+                "ms_per_step": tot_ms, "ms_infer": inf_ms, "ms_solve": sol_ms,
+                "value": px / (tot_ms / 1e3) / 1e6,
+                "mean_iters": w_it.double().mean().item(),
+                "mean_iters_photon_start": iters_n / n_tiles,
+                "mean_evals": w_ev.double().mean().item(),
+                "fallback_frac": w_fb.double().mean().item(),
+                "infer_tflops": inf_flops / (inf_ms / 1e3) / 1e12,
+                "infer_flop_per_tile": INFER_FLOP_PER_TILE,
+                "speedup_vs_photon_start": (total_ms / args.steps) / tot_ms,
+                "_cost": w_cost.cpu().numpy()}
+        del u0
 
     pk, pk_src = peaks()
     n_sms = torch.cuda.get_device_properties(dev).multi_processor_count
@@ -434,8 +480,11 @@ def run_ours(args, world, rank, local):
         "gpu_launches": args.steps,
         "clocks": clk,
     }
-    if plain is not None:
-        line["plain_gpu"] = plain
+    for pform, rec in plain.items():
+        line["plain_gpu" if pform == "plain_wg" else "plain_gpu_warp"] = {
+            k: v for k, v in rec.items() if not k.startswith("_")}
+    if warm is not None:
+        line["warm_start"] = {k: v for k, v in warm.items() if not k.startswith("_")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         imgs = images.cpu().numpy()
@@ -448,10 +497,145 @@ def run_ours(args, world, rank, local):
             "sample": "%d of %d frames, one per thread, pyCNCS cReduceNoise FP64, "
                       "max_iterations=%d" % (n, T, w["max_iters"])}
         line["accuracy"] = accuracy_gate(w, cost.cpu().numpy(), args.accuracy_tiles)
-        if plain is not None:
-            line["plain_gpu"]["accuracy"] = accuracy_gate(w, p_cost_np, args.accuracy_tiles)
+        for pform, rec in plain.items():
+            key = "plain_gpu" if pform == "plain_wg" else "plain_gpu_warp"
+            line[key]["accuracy"] = accuracy_gate(w, rec["_cost"], args.accuracy_tiles)
+        if warm is not None:
+            line["warm_start"]["accuracy"] = accuracy_gate(w, warm["_cost"], args.accuracy_tiles)
     if rank == 0:
         print(json.dumps(line), flush=True)
+    return 0
+
+
+def mixed_accuracy(stacks, cost, n_sample, seed=0):
+    """accuracy_gate over a batch: a random sample of tiles across all stacks,
+    each judged against the FP64 optimum with its own stack's alpha and mask."""
+    from oracle import numpy_ref as nr
+    per, offs = [], [0]
+    for st in stacks:
+        T, H, W = st["images"].shape
+        per.append(len(nr.tile_origins(H)) * len(nr.tile_origins(W)))
+        offs.append(offs[-1] + T * per[-1])
+    rng = numpy.random.default_rng(seed)
+    idx = numpy.sort(rng.choice(offs[-1], size=min(n_sample, offs[-1]), replace=False))
+    gaps = []
+    for t in idx:
+        k = int(numpy.searchsorted(offs, t, side="right") - 1)
+        st = stacks[k]
+        f, rem = divmod(int(t - offs[k]), per[k])
+        H, W = st["images"].shape[1:]
+        ox, oy = nr.tile_origins(H), nr.tile_origins(W)
+        i, j = divmod(rem, len(oy))
+        im = numpy.pad(st["images"][f].cpu().numpy().astype(numpy.float64), 1, "edge")
+        g = st["gamma"].cpu().numpy().astype(numpy.float64)
+        g = numpy.pad(g if g.ndim == 2 else g[f], 1, "edge")
+        ms = numpy.fft.fftshift(st["mask"]).astype(numpy.float32).astype(numpy.float64)
+        _, fstar, _ = nr.newton_solve(im[None, ox[i]:ox[i] + 16, oy[j]:oy[j] + 16],
+                                      g[None, ox[i]:ox[i] + 16, oy[j]:oy[j] + 16], ms,
+                                      st["alpha"])
+        gaps.append(float(nr.rel_cost_gap(cost[t:t + 1], fstar)[0]))
+    gaps = numpy.array(gaps)
+    return {"tiles_checked": int(idx.size), "frac_within_1e-4": float((gaps <= 1e-4).mean()),
+            "max_rel_gap": float(gaps.max()), "median_rel_gap": float(numpy.median(gaps)),
+            "referee": "FP64 damped Newton (oracle/numpy_ref.py), per stack alpha and mask"}
+
+
+def run_mixed(args, world, rank, local):
+    """The mixed-workload batch: 64 stacks (own shape, alpha, mask) solved by
+    one batched launch captured in a CUDA graph, launch parameters chosen by
+    the autotuner.  One batch per rank (replicas)."""
+    import ncs_b200
+    from ncs_b200 import sim, tune
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stacks = sim.make_mixed(args.stacks, seed=4242 + rank, device=dev)
+    px = float(sum(st["images"].numel() for st in stacks))
+    solver = ncs_b200.Solver(max_iters=200)
+    outs = solver.batch_set(stacks)
+    stats = solver.batch_stats()
+    best, tried = tune.autotune(solver, lambda: solver.batch_reduce_noise(), tune.batch_key(solver))
+    solver.batch_reduce_noise(stats=stats)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        solver.batch_reduce_noise()
+    for _ in range(args.warmup):
+        graph.replay()
+    stream = torch.cuda.current_stream(dev)
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    total_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    value = sum_over_ranks(px, world) * args.steps / (total_ms / 1e3) / 1e6
+
+    # end to end: pinned host stacks in, one batched solve, results out (only
+    # when the host can pin both copies of the batch with room to spare)
+    import psutil
+    e2e = None
+    need = 2 * 4 * px
+    if psutil.virtual_memory().available > 3 * need:
+        h_in = [st["images"].cpu().pin_memory() for st in stacks]
+        h_out = [torch.empty_like(h).pin_memory() for h in h_in]
+        e2e_steps = max(1, min(args.steps, 3))
+        barrier(world)
+        torch.cuda.synchronize()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(e2e_steps):
+            for st, h in zip(stacks, h_in):
+                st["images"].copy_(h, non_blocking=True)
+            graph.replay()
+            for o, h in zip(outs, h_out):
+                h.copy_(o, non_blocking=True)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
+        e2e = {"value": sum_over_ranks(px, world) * e2e_steps / (e2e_ms / 1e3) / 1e6,
+               "unit": "Mpixel/s",
+               "h2d_bytes_per_step": int(sum(h.numel() * 4 for h in h_in)),
+               "d2h_bytes_per_step": int(sum(h.numel() * 4 for h in h_out)),
+               "api": "per-stack pinned copies + Solver.batch_reduce_noise (graph replay), "
+                      "one stream"}
+        del h_in, h_out
+    else:
+        e2e = {"value": None, "unit": "Mpixel/s", "h2d_bytes_per_step": 0,
+               "d2h_bytes_per_step": 0,
+               "skipped": "host RAM below 3x the %.1f GB of pinned copies" % (need / 1e9)}
+    sides = sorted({st["side"] for st in stacks})
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded chains or beads, sCMOS camera model)",
+        "config": {"workload": "mixed%d: %d stacks, sides %s, %d frames in all, own alpha "
+                               "U(0.05,0.5) / NA / wavelength / mask per stack, spectral form, "
+                               "one batched launch replayed from a CUDA graph"
+                               % (len(stacks), len(stacks), sides,
+                                  sum(st["T"] for st in stacks)),
+                   "pixels": px, "tiles": solver.batch_tiles, "autotuned": best,
+                   "parallelism": "replicas (one batch per rank)"},
+        "mean_iters": stats["iters"].double().mean().item(),
+        "status": {str(k): int((stats["status"] == k).sum()) for k in range(-5, 1)},
+        "autotune_ms": tried,
+        "e2e": e2e,
+        "gpu_launches": args.steps,
+        "clocks": clk,
+    }
+    if rank == 0:
+        line["accuracy"] = mixed_accuracy(stacks, stats["cost"].cpu().numpy(),
+                                          args.accuracy_tiles)
+        print(json.dumps(line), flush=True)
+    del graph
     return 0
 
 
@@ -466,8 +650,12 @@ def main():
     ap.add_argument("--form", default="spectral", choices=sorted(KERNEL))
     ap.add_argument("--no-compare-plain", action="store_true",
                     help="skip timing the plain form on the same stack")
+    ap.add_argument("--no-warm-start", action="store_true",
+                    help="skip the learned warm-start leg")
     ap.add_argument("--accuracy-tiles", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stacks", type=int, default=64,
+                    help="stacks in the mixed workload (--workload mixed)")
     args = ap.parse_args()
     if args.impl == "reference":
         # rank 0 alone times the CPU path; no process group is needed
@@ -475,6 +663,8 @@ def main():
                              int(os.environ.get("RANK", "0")))
     world, rank, local = dist_setup()
     try:
+        if args.workload == "mixed":
+            return run_mixed(args, world, rank, local)
         return run_ours(args, world, rank, local)
     finally:
         if world > 1:

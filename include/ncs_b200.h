@@ -126,11 +126,135 @@ int ncsb_reduce_noise(ncsb_handle *h, const float *images, int n_frames, int hei
  * Tile-level solve with the reference kernel's data layout: data_in and
  * gamma_in are [n_tiles][16][16] FP32 (gamma per tile, ncs.cu:931),
  * data_out [n_tiles][16][16]; iters / status / cost / evals optional [n_tiles].
- * u0 (optional, [n_tiles][16][16]) replaces the start u0 = data_in.
+ * u0 (optional, [n_tiles][16][16]) replaces the start u0 = data_in; in the
+ * spectral form a tile whose u0 has a higher cost than data_in starts at
+ * data_in (as in ncsb_reduce_noise_start).
  */
 int ncsb_solve_tiles(ncsb_handle *h, const float *data_in, const float *gamma_in,
                      const float *u0, int64_t n_tiles, float *data_out, int32_t *iters,
                      int32_t *status, double *cost, int32_t *evals, void *stream);
+
+/*
+ * ncsb_reduce_noise from a proposed start (the learned warm start; no
+ * counterpart in the reference, whose solve always starts at u = d,
+ * clib/pyCNCS/ncs.c:548-551, cuda/ncs.cu:933).  u0_tiles: [ncsb_num_tiles()][16][16] FP32,
+ * one proposal per tile in (frame, tile-row, tile-col) order, halo included,
+ * as ncsb_net_infer_stack writes it.  Each tile starts at its proposal unless
+ * the proposal's cost is higher than that of the photon image, in which case
+ * it starts at u = d exactly as ncsb_reduce_noise does; the stopping rule is
+ * unchanged.  tile_start (optional, [n_tiles]) receives 0 where the proposal
+ * was used and 1 where the tile fell back to the photon image.  Spectral form
+ * only (NCSB_EINVAL otherwise); other arguments as ncsb_reduce_noise.
+ */
+int ncsb_reduce_noise_start(ncsb_handle *h, const float *images, int n_frames, int height,
+                            int width, const float *gamma, int gamma_per_frame,
+                            const float *u0_tiles, float *out, int32_t *tile_iters,
+                            int32_t *tile_status, double *tile_cost, int32_t *tile_evals,
+                            int32_t *tile_start, void *stream);
+
+/* ---- batched launch: many stacks, one persistent queue -------------------
+ * No counterpart in the reference, which processes one stack per call with
+ * one alpha and one mask (cuda/pyCUDANCS/ncs.py:35-173).  Here several stacks
+ * -- each with its own shape, alpha and OTF mask -- are solved by one launch
+ * whose work queue spans all their tiles, so small stacks do not leave the GPU
+ * idle and a whole acquisition session is one kernel.  Spectral form only. */
+typedef struct {
+    const float *images;      /* device [n_frames][height][width] photo-electrons */
+    const float *gamma;       /* device [height][width] (gamma_per_frame == 0) or
+                                 [n_frames][height][width] */
+    float *out;               /* device [n_frames][height][width] */
+    int32_t n_frames, height, width, gamma_per_frame;
+    double alpha;             /* this stack's alpha */
+    float mask_shifted[256];  /* this stack's 16x16 OTF mask, DC at [0][0] (host values) */
+} ncsb_stack;
+
+#define NCSB_MAX_STACKS 65536
+
+/* Upload the descriptors of n_stacks stacks (1..NCSB_MAX_STACKS) to the
+ * handle: validation as ncsb_reduce_noise per stack (NCSB_ESIZE for frames
+ * under 14 x 14), per-stack mask tables, tile ranges.  Synchronous; allocates
+ * only when n_stacks exceeds the largest batch the handle has held.  The
+ * device buffers named in the descriptors must stay valid while the batch is
+ * launched. */
+int ncsb_batch_set(ncsb_handle *h, const ncsb_stack *stacks, int n_stacks);
+
+/* Total tiles of the current batch: the sum of ncsb_num_tiles() over its
+ * stacks, in stack order (the order of the per-tile outputs). */
+int ncsb_batch_num_tiles(const ncsb_handle *h, int64_t *n_tiles);
+
+/* Solve every tile of the current batch in one launch on `stream`: a counter
+ * reset and one kernel, nothing else, so the call can be captured into a CUDA
+ * graph and replayed (ncsb_batch_set must happen before the capture).
+ * u0_tiles (optional, [n_tiles][16][16]) gives proposed starts as in
+ * ncsb_reduce_noise_start, tile_start (optional) receives the fallback flags;
+ * tile_iters / tile_status / tile_cost / tile_evals are optional [n_tiles]. */
+int ncsb_batch_reduce_noise(ncsb_handle *h, const float *u0_tiles, int32_t *tile_iters,
+                            int32_t *tile_status, double *tile_cost, int32_t *tile_evals,
+                            int32_t *tile_start, void *stream);
+
+/* ---- learned warm start: a 4-layer 3x3 convolutional network ------------
+ * Maps each tile's photon image d and gamma map to a proposed start.  Input
+ * features per tile: x0 = (d - mu) / s, x1 = sqrt(max(d, 0) + gamma) / s with
+ * mu, s = mean and standard deviation + 1 of the tile's d; layers 2->32->32->32->1
+ * channels, 3x3 kernels with zero padding, ReLU after the first three; the
+ * proposal is u0 = d + s y.  No counterpart in the reference.
+ *
+ * Tensors are FP32 device buffers: activations [n][channels][16][16]; weights
+ * of a layer stored as wt[cin][3*ky + kx][cout] (ky, kx the kernel offsets
+ * -1..1 shifted by one), bias [cout].  The packed parameter vector of the
+ * whole network holds w1, b1, w2, b2, w3, b3, w4, b4 in that order
+ * (ncsb_net_param_count() floats).  All calls are asynchronous on `stream`. */
+int ncsb_net_param_count(void);
+
+/* y = conv3x3(x) + b (ReLU if relu), for (cin, cout) in {(2,32), (32,32),
+ * (32,1), (1,32)}; b may be NULL (zero bias).  One 16x16 image per tile. */
+int ncsb_net_conv_fwd(const float *x, const float *wt, const float *b, float *y, int n_tiles,
+                      int cin, int cout, int relu, void *stream);
+
+/* Weight and bias gradients of conv3x3, ACCUMULATED into dwt [cin][9][cout]
+ * and db [cout]: dwt += sum_tiles,pixels x (*) dy, db += sum dy.
+ * (cin, cout) in {(2,32), (32,32), (32,1)}. */
+int ncsb_net_conv_wgrad(const float *x, const float *dy, float *dwt, float *db, int n_tiles,
+                        int cin, int cout, void *stream);
+
+/* Weights of the input-gradient convolution: wf[cout][8 - tap][cin] =
+ * wt[cin][tap][cout], so that ncsb_net_conv_fwd(dy, wf, NULL, dx, n, cout,
+ * cin, 0) gives dx = conv3x3^T(dy). */
+int ncsb_net_flip(const float *wt, float *wf, int cin, int cout, void *stream);
+
+/* g[i] = 0 where act[i] <= 0 (ReLU backward through the layer output act). */
+int ncsb_net_relu_bwd(float *g, const float *act, int64_t n, void *stream);
+
+/* Mean squared error: g = 2 (y - t) / n, and loss[0] += mean((y - t)^2)
+ * (loss must be zeroed by the caller). */
+int ncsb_net_mse_grad(const float *y, const float *t, float *g, float *loss, int64_t n,
+                      void *stream);
+
+/* One Adam step (bias-corrected, step >= 1) over n parameters. */
+int ncsb_net_adam(float *w, const float *g, float *m, float *v, int64_t n, float lr, float b1,
+                  float b2, float eps, int step, void *stream);
+
+/* Network input features x [n][2][16][16] and per-tile (mu, s) scale [n][2]
+ * from tiles d, gamma [n][16][16]. */
+int ncsb_net_features(const float *d, const float *gamma, float *x, float *scale, int n_tiles,
+                      void *stream);
+
+/* Whole-network inference straight from a stack: cuts each tile (the
+ * solvers' segmentation) and writes the proposal u0_tiles
+ * [ncsb_num_tiles()][16][16] for ncsb_reduce_noise_start.  Proposals are
+ * kept feasible: u0 + gamma >= 0.05 max(d + gamma, 1e-3). */
+int ncsb_net_infer_stack(const float *params, const float *images, int n_frames, int height,
+                         int width, const float *gamma, int gamma_per_frame, float *u0_tiles,
+                         void *stream);
+
+/* The same inference over the handle's current batch (ncsb_batch_set):
+ * u0_tiles [ncsb_batch_num_tiles()][16][16] in the batch's tile order. */
+int ncsb_net_infer_batch(const float *params, const ncsb_handle *h, float *u0_tiles,
+                         void *stream);
+
+/* The same inference on tiles d, gamma [n][16][16] -> u0 [n][16][16]. */
+int ncsb_net_infer_tiles(const float *params, const float *d, const float *gamma, int64_t n_tiles,
+                         float *u0, void *stream);
 
 /*
  * ncsb_reduce_noise without a handle and without allocating device memory.

@@ -49,11 +49,32 @@ class NcsbParams(ctypes.Structure):
     ]
 
 
+class NcsbStack(ctypes.Structure):
+    """ncsb_stack: one stack of a batched launch."""
+    _fields_ = [
+        ("images", ctypes.c_void_p),
+        ("gamma", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("n_frames", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("gamma_per_frame", ctypes.c_int32),
+        ("alpha", ctypes.c_double),
+        ("mask_shifted", ctypes.c_float * 256),
+    ]
+
+
+MAX_STACKS = 65536
+
 # Every symbol include/ncs_b200.h declares (checked by the tests).
 EXPORTS = [
     "ncsb_default_params", "ncsb_create", "ncsb_set_params", "ncsb_destroy", "ncsb_last_error",
     "ncsb_set_otf_mask", "ncsb_num_tiles", "ncsb_reduce_noise", "ncsb_solve_tiles",
-    "ncsb_reduce_noise_noalloc",
+    "ncsb_reduce_noise_noalloc", "ncsb_reduce_noise_start",
+    "ncsb_net_param_count", "ncsb_net_conv_fwd", "ncsb_net_conv_wgrad", "ncsb_net_flip",
+    "ncsb_net_relu_bwd", "ncsb_net_mse_grad", "ncsb_net_adam", "ncsb_net_features",
+    "ncsb_net_infer_stack", "ncsb_net_infer_tiles", "ncsb_net_infer_batch",
+    "ncsb_batch_set", "ncsb_batch_num_tiles", "ncsb_batch_reduce_noise",
 ]
 
 _lib = None
@@ -92,6 +113,31 @@ def load():
                                               ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp,
                                               vp, vp, vp, vp, vp]
     lib.ncsb_reduce_noise_noalloc.restype = ctypes.c_int
+    lib.ncsb_reduce_noise_start.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
+                                            ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.ncsb_reduce_noise_start.restype = ctypes.c_int
+    ci, f32 = ctypes.c_int, ctypes.c_float
+    lib.ncsb_net_param_count.argtypes = []
+    lib.ncsb_net_conv_fwd.argtypes = [vp, vp, vp, vp, ci, ci, ci, ci, vp]
+    lib.ncsb_net_conv_wgrad.argtypes = [vp, vp, vp, vp, ci, ci, ci, vp]
+    lib.ncsb_net_flip.argtypes = [vp, vp, ci, ci, vp]
+    lib.ncsb_net_relu_bwd.argtypes = [vp, vp, i64, vp]
+    lib.ncsb_net_mse_grad.argtypes = [vp, vp, vp, vp, i64, vp]
+    lib.ncsb_net_adam.argtypes = [vp, vp, vp, vp, i64, f32, f32, f32, f32, ci, vp]
+    lib.ncsb_net_features.argtypes = [vp, vp, vp, vp, ci, vp]
+    lib.ncsb_net_infer_stack.argtypes = [vp, vp, ci, ci, ci, vp, ci, vp, vp]
+    lib.ncsb_net_infer_tiles.argtypes = [vp, vp, vp, i64, vp, vp]
+    lib.ncsb_net_infer_batch.argtypes = [vp, vp, vp, vp]
+    lib.ncsb_batch_set.argtypes = [vp, P(NcsbStack), ctypes.c_int]
+    lib.ncsb_batch_set.restype = ctypes.c_int
+    lib.ncsb_batch_num_tiles.argtypes = [vp, P(i64)]
+    lib.ncsb_batch_num_tiles.restype = ctypes.c_int
+    lib.ncsb_batch_reduce_noise.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.ncsb_batch_reduce_noise.restype = ctypes.c_int
+    for name in ("ncsb_net_infer_batch", "ncsb_net_param_count", "ncsb_net_conv_fwd", "ncsb_net_conv_wgrad",
+                 "ncsb_net_flip", "ncsb_net_relu_bwd", "ncsb_net_mse_grad", "ncsb_net_adam",
+                 "ncsb_net_features", "ncsb_net_infer_stack", "ncsb_net_infer_tiles"):
+        getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib
 

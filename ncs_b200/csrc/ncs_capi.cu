@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/ncs_b200.h"
 #include "ncs_internal.cuh"
@@ -17,7 +18,11 @@ int plain_max_ctas_per_sm();
 cudaError_t launch_warp_blocks(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
 int warp_max_ctas_per_sm(int m, int blocks);
 cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
-int spectral_max_ctas_per_sm(int m, int blocks);
+int spectral_max_ctas_per_sm(int m, int blocks, bool warm, bool batch);
+namespace net {
+int launch_infer_batch(const float* params, const StackDesc* stacks, int n_stacks,
+                       long long n_tiles, float* u0, cudaStream_t s);
+}  // namespace net
 }  // namespace ncsb
 
 struct ncsb_handle {
@@ -27,6 +32,13 @@ struct ncsb_handle {
     bool has_mask = false;
     float* d_msq = nullptr;                 // [256] M^2/256, kernel spectral layout
     unsigned long long* d_queue = nullptr;  // work counter
+    // batched launch (ncsb_batch_set): stack descriptors, per-stack lane-layout
+    // M^2/256 tables, capacity in stacks, current count and total tiles
+    ncsb::StackDesc* d_stacks = nullptr;
+    float* d_mk_lane = nullptr;
+    int batch_cap = 0;
+    int n_stacks = 0;
+    long long batch_tiles = 0;
     std::string err;
 };
 
@@ -52,6 +64,31 @@ int check_params(const ncsb_params* p, std::string* why) {
     if (p->mode != NCSB_MODE_PLAIN && p->mode != NCSB_MODE_PLAIN_WG && p->mode != NCSB_MODE_SPECTRAL) { *why = "unsupported mode"; return NCSB_EINVAL; }
     if (p->ctas_per_sm < 0) { *why = "ctas_per_sm must be >= 0"; return NCSB_EINVAL; }
     return NCSB_OK;
+}
+
+// Symmetrised M^2/256 in natural order [kr][kc] from a shifted 16x16 mask.
+// For real u the noise term only sees the symmetric part of M^2
+// (|U_k| = |U_-k|), and the kernels' real-output inverse transforms rely on
+// it; a mask passing checkOTFMask is unchanged.
+bool build_msq(const float* mask, float tab[256]) {
+    for (int i = 0; i < 16; ++i)
+        for (int j = 0; j < 16; ++j) {
+            const double a = mask[i * 16 + j], b = mask[((16 - i) & 15) * 16 + ((16 - j) & 15)];
+            if (!std::isfinite(a)) return false;
+            tab[i * 16 + j] = (float)(0.5 * (a * a + b * b) / 256.0);
+        }
+    return true;
+}
+
+int bitrev3_host(int i) { return ((i & 1) << 2) | (i & 2) | ((i & 4) >> 2); }
+
+// The spectral kernel's lane layout of the table: lane L holds, at positions
+// 8 L .. 8 L + 7, the values of its 8 spectral bins (ncs_spectral.cu).
+void lane_layout(const float nat[256], float* out) {
+    for (int idx = 0; idx < 256; ++idx) {
+        const int L = idx >> 3, i = idx & 7;
+        out[idx] = nat[(2 * bitrev3_host(i) + (L & 1)) * 16 + (L >> 1)];
+    }
 }
 
 int tiles_along(int n) {
@@ -82,7 +119,8 @@ int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s) {
     int per_sm = h->p.ctas_per_sm > 0
                      ? h->p.ctas_per_sm
                      : (wg ? ncsb::plain_max_ctas_per_sm()
-                           : (spec ? ncsb::spectral_max_ctas_per_sm(a.m, 0)
+                           : (spec ? ncsb::spectral_max_ctas_per_sm(a.m, 0, a.u0 != nullptr,
+                                                                   a.stacks != nullptr)
                                    : ncsb::warp_max_ctas_per_sm(a.m, 0)));
     // warp-per-tile CTAs hold 4 tiles at a time
     const long long tiles_per_cta = wg ? 1 : 4;
@@ -150,6 +188,8 @@ int ncsb_destroy(ncsb_handle* h) {
     if (!h) return NCSB_EINVAL;
     cudaFree(h->d_msq);
     cudaFree(h->d_queue);
+    cudaFree(h->d_stacks);
+    cudaFree(h->d_mk_lane);
     delete h;
     return NCSB_OK;
 }
@@ -159,21 +199,10 @@ const char* ncsb_last_error(const ncsb_handle* h) { return h ? h->err.c_str() : 
 int ncsb_set_otf_mask(ncsb_handle* h, const float* mask) {
     if (!h) return NCSB_EINVAL;
     if (!mask) return fail(h, NCSB_EINVAL, "mask is NULL");
-    // M^2, symmetrised over k -> -k: for real u the noise term only sees the
-    // symmetric part (|U_k| = |U_-k|), and the kernel's real-output inverse
-    // transform relies on it.  A mask passing checkOTFMask is unchanged.
-    double m2[16][16];
-    for (int i = 0; i < 16; ++i)
-        for (int j = 0; j < 16; ++j) {
-            const double a = mask[i * 16 + j], b = mask[((16 - i) & 15) * 16 + ((16 - j) & 15)];
-            if (!std::isfinite(a)) return fail(h, NCSB_EINVAL, "mask has a non-finite value");
-            m2[i][j] = 0.5 * (a * a + b * b);
-        }
-    // Natural order [kr][kc], scaled by 1/256; each kernel permutes it into
-    // its own spectral layout when a CTA starts.
+    // natural order [kr][kc], scaled by 1/256; each kernel permutes it into
+    // its own spectral layout when a CTA starts
     float tab[256];
-    for (int i = 0; i < 16; ++i)
-        for (int j = 0; j < 16; ++j) tab[i * 16 + j] = (float)(m2[i][j] / 256.0);
+    if (!build_msq(mask, tab)) return fail(h, NCSB_EINVAL, "mask has a non-finite value");
     cudaError_t e = cudaMemcpy(h->d_msq, tab, sizeof(tab), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpy(mask)");
     h->has_mask = true;
@@ -220,6 +249,42 @@ int ncsb_reduce_noise(ncsb_handle* h, const float* images, int n_frames, int hei
     return launch(h, a, (cudaStream_t)stream);
 }
 
+int ncsb_reduce_noise_start(ncsb_handle* h, const float* images, int n_frames, int height,
+                            int width, const float* gamma, int gamma_per_frame,
+                            const float* u0_tiles, float* out, int32_t* tile_iters,
+                            int32_t* tile_status, double* tile_cost, int32_t* tile_evals,
+                            int32_t* tile_start, void* stream) {
+    if (!h) return NCSB_EINVAL;
+    if (h->p.mode != NCSB_MODE_SPECTRAL)
+        return fail(h, NCSB_EINVAL, "a proposed start needs the spectral form");
+    if (!u0_tiles) return fail(h, NCSB_EINVAL, "null proposal");
+    if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
+    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
+    if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
+    if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
+        return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
+    if (n_frames == 0) return NCSB_OK;
+    ncsb::SolveArgs a{};
+    a.tile_mode = 0;
+    a.data = images;
+    a.gamma = gamma;
+    a.u0 = u0_tiles;
+    a.start = tile_start;
+    a.gamma_frame_stride = gamma_per_frame ? (long long)height * width : 0;
+    a.out = out;
+    a.T = n_frames;
+    a.H = height;
+    a.W = width;
+    a.tiles_x = tiles_along(height);
+    a.tiles_y = tiles_along(width);
+    a.n_tiles = (long long)n_frames * a.tiles_x * a.tiles_y;
+    a.iters = tile_iters;
+    a.status = tile_status;
+    a.cost = tile_cost;
+    a.evals = tile_evals;
+    return launch(h, a, (cudaStream_t)stream);
+}
+
 int ncsb_solve_tiles(ncsb_handle* h, const float* data_in, const float* gamma_in, const float* u0,
                      int64_t n_tiles, float* data_out, int32_t* iters, int32_t* status,
                      double* cost, int32_t* evals, void* stream) {
@@ -240,6 +305,102 @@ int ncsb_solve_tiles(ncsb_handle* h, const float* data_in, const float* gamma_in
     a.cost = cost;
     a.evals = evals;
     return launch(h, a, (cudaStream_t)stream);
+}
+
+int ncsb_batch_set(ncsb_handle* h, const ncsb_stack* stacks, int n_stacks) {
+    if (!h) return NCSB_EINVAL;
+    if (!stacks || n_stacks < 1 || n_stacks > NCSB_MAX_STACKS)
+        return fail(h, NCSB_EINVAL, "need 1..NCSB_MAX_STACKS stacks");
+    std::vector<ncsb::StackDesc> desc(n_stacks);
+    std::vector<float> mk((size_t)n_stacks * 256);
+    long long total = 0;
+    for (int i = 0; i < n_stacks; ++i) {
+        const ncsb_stack& st = stacks[i];
+        const std::string at = "stack " + std::to_string(i) + ": ";
+        if (!st.images || !st.gamma || !st.out) return fail(h, NCSB_EINVAL, at + "null buffer");
+        if (st.n_frames < 1 || st.height <= 0 || st.width <= 0)
+            return fail(h, NCSB_EINVAL, at + "bad shape");
+        if (st.height < NCSB_TILE - 2 || st.width < NCSB_TILE - 2)
+            return fail(h, NCSB_ESIZE, at + "frames must be at least 14 x 14");
+        if (!std::isfinite(st.alpha) || st.alpha < 0.0)
+            return fail(h, NCSB_EINVAL, at + "alpha must be finite and >= 0");
+        float nat[256];
+        if (!build_msq(st.mask_shifted, nat)) return fail(h, NCSB_EINVAL, at + "non-finite mask");
+        lane_layout(nat, mk.data() + (size_t)i * 256);
+        ncsb::StackDesc& d = desc[i];
+        d.data = st.images;
+        d.gamma = st.gamma;
+        d.out = st.out;
+        d.gamma_frame_stride = st.gamma_per_frame ? (long long)st.height * st.width : 0;
+        d.tile_begin = total;
+        d.T = st.n_frames;
+        d.H = st.height;
+        d.W = st.width;
+        d.tiles_x = tiles_along(st.height);
+        d.tiles_y = tiles_along(st.width);
+        d.alpha = (float)st.alpha;
+        total += (long long)st.n_frames * d.tiles_x * d.tiles_y;
+    }
+    cudaError_t e = cudaSuccess;
+    if (n_stacks > h->batch_cap) {
+        cudaFree(h->d_stacks);
+        cudaFree(h->d_mk_lane);
+        h->d_stacks = nullptr;
+        h->d_mk_lane = nullptr;
+        h->batch_cap = 0;
+        h->n_stacks = 0;
+        e = cudaMalloc(&h->d_stacks, sizeof(ncsb::StackDesc) * n_stacks);
+        if (e == cudaSuccess) e = cudaMalloc(&h->d_mk_lane, sizeof(float) * 256 * n_stacks);
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc(batch)");
+        h->batch_cap = n_stacks;
+    }
+    e = cudaMemcpy(h->d_stacks, desc.data(), sizeof(ncsb::StackDesc) * n_stacks,
+                   cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(h->d_mk_lane, mk.data(), sizeof(float) * mk.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpy(batch)");
+    h->n_stacks = n_stacks;
+    h->batch_tiles = total;
+    // resolve the kernel variants' attributes now, outside any stream capture
+    ncsb::spectral_max_ctas_per_sm(h->p.m, 0, false, true);
+    ncsb::spectral_max_ctas_per_sm(h->p.m, 0, true, true);
+    return NCSB_OK;
+}
+
+int ncsb_batch_num_tiles(const ncsb_handle* h, int64_t* n_tiles) {
+    if (!h || !n_tiles) return NCSB_EINVAL;
+    *n_tiles = h->batch_tiles;
+    return NCSB_OK;
+}
+
+int ncsb_batch_reduce_noise(ncsb_handle* h, const float* u0_tiles, int32_t* tile_iters,
+                            int32_t* tile_status, double* tile_cost, int32_t* tile_evals,
+                            int32_t* tile_start, void* stream) {
+    if (!h) return NCSB_EINVAL;
+    if (h->p.mode != NCSB_MODE_SPECTRAL)
+        return fail(h, NCSB_EINVAL, "batched launches need the spectral form");
+    if (h->n_stacks < 1) return fail(h, NCSB_EINVAL, "call ncsb_batch_set first");
+    ncsb::SolveArgs a{};
+    a.tile_mode = 0;
+    a.stacks = h->d_stacks;
+    a.n_stacks = h->n_stacks;
+    a.mk_lane = h->d_mk_lane;
+    a.u0 = u0_tiles;
+    a.start = tile_start;
+    a.n_tiles = h->batch_tiles;
+    a.iters = tile_iters;
+    a.status = tile_status;
+    a.cost = tile_cost;
+    a.evals = tile_evals;
+    return launch(h, a, (cudaStream_t)stream);
+}
+
+int ncsb_net_infer_batch(const float* params, const ncsb_handle* h, float* u0_tiles,
+                         void* stream) {
+    if (!params || !h || !u0_tiles) return NCSB_EINVAL;
+    if (h->n_stacks < 1) return NCSB_EINVAL;
+    return ncsb::net::launch_infer_batch(params, h->d_stacks, h->n_stacks, h->batch_tiles,
+                                         u0_tiles, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -28,12 +28,25 @@ enum Status : int32_t {
     kReachedMaxPrecision = -5,
 };
 
+// One stack of a batched launch (device copy of ncsb_stack plus its tile
+// range).  Field names match SolveArgs so kernels read either the same way.
+struct StackDesc {
+    const float* data;             // [T][H][W]
+    const float* gamma;            // [H][W] or [T][H][W]
+    float* out;                    // [T][H][W]
+    long long gamma_frame_stride;  // 0 or H*W
+    long long tile_begin;          // first tile of this stack in the batch's order
+    int T, H, W, tiles_x, tiles_y;
+    float alpha;
+};
+
 // Launch description shared by every solver form.
 struct SolveArgs {
     int tile_mode;                 // 0: stack in / stack out, 1: tiles in / tiles out
     const float* data;             // stack [T][H][W] or tiles [N][256]
     const float* gamma;            // [H][W], [T][H][W] or tiles [N][256]
-    const float* u0;               // optional start, tile mode only [N][256]
+    const float* u0;               // optional proposed start [N][256] (tile order)
+    int32_t* start;                // optional [N]: 1 = proposal rejected, solve from d
     long long gamma_frame_stride;  // stack mode: 0 (shared map) or H*W
     float* out;                    // stack [T][H][W] or tiles [N][256]
     int T, H, W;
@@ -47,6 +60,11 @@ struct SolveArgs {
     const float* msq;              // [256] M^2/256, natural order [kr][kc], symmetrised
     float alpha, eps, c1, min_step;
     int max_iters, m;
+    // batched launch (spectral form): n_stacks descriptors sorted by
+    // tile_begin, and per stack the M^2/256 table in the kernel's lane layout
+    const StackDesc* stacks;
+    int n_stacks;
+    const float* mk_lane;          // [n_stacks][256]
 };
 
 __device__ __forceinline__ int bitrev4(int v) {

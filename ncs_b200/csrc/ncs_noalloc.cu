@@ -26,7 +26,7 @@ int plain_max_ctas_per_sm();
 cudaError_t launch_warp(const SolveArgs& args, int grid, cudaStream_t stream);
 int warp_max_ctas_per_sm(int m);
 cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
-int spectral_max_ctas_per_sm(int m, int blocks);
+int spectral_max_ctas_per_sm(int m, int blocks, bool warm, bool batch);
 }  // namespace ncsb
 
 namespace {
@@ -164,7 +164,7 @@ extern "C" int ncsb_reduce_noise_noalloc(const ncsb_params* p, const float* mask
     const int per_sm = p->ctas_per_sm > 0
                            ? p->ctas_per_sm
                            : (wg ? dev->ctas_per_sm
-                                 : (spec ? ncsb::spectral_max_ctas_per_sm(a.m, 0)
+                                 : (spec ? ncsb::spectral_max_ctas_per_sm(a.m, 0, false, false)
                                          : ncsb::warp_max_ctas_per_sm(a.m)));
     const long long tiles_per_cta = wg ? 1 : 4;
     long long grid = (long long)per_sm * dev->num_sms;

@@ -24,6 +24,12 @@
 // rule stitching -- is that of the other solvers.  The first trial step is 1
 // (H0 has the right scale); the reference's first step 1/||g||
 // (ncs.cu:980-984) compensates for an identity start.
+//
+// Proposed start (a.u0, tile or stack mode): the first pass transforms the
+// proposal, a second one the photon image d, and the solve starts from
+// whichever has the lower cost, so a proposal never makes a tile start worse
+// than the reference's u = d; the photon-image start is then bit-identical to
+// a solve without a proposal.
 #include "ncs_warp_common.cuh"
 
 namespace ncsb {
@@ -37,9 +43,32 @@ __host__ __device__ constexpr size_t spec_warp_bytes(int m) {
     return ((sizeof(WarpSmem) + 15) / 16) * 16 + 3 * (size_t)m * 32 * 2 * sizeof(float4);
 }
 
+// Per-stack pointers and geometry: the kernel parameters of a single-stack
+// launch, or the warp's current stack descriptor of a batched one.
+struct Geo {
+    const float* data;
+    const float* gamma;
+    float* out;
+    long long gstride;
+    int H, W, tiles_x, tiles_y;
+};
+
+template <bool Batch>
+__device__ __forceinline__ Geo geo_of(const SolveArgs& a, const StackDesc& sd) {
+    if constexpr (Batch)
+        return Geo{sd.data, sd.gamma, sd.out, sd.gamma_frame_stride, sd.H, sd.W, sd.tiles_x,
+                   sd.tiles_y};
+    else
+        return Geo{a.data, a.gamma, a.out, a.gamma_frame_stride, a.H, a.W, a.tiles_x, a.tiles_y};
+}
+
 }  // namespace
 
-template <int MinBlocks, int MaxM>
+// Warm: the launch carries proposals (a.u0); the cold variant compiles
+// without the start passes.  Batch: tiles of several stacks (own alpha and
+// mask each, a.stacks) share one queue; a tile's stack is found by binary
+// search over the stacks' first tiles.
+template <int MinBlocks, int MaxM, bool Warm, bool Batch>
 __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kernel(const SolveArgs a) {
     static_assert(MaxM >= 1 && MaxM <= kMaxM, "history capacity");
     extern __shared__ __align__(16) unsigned char dsm[];
@@ -52,27 +81,47 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
     float4* hy = hs + (size_t)mcap * 64;
     float4* hq = hy + (size_t)mcap * 64;
 
-    for (int idx = threadIdx.x; idx < 256; idx += blockDim.x) {
-        const int L = idx >> 3, i = idx & 7;
-        mtab[idx] = a.msq[(2 * bitrev3(i) + (L & 1)) * 16 + (L >> 1)];
-    }
-    __syncthreads();
+    __shared__ StackDesc sdesc[kWarps];  // Batch: each warp's current stack
     const LaneGeo G = lane_geo(lane);
     float mk[8];  // M^2/256 at this lane's 8 spectral positions
-    {
+    float alpha = a.alpha, two_alpha = 2.0f * a.alpha, two_alpha_256 = 512.0f * a.alpha;
+    if constexpr (!Batch) {
+        for (int idx = threadIdx.x; idx < 256; idx += blockDim.x) {
+            const int L = idx >> 3, i = idx & 7;
+            mtab[idx] = a.msq[(2 * bitrev3(i) + (L & 1)) * 16 + (L >> 1)];
+        }
+        __syncthreads();
         const float4 m0 = *reinterpret_cast<const float4*>(mtab + lane * 8);
         const float4 m1 = *reinterpret_cast<const float4*>(mtab + lane * 8 + 4);
         mk[0] = m0.x; mk[1] = m0.y; mk[2] = m0.z; mk[3] = m0.w;
         mk[4] = m1.x; mk[5] = m1.y; mk[6] = m1.z; mk[7] = m1.w;
     }
-    const float alpha = a.alpha, two_alpha = 2.0f * a.alpha;
-    const float two_alpha_256 = 512.0f * a.alpha;
 
     for (;;) {
         unsigned long long tk = 0;
         if (lane == 0) tk = atomicAdd(a.queue, 1ull);
         const long long tile = (long long)__shfl_sync(kFull, tk, 0);
         if (tile >= a.n_tiles) break;
+        long long lt = tile;  // index of the tile within its stack
+        if constexpr (Batch) {
+            int lo = 0, hi = a.n_stacks - 1;
+            while (lo < hi) {  // last stack whose first tile is <= tile
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(&a.stacks[mid].tile_begin) <= tile) lo = mid;
+                else hi = mid - 1;
+            }
+            __syncwarp();  // every lane is done with the previous tile's descriptor
+            if (lane == 0) sdesc[wid] = a.stacks[lo];
+            __syncwarp();
+            lt = tile - sdesc[wid].tile_begin;
+            alpha = sdesc[wid].alpha;
+            two_alpha = 2.0f * alpha;
+            two_alpha_256 = 512.0f * alpha;
+            const float4* mt = reinterpret_cast<const float4*>(a.mk_lane + (size_t)lo * 256) + lane * 2;
+            const float4 m0 = __ldg(mt), m1 = __ldg(mt + 1);
+            mk[0] = m0.x; mk[1] = m0.y; mk[2] = m0.z; mk[3] = m0.w;
+            mk[4] = m1.x; mk[5] = m1.y; mk[6] = m1.z; mk[7] = m1.w;
+        }
 
         // ---- gather the tile (segmentation, ncs.c:66-113) ---------------------
         float d[8], gm[8], u[8];
@@ -86,31 +135,63 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     const int off = (G.P + 8 * s) * kTile + G.Qd + 4 * j;
                     d[2 * j + s] = __ldg(a.data + base + off);
                     gm[2 * j + s] = __ldg(a.gamma + base + off);
-                    u[2 * j + s] = a.u0 ? __ldg(a.u0 + base + off) : d[2 * j + s];
+                    u[2 * j + s] = Warm ? __ldg(a.u0 + base + off) : d[2 * j + s];
                 }
         } else {
-            const long long per_frame = (long long)a.tiles_x * a.tiles_y;
-            f = (int)(tile / per_frame);
-            const int rem = (int)(tile - (long long)f * per_frame);
-            const int ti = rem / a.tiles_y, tj = rem - (rem / a.tiles_y) * a.tiles_y;
-            ox = tile_origin(ti, a.H);
-            oy = tile_origin(tj, a.W);
-            own_r = (ti + 1 < a.tiles_x ? tile_origin(ti + 1, a.H) : ox + 14) - ox;
-            own_c = (tj + 1 < a.tiles_y ? tile_origin(tj + 1, a.W) : oy + 14) - oy;
-            const float* img = a.data + (long long)f * a.H * a.W;
-            const float* gmap = a.gamma + (long long)f * a.gamma_frame_stride;
+            const Geo sg = geo_of<Batch>(a, sdesc[wid]);
+            const long long per_frame = (long long)sg.tiles_x * sg.tiles_y;
+            f = (int)(lt / per_frame);
+            const int rem = (int)(lt - (long long)f * per_frame);
+            const int ti = rem / sg.tiles_y, tj = rem - (rem / sg.tiles_y) * sg.tiles_y;
+            ox = tile_origin(ti, sg.H);
+            oy = tile_origin(tj, sg.W);
+            own_r = (ti + 1 < sg.tiles_x ? tile_origin(ti + 1, sg.H) : ox + 14) - ox;
+            own_c = (tj + 1 < sg.tiles_y ? tile_origin(tj + 1, sg.W) : oy + 14) - oy;
+            const float* img = sg.data + (long long)f * sg.H * sg.W;
+            const float* gmap = sg.gamma + (long long)f * sg.gstride;
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
-                const long long row = clampi(ox + G.P + 8 * s - 1, 0, a.H - 1);
+                const long long row = clampi(ox + G.P + 8 * s - 1, 0, sg.H - 1);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const int col = clampi(oy + G.Qd + 4 * j - 1, 0, a.W - 1);
-                    d[2 * j + s] = __ldg(img + row * a.W + col);
-                    gm[2 * j + s] = __ldg(gmap + row * a.W + col);
+                    const int col = clampi(oy + G.Qd + 4 * j - 1, 0, sg.W - 1);
+                    d[2 * j + s] = __ldg(img + row * sg.W + col);
+                    gm[2 * j + s] = __ldg(gmap + row * sg.W + col);
                     u[2 * j + s] = d[2 * j + s];
                 }
             }
+            if (Warm) {
+                const float* ut = a.u0 + tile * kPix;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int s = 0; s < 2; ++s)
+                        u[2 * j + s] = __ldg(ut + (G.P + 8 * s) * kTile + G.Qd + 4 * j);
+            }
         }
+        // the photon image again, for the start passes of a proposed start
+        // (re-read rather than kept in registers through the solve)
+        auto load_d = [&](float (&dst)[8]) {
+            if (a.tile_mode) {
+                const float* dt = a.data + tile * kPix;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int s = 0; s < 2; ++s)
+                        dst[2 * j + s] = __ldg(dt + (G.P + 8 * s) * kTile + G.Qd + 4 * j);
+            } else {
+                const Geo sg = geo_of<Batch>(a, sdesc[wid]);
+                const float* img = sg.data + (long long)f * sg.H * sg.W;
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const long long row = clampi(ox + G.P + 8 * s - 1, 0, sg.H - 1);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        dst[2 * j + s] =
+                            __ldg(img + row * sg.W + clampi(oy + G.Qd + 4 * j - 1, 0, sg.W - 1));
+                }
+            }
+        };
         float c[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) c[i] = d[i] + gm[i];
@@ -123,13 +204,20 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
         int status = kUnstarted, iters = 0, evals = 1, k = 0, newest = -1;
         float lam = 1.0f;
         bool first = true;
+        // start passes left: 2 = transform the proposal, then 1 = the photon image
+        int start_pass = Warm ? 2 : 0;
+        int fell_back = 0;
 
         for (;;) {
             if (!first && iters >= a.max_iters) { status = kReachedMaxIters; break; }
             float q[8];
             if (first) {
+                if (start_pass == 1) {
+                    load_d(q);
+                } else {
 #pragma unroll
-                for (int i = 0; i < 8; ++i) q[i] = u[i];
+                    for (int i = 0; i < 8; ++i) q[i] = u[i];
+                }
             } else {
                 // two-loop, first half (newest pair first)
 #pragma unroll
@@ -175,6 +263,39 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 }
             }
             if (first) {
+                if (start_pass == 2) {  // keep Q u0, transform d next
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) w[i] = p[i];
+                    start_pass = 1;
+                    continue;
+                }
+                if (start_pass == 1) {
+                    // f(u0) - f(d) = sum[(u0 - d) - c (log(u0 + gamma) - log(d + gamma))]
+                    //                + alpha (u0'Q u0 - d'Q d);  p = Q d, w = Q u0
+                    float dd[8];
+                    load_d(dd);
+                    float dl = 0.0f, dq = 0.0f;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        // explicitly rounded operations: an FMA contraction of
+                        // the two logs' scalings, or of the two products, would
+                        // leave a rounding residue instead of 0 when u0 = d
+                        const float lr = __fsub_rn(__logf(fmaxf(u[i] + gm[i], kFitMin)),
+                                                   __logf(fmaxf(dd[i] + gm[i], kFitMin)));
+                        dl += fmaf(-c[i], lr, u[i] - dd[i]);
+                        dq += __fsub_rn(__fmul_rn(u[i], w[i]), __fmul_rn(dd[i], p[i]));
+                    }
+                    const double delta = warp_sum_d((double)dl + (double)alpha * (double)dq);
+                    if (delta <= 0.0) {
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) p[i] = w[i];
+                    } else {
+                        fell_back = 1;
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) u[i] = dd[i];
+                    }
+                    start_pass = 0;
+                }
                 first = false;
                 float uu = 0.0f, gg = 0.0f, ll = 0.0f;
 #pragma unroll
@@ -323,6 +444,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             if (a.iters) a.iters[tile] = iters;
             if (a.status) a.status[tile] = status;
             if (a.evals) a.evals[tile] = evals;
+            if (Warm && a.start) a.start[tile] = fell_back;
         }
         if (a.tile_mode) {
             const long long base = tile * kPix;
@@ -332,7 +454,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 for (int s = 0; s < 2; ++s)
                     a.out[base + (G.P + 8 * s) * kTile + G.Qd + 4 * j] = u[2 * j + s];
         } else {
-            float* o = a.out + (long long)f * a.H * a.W;
+            const Geo sg = geo_of<Batch>(a, sdesc[wid]);
+            float* o = sg.out + (long long)f * sg.H * sg.W;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int cc = G.Qd + 4 * j;
@@ -341,7 +464,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 for (int s = 0; s < 2; ++s) {
                     const int rr = G.P + 8 * s;
                     if (rr >= 1 && rr <= own_r)
-                        o[(long long)(ox + rr - 1) * a.W + oy + cc - 1] = u[2 * j + s];
+                        o[(long long)(ox + rr - 1) * sg.W + oy + cc - 1] = u[2 * j + s];
                 }
             }
         }
@@ -358,16 +481,21 @@ size_t spectral_smem_bytes(int m) {
 }
 
 template <int MaxM>
-KernelFn spectral_variant_m(int blocks) {
+KernelFn spectral_variant_m(int blocks, bool warm, bool batch) {
+    // proposals and batches: the default grid only
+    if (batch) return warm ? ncs_spectral_kernel<3, MaxM, true, true>
+                           : ncs_spectral_kernel<3, MaxM, false, true>;
+    if (warm) return ncs_spectral_kernel<3, MaxM, true, false>;
     switch (blocks <= 3 ? 3 : (blocks >= 5 ? 5 : blocks)) {
-        case 3: return ncs_spectral_kernel<3, MaxM>;
-        case 4: return ncs_spectral_kernel<4, MaxM>;
-        default: return ncs_spectral_kernel<5, MaxM>;
+        case 3: return ncs_spectral_kernel<3, MaxM, false, false>;
+        case 4: return ncs_spectral_kernel<4, MaxM, false, false>;
+        default: return ncs_spectral_kernel<5, MaxM, false, false>;
     }
 }
 
-KernelFn spectral_variant(int blocks, int m) {
-    return m <= 2 ? spectral_variant_m<2>(blocks) : spectral_variant_m<4>(blocks);
+KernelFn spectral_variant(int blocks, int m, bool warm, bool batch) {
+    return m <= 2 ? spectral_variant_m<2>(blocks, warm, batch)
+                  : spectral_variant_m<4>(blocks, warm, batch);
 }
 
 int spectral_default_blocks(int m) {
@@ -386,16 +514,18 @@ int spectral_default_blocks(int m) {
 
 cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream) {
     const size_t smem = spectral_smem_bytes(args.m);
-    const KernelFn fn = spectral_variant(blocks > 0 ? blocks : spectral_default_blocks(args.m), args.m);
+    const KernelFn fn = spectral_variant(blocks > 0 ? blocks : spectral_default_blocks(args.m), args.m,
+                                         args.u0 != nullptr, args.stacks != nullptr);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     fn<<<grid, kWarpCtaThreads, smem, stream>>>(args);
     return cudaGetLastError();
 }
 
-int spectral_max_ctas_per_sm(int m, int blocks) {
+int spectral_max_ctas_per_sm(int m, int blocks, bool warm, bool batch) {
     const size_t smem = spectral_smem_bytes(m);
-    const KernelFn fn = spectral_variant(blocks > 0 ? blocks : spectral_default_blocks(m), m);
+    const KernelFn fn =
+        spectral_variant(blocks > 0 ? blocks : spectral_default_blocks(m), m, warm, batch);
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return 1;

@@ -156,6 +156,114 @@ class Solver:
             return out, iters, status, cost
         return out
 
+    def reduce_noise_from(self, images, gamma, u0_tiles, out=None, stream=None):
+        """reduce_noise starting each tile at a proposal (spectral form only).
+
+        ``u0_tiles`` is [n_tiles, 16, 16] in (frame, tile-row, tile-col) order
+        (``WarmStartNet.propose_stack``).  A tile whose proposal costs more
+        than its photon image starts at the photon image instead.  Returns
+        (out, iters, status, cost, evals, fell_back) with the per-tile arrays
+        on the device; fell_back is 1 where the photon-image start was used."""
+        images = self._tensor(images, "images")
+        T, H, W = images.shape
+        gamma = self._tensor(gamma, "gamma")
+        if gamma.shape == (H, W):
+            per_frame = 0
+        elif gamma.shape == (T, H, W):
+            per_frame = 1
+        else:
+            raise ValueError("gamma must be [H, W] or [T, H, W]")
+        n = self.num_tiles(T, H, W)
+        u0_tiles = self._tensor(u0_tiles, "u0_tiles", (n, 16, 16))
+        out = torch.empty_like(images) if out is None else self._tensor(out, "out", (T, H, W))
+        iters = torch.empty(n, dtype=torch.int32, device=self.device)
+        status = torch.empty(n, dtype=torch.int32, device=self.device)
+        cost = torch.empty(n, dtype=torch.float64, device=self.device)
+        evals = torch.empty(n, dtype=torch.int32, device=self.device)
+        start = torch.empty(n, dtype=torch.int32, device=self.device)
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_reduce_noise_start(
+                self._handle, _ptr(images), T, H, W, _ptr(gamma), per_frame, _ptr(u0_tiles),
+                _ptr(out), _ptr(iters), _ptr(status), _ptr(cost), _ptr(evals), _ptr(start),
+                ctypes.c_void_p(s.cuda_stream)))
+        return out, iters, status, cost, evals, start
+
+    # ---- batched launch: many stacks, each with its own alpha and mask ------
+    def batch_set(self, stacks):
+        """Register a batch of stacks for ``batch_reduce_noise``.  ``stacks`` is
+        a sequence of dicts with ``images`` [T, H, W] and ``gamma`` ([H, W] or
+        [T, H, W]) float32 CUDA tensors, ``alpha``, and ``mask`` (centred
+        16 x 16) or ``mask_shifted``; ``out`` (optional) receives the result
+        (allocated here otherwise).  Returns the list of output tensors.  The
+        tensors must stay alive while the batch is launched."""
+        n = len(stacks)
+        if not 1 <= n <= _lib.MAX_STACKS:
+            raise ValueError("need 1..%d stacks" % _lib.MAX_STACKS)
+        arr = (_lib.NcsbStack * n)()
+        keep, outs = [], []
+        for i, st in enumerate(stacks):
+            images = self._tensor(st["images"], "images")
+            if images.dim() == 2:
+                images = images.unsqueeze(0)
+            T, H, W = images.shape
+            gamma = self._tensor(st["gamma"], "gamma")
+            if gamma.shape == (H, W):
+                per_frame = 0
+            elif gamma.shape == (T, H, W):
+                per_frame = 1
+            else:
+                raise ValueError("stack %d: gamma must be [H, W] or [T, H, W]" % i)
+            out = st.get("out")
+            out = torch.empty_like(images) if out is None else self._tensor(out, "out", (T, H, W))
+            if "mask_shifted" in st:
+                ms = numpy.asarray(st["mask_shifted"], dtype=numpy.float32)
+            else:
+                ms = numpy.fft.fftshift(numpy.asarray(st["mask"])).astype(numpy.float32)
+            if ms.shape != (16, 16):
+                raise ValueError("stack %d: OTF mask must be 16 x 16" % i)
+            a = arr[i]
+            a.images, a.gamma, a.out = images.data_ptr(), gamma.data_ptr(), out.data_ptr()
+            a.n_frames, a.height, a.width, a.gamma_per_frame = T, H, W, per_frame
+            a.alpha = float(st["alpha"])
+            ctypes.memmove(a.mask_shifted, numpy.ascontiguousarray(ms).ctypes.data, 1024)
+            keep.append((images, gamma, out))
+            outs.append(out)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_batch_set(self._handle, arr, n))
+        self._batch = keep
+        n_tiles = ctypes.c_int64(0)
+        self._check(self.lib.ncsb_batch_num_tiles(self._handle, ctypes.byref(n_tiles)))
+        self.batch_tiles = n_tiles.value
+        return outs
+
+    def batch_reduce_noise(self, u0_tiles=None, stats=None, stream=None):
+        """Solve the registered batch in one launch.  ``u0_tiles`` (optional,
+        [batch_tiles, 16, 16]) are proposed starts; ``stats`` (optional) is a
+        dict of preallocated per-tile device tensors with keys among iters,
+        status, evals, start (int32) and cost (float64).  Only a counter reset
+        and one kernel are issued, so the call can be captured in a CUDA
+        graph."""
+        if getattr(self, "_batch", None) is None:
+            raise RuntimeError("call batch_set first")
+        if u0_tiles is not None:
+            u0_tiles = self._tensor(u0_tiles, "u0_tiles", (self.batch_tiles, 16, 16))
+        st = stats or {}
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_batch_reduce_noise(
+                self._handle, _ptr(u0_tiles), _ptr(st.get("iters")), _ptr(st.get("status")),
+                _ptr(st.get("cost")), _ptr(st.get("evals")), _ptr(st.get("start")),
+                ctypes.c_void_p(s.cuda_stream)))
+
+    def batch_stats(self):
+        """Per-tile device tensors sized for the registered batch."""
+        n = self.batch_tiles
+        i32 = dict(dtype=torch.int32, device=self.device)
+        return {"iters": torch.empty(n, **i32), "status": torch.empty(n, **i32),
+                "evals": torch.empty(n, **i32), "start": torch.empty(n, **i32),
+                "cost": torch.empty(n, dtype=torch.float64, device=self.device)}
+
     def reduce_noise_host(self, images, gamma, out=None, chunk_frames=None, n_streams=3):
         """Host stack in, host stack out, with the copies hidden behind the solve.
 

@@ -54,11 +54,12 @@ def wlc_emitters(n_chains, field, rng, lp=2.0, length=(5.0, 10.0), spacing=0.02)
 
 def render(emitters_px, H, W, sigma_px, photons, bg, half=5):
     """bg + photons * pixel-integrated Gaussian PSF at each emitter (px units,
-    pixel i spans [i, i+1))."""
+    pixel i spans [i, i+1)); ``photons`` is a scalar or one value per emitter."""
     from scipy.special import erf
     img = numpy.full((H, W), float(bg))
     s2 = math.sqrt(2.0) * sigma_px
-    for x, y in emitters_px:  # x along W (columns), y along H (rows)
+    ph = numpy.broadcast_to(numpy.asarray(photons, dtype=numpy.float64), (len(emitters_px),))
+    for (x, y), photons in zip(emitters_px, ph):  # x along W (columns), y along H (rows)
         cx, cy = int(math.floor(x)), int(math.floor(y))
         cols = numpy.arange(cx - half, cx + half + 1)
         rows = numpy.arange(cy - half, cy + half + 1)
@@ -82,19 +83,28 @@ def camera_maps(H, W, rng, hot=0.0):
 
 
 def make_stack(name="stack512", T=None, device="cuda", seed=1234, pixel=0.1, NA=1.4,
-               wavelength=0.7):
+               wavelength=0.7, **overrides):
     """Build a named workload.  Returns a dict with ``images`` [T,H,W] and
     ``gamma`` [H,W] (float32 torch tensors on ``device``), ``mask`` (centred
-    16x16 numpy), ``alpha``, ``max_iters`` and the generating parameters."""
+    16x16 numpy), ``alpha``, ``max_iters`` and the generating parameters.
+    ``overrides`` replace workload fields (H, W, chains, bg, hot, photons);
+    ``photons=(lo, hi)`` draws each emitter's photon count from U(lo, hi)."""
     cfg = dict(WORKLOADS[name])
     if T is not None:
         cfg["T"] = int(T)
+    for k, v in overrides.items():
+        if k not in cfg:
+            raise KeyError("unknown workload field %r" % (k,))
+        cfg[k] = v
     rng = numpy.random.default_rng(seed)
     H, W = cfg["H"], cfg["W"]
     field = max(H, W) * pixel
     em = wlc_emitters(cfg["chains"], field, rng) / pixel
     sigma_px = 0.21 * wavelength / NA / pixel
-    ideal = render(em, H, W, sigma_px, cfg["photons"], cfg["bg"])
+    photons = cfg["photons"]
+    if isinstance(photons, (tuple, list)):
+        photons = rng.uniform(photons[0], photons[1], size=len(em))
+    ideal = render(em, H, W, sigma_px, photons, cfg["bg"])
     offset, gain, var = camera_maps(H, W, rng, cfg["hot"])
     dev = torch.device(device)
     g = torch.Generator(device=dev)
@@ -116,3 +126,59 @@ def make_stack(name="stack512", T=None, device="cuda", seed=1234, pixel=0.1, NA=
     mask = otf_weighted_mask(16, pixel, NA, wavelength)
     return dict(images=images, gamma=gamma, mask=mask, alpha=cfg["alpha"],
                 max_iters=cfg["max_iters"], ideal=ideal, name=name, seed=seed, cfg=cfg)
+
+
+def beads(n, field, rng):
+    """Positions (x, y) of n sparse point emitters, uniform over the field."""
+    return rng.uniform(0.0, field, size=(n, 2))
+
+
+def make_mixed(n_stacks=64, seed=4242, device="cuda", sides=(64, 128, 256, 512, 1024, 2048),
+               frames=(10, 200), pixel=0.1):
+    """The mixed-workload batch: ``n_stacks`` stacks with ROI sides drawn from
+    ``sides`` and frame counts U{frames}, each with its own alpha U(0.05, 0.5),
+    NA in {1.2, 1.4, 1.49} and wavelength in {520, 600, 700} nm (hence its own
+    OTF-weighted mask), and either worm-like chains (100 photons per emitter,
+    12 chains per 512 x 512 field) or sparse beads (Gaussian spots of 2000
+    photons, 0.05 per um^2); background 10 photons/px and the camera model of
+    ``camera_maps``.  Returns a list of dicts as ``make_stack`` does."""
+    rng = numpy.random.default_rng(seed)
+    dev = torch.device(device)
+    out = []
+    for k in range(n_stacks):
+        side = int(rng.choice(sides))
+        T = int(rng.integers(frames[0], frames[1] + 1))
+        alpha = float(rng.uniform(0.05, 0.5))
+        NA = float(rng.choice([1.2, 1.4, 1.49]))
+        wl = float(rng.choice([0.52, 0.6, 0.7]))
+        kind = "chains" if rng.uniform() < 0.5 else "beads"
+        field = side * pixel
+        sigma_px = 0.21 * wl / NA / pixel
+        if kind == "chains":
+            n_ch = max(1, int(round(12.0 * side * side / (512.0 * 512.0))))
+            ideal = render(wlc_emitters(n_ch, field, rng) / pixel, side, side, sigma_px, 100.0,
+                           10.0)
+        else:
+            n_b = max(1, int(round(0.05 * field * field)))
+            ideal = render(beads(n_b, field, rng) / pixel, side, side, sigma_px, 2000.0, 10.0)
+        offset, gain, var = camera_maps(side, side, rng)
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed * 1000 + k)
+        t_ideal = torch.as_tensor(ideal, dtype=torch.float32, device=dev)
+        t_gain = torch.as_tensor(gain, dtype=torch.float32, device=dev)
+        t_off = torch.as_tensor(offset, dtype=torch.float32, device=dev)
+        t_sd = torch.as_tensor(numpy.sqrt(var), dtype=torch.float32, device=dev)
+        images = torch.empty((T, side, side), dtype=torch.float32, device=dev)
+        chunk = max(1, (1 << 26) // (side * side))
+        for f0 in range(0, T, chunk):
+            n = min(chunk, T - f0)
+            phot = torch.poisson(t_ideal.expand(n, side, side).contiguous(), generator=g)
+            adu = phot * t_gain + t_sd * torch.randn((n, side, side), generator=g,
+                                                     device=dev) + t_off
+            d = (adu - t_off) / t_gain
+            images[f0:f0 + n] = torch.where(d <= 0, torch.full_like(d, 1e-6), d)
+        gamma = torch.as_tensor(var / gain ** 2, dtype=torch.float32, device=dev)
+        out.append(dict(images=images, gamma=gamma, mask=otf_weighted_mask(16, pixel, NA, wl),
+                        alpha=alpha, NA=NA, wavelength=wl, kind=kind, side=side, T=T,
+                        name="mixed[%d]" % k))
+    return out

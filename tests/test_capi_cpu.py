@@ -60,3 +60,24 @@ def test_null_handle_is_rejected(lib):
     n = ctypes.c_int64()
     assert lib.ncsb_num_tiles(1, 16, 16, None) == _lib.NCSB_EINVAL
     assert lib.ncsb_num_tiles(-1, 16, 16, ctypes.byref(n)) == _lib.NCSB_EINVAL
+
+
+def test_stack_descriptor_layout():
+    """ctypes mirror of ncsb_stack: 3 pointers, 4 int32, a double, 256 floats."""
+    import ctypes
+    from ncs_b200 import _lib
+    S = _lib.NcsbStack
+    assert ctypes.sizeof(S) == 3 * 8 + 4 * 4 + 8 + 256 * 4
+    assert S.alpha.offset == 40 and S.mask_shifted.offset == 48
+
+
+def test_mixed_workload_parameters():
+    from ncs_b200 import sim
+    st = sim.make_mixed(12, seed=5, device="cpu", sides=(64, 128), frames=(2, 4))
+    for s in st:
+        T, H, W = s["images"].shape
+        assert H == W == s["side"] and H in (64, 128) and 2 <= T <= 4
+        assert 0.05 <= s["alpha"] <= 0.5 and s["NA"] in (1.2, 1.4, 1.49)
+        assert s["wavelength"] in (0.52, 0.6, 0.7) and s["kind"] in ("chains", "beads")
+        assert s["mask"].shape == (16, 16) and (s["images"] > 0).all()
+    assert len({(s["NA"], s["wavelength"]) for s in st}) > 1

@@ -152,6 +152,84 @@ int ncsb_reduce_noise_start(ncsb_handle *h, const float *images, int n_frames, i
                             int32_t *tile_status, double *tile_cost, int32_t *tile_evals,
                             int32_t *tile_start, void *stream);
 
+/* ---- raw camera frames: the preprocessing prologue fused into the solve ---
+ * The reference converts ADU to photo-electrons on the host before the solve
+ * (python3-6/pyNCS/denoisetools.py:222-224, python3-6/NCSdemo_experiment.py:47-49:
+ * d = (ADU - offset) / gain, d <= 0 -> 1e-6; gamma = var / gain^2,
+ * denoisetools.py:266), and for cameras with several gain amplifiers picks
+ * each pixel's gain and variance maps by its ADU level (matlab/genmaps.m:29-62:
+ * level 0 below levels[0], level k for levels[k-1] <= ADU < levels[k], the
+ * last level above the last threshold).  Here the solver's tile gather does
+ * this per pixel, so neither d nor gamma is ever written to memory. */
+typedef struct {
+    const float *offset;    /* device [height][width], ADU */
+    const float *gain;      /* device [n_levels][height][width], ADU per photo-electron (> 0) */
+    const float *variance;  /* device [n_levels][height][width], ADU^2 */
+    int32_t n_levels;       /* 1..4 gain / variance map pairs */
+    float levels[3];        /* ascending ADU thresholds between the pairs (n_levels - 1 used) */
+} ncsb_calibration;
+
+/* ncsb_reduce_noise on raw ADU frames adu [n_frames][height][width] with the
+ * camera calibration `cal` (host struct of device pointers).  out is in
+ * photo-electrons, as ncsb_reduce_noise's.  Spectral form only. */
+int ncsb_reduce_noise_adu(ncsb_handle *h, const float *adu, int n_frames, int height, int width,
+                          const ncsb_calibration *cal, float *out, int32_t *tile_iters,
+                          int32_t *tile_status, double *tile_cost, int32_t *tile_evals,
+                          void *stream);
+
+/* ---- OTF masks from optics parameters, built on the device ---------------
+ * genfilter of the reference (python3-6/pyNCS/denoisetools.py:227-261 with
+ * genkspace :96-101): a raised-cosine high-pass of the radial frequency
+ * |k| = sqrt(X^2 + Y^2) / (16 pixel_size), X, Y = -8..7, for the types
+ * pureN, adjustable (w, h) and OTFweighted; plus INCOHERENT, 1 - the
+ * circular-pupil incoherent OTF inside the cutoff 2 NA / lambda (1 outside),
+ * the mask of the synthetic workloads.  Lengths in one unit (e.g. um). */
+#define NCSB_MASK_OTFWEIGHTED 0
+#define NCSB_MASK_PUREN 1
+#define NCSB_MASK_ADJUSTABLE 2
+#define NCSB_MASK_INCOHERENT 3
+
+typedef struct {
+    int32_t type;        /* NCSB_MASK_* */
+    double pixel_size;   /* sample spacing */
+    double na;           /* numerical aperture */
+    double wavelength;   /* emission wavelength */
+    double w, h;         /* adjustable type only: 0 < w, 0 < h < 1 (reference defaults 1, 0.7) */
+} ncsb_optics;
+
+/* n centred 16x16 masks (DC at [8][8], the reference's orientation) written
+ * to masks_centred (device, [n][16][16] FP32), computed in FP64 on the
+ * device.  NCSB_EINVAL for an unknown type or non-positive parameters. */
+int ncsb_genfilter(const ncsb_optics *optics, int n, float *masks_centred, void *stream);
+
+/* ---- simulator: synthetic sCMOS stacks generated on the device ------------
+ * Replaces the reference's host-side simulation loops (python3-6/pyNCS/
+ * denoisetools.py:118-186 genidealimage / SRhist, :205-225 addnoise /
+ * gendatastack).  Random numbers come from Philox4x32-10 keyed by `seed` and
+ * addressed by (pixel, frame, draw), so results do not depend on the launch. */
+
+/* ideal [height][width] = background + sum over emitters of photons x the
+ * pixel-integrated Gaussian PSF (sigma_px, footprint |floor(x_e) - x| <= half,
+ * half <= 16).  emitters_sorted: device [n][3] FP32 (x along width, y along
+ * height, photons; pixel i spans [i, i+1)), sorted by 8 x 8-pixel cell
+ * (cell = clamp(floor(y)/8) * ceil(width/8) + clamp(floor(x)/8));
+ * cell_start: device [ncells + 1] int32 offsets into the sorted list. */
+int ncsb_sim_render(const float *emitters_sorted, const int *cell_start, int height, int width,
+                    double sigma_px, int half, float background, float *ideal, void *stream);
+
+/* n_frames independent camera frames of one ideal image: n ~ Poisson(ideal),
+ * ADU = n gain + sqrt(variance) N(0,1) + offset (addnoise), and/or the
+ * photo-electrons (ADU - offset) / gain with values <= 0 set to 1e-6
+ * (gendatastack).  Maps [height][width]; adu and photo_electrons
+ * [n_frames][height][width] (either may be NULL, not both). */
+int ncsb_sim_camera(const float *ideal, int n_frames, int height, int width, const float *offset,
+                    const float *gain, const float *variance, uint64_t seed, float *adu,
+                    float *photo_electrons, void *stream);
+
+/* The generator's uniform deviates in (0, 1) for counters (i, frame, 0, 0),
+ * i < n (for statistical tests of the generator). */
+int ncsb_sim_uniforms(int64_t n, uint32_t frame, uint64_t seed, float *out, void *stream);
+
 /* ---- batched launch: many stacks, one persistent queue -------------------
  * No counterpart in the reference, which processes one stack per call with
  * one alpha and one mask (cuda/pyCUDANCS/ncs.py:35-173).  Here several stacks
@@ -166,6 +244,9 @@ typedef struct {
     int32_t n_frames, height, width, gamma_per_frame;
     double alpha;             /* this stack's alpha */
     float mask_shifted[256];  /* this stack's 16x16 OTF mask, DC at [0][0] (host values) */
+    int32_t mask_from_optics; /* nonzero: ignore mask_shifted, build the mask from optics
+                                 on the device */
+    ncsb_optics optics;
 } ncsb_stack;
 
 #define NCSB_MAX_STACKS 65536

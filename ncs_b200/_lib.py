@@ -49,6 +49,28 @@ class NcsbParams(ctypes.Structure):
     ]
 
 
+MASK_TYPES = {"OTFweighted": 0, "pureN": 1, "adjustable": 2, "incoherent": 3}
+
+
+class NcsbOptics(ctypes.Structure):
+    """ncsb_optics: parameters of a mask built on the device."""
+    _fields_ = [
+        ("type", ctypes.c_int32),
+        ("pixel_size", ctypes.c_double),
+        ("na", ctypes.c_double),
+        ("wavelength", ctypes.c_double),
+        ("w", ctypes.c_double),
+        ("h", ctypes.c_double),
+    ]
+
+
+def optics(type="OTFweighted", pixel_size=0.1, NA=1.4, wavelength=0.7, w=1.0, h=0.7):
+    o = NcsbOptics()
+    o.type = MASK_TYPES[type]
+    o.pixel_size, o.na, o.wavelength, o.w, o.h = pixel_size, NA, wavelength, w, h
+    return o
+
+
 class NcsbStack(ctypes.Structure):
     """ncsb_stack: one stack of a batched launch."""
     _fields_ = [
@@ -61,6 +83,19 @@ class NcsbStack(ctypes.Structure):
         ("gamma_per_frame", ctypes.c_int32),
         ("alpha", ctypes.c_double),
         ("mask_shifted", ctypes.c_float * 256),
+        ("mask_from_optics", ctypes.c_int32),
+        ("optics", NcsbOptics),
+    ]
+
+
+class NcsbCalibration(ctypes.Structure):
+    """ncsb_calibration: camera maps for raw-ADU input."""
+    _fields_ = [
+        ("offset", ctypes.c_void_p),
+        ("gain", ctypes.c_void_p),
+        ("variance", ctypes.c_void_p),
+        ("n_levels", ctypes.c_int32),
+        ("levels", ctypes.c_float * 3),
     ]
 
 
@@ -75,6 +110,8 @@ EXPORTS = [
     "ncsb_net_relu_bwd", "ncsb_net_mse_grad", "ncsb_net_adam", "ncsb_net_features",
     "ncsb_net_infer_stack", "ncsb_net_infer_tiles", "ncsb_net_infer_batch",
     "ncsb_batch_set", "ncsb_batch_num_tiles", "ncsb_batch_reduce_noise",
+    "ncsb_reduce_noise_adu", "ncsb_genfilter",
+    "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms",
 ]
 
 _lib = None
@@ -127,6 +164,17 @@ def load():
     lib.ncsb_net_features.argtypes = [vp, vp, vp, vp, ci, vp]
     lib.ncsb_net_infer_stack.argtypes = [vp, vp, ci, ci, ci, vp, ci, vp, vp]
     lib.ncsb_net_infer_tiles.argtypes = [vp, vp, vp, i64, vp, vp]
+    lib.ncsb_reduce_noise_adu.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          P(NcsbCalibration), vp, vp, vp, vp, vp, vp]
+    lib.ncsb_reduce_noise_adu.restype = ctypes.c_int
+    lib.ncsb_sim_render.argtypes = [vp, vp, ci, ci, ctypes.c_double, ci, f32, vp, vp]
+    lib.ncsb_sim_render.restype = ctypes.c_int
+    lib.ncsb_sim_camera.argtypes = [vp, ci, ci, ci, vp, vp, vp, ctypes.c_uint64, vp, vp, vp]
+    lib.ncsb_sim_camera.restype = ctypes.c_int
+    lib.ncsb_sim_uniforms.argtypes = [i64, ctypes.c_uint32, ctypes.c_uint64, vp, vp]
+    lib.ncsb_sim_uniforms.restype = ctypes.c_int
+    lib.ncsb_genfilter.argtypes = [P(NcsbOptics), ctypes.c_int, vp, vp]
+    lib.ncsb_genfilter.restype = ctypes.c_int
     lib.ncsb_net_infer_batch.argtypes = [vp, vp, vp, vp]
     lib.ncsb_batch_set.argtypes = [vp, P(NcsbStack), ctypes.c_int]
     lib.ncsb_batch_set.restype = ctypes.c_int

@@ -19,6 +19,11 @@ cudaError_t launch_warp_blocks(const SolveArgs& args, int grid, int blocks, cuda
 int warp_max_ctas_per_sm(int m, int blocks);
 cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
 int spectral_max_ctas_per_sm(int m, int blocks, bool warm, bool batch);
+namespace masks {
+bool valid(const ncsb_optics& o);
+cudaError_t launch_masks(const ncsb_optics* d_optics, int n, float* centred, float* lane,
+                         const int* d_slot, cudaStream_t s);
+}  // namespace masks
 namespace net {
 int launch_infer_batch(const float* params, const StackDesc* stacks, int n_stacks,
                        long long n_tiles, float* u0, cudaStream_t s);
@@ -285,6 +290,49 @@ int ncsb_reduce_noise_start(ncsb_handle* h, const float* images, int n_frames, i
     return launch(h, a, (cudaStream_t)stream);
 }
 
+int ncsb_reduce_noise_adu(ncsb_handle* h, const float* adu, int n_frames, int height, int width,
+                          const ncsb_calibration* cal, float* out, int32_t* tile_iters,
+                          int32_t* tile_status, double* tile_cost, int32_t* tile_evals,
+                          void* stream) {
+    if (!h) return NCSB_EINVAL;
+    if (h->p.mode != NCSB_MODE_SPECTRAL)
+        return fail(h, NCSB_EINVAL, "raw-ADU input needs the spectral form");
+    if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
+    if (!adu || !out || !cal || !cal->offset || !cal->gain || !cal->variance)
+        return fail(h, NCSB_EINVAL, "null buffer");
+    if (cal->n_levels < 1 || cal->n_levels > 4)
+        return fail(h, NCSB_EINVAL, "n_levels must be 1..4");
+    for (int q = 0; q + 1 < cal->n_levels; ++q) {
+        if (!std::isfinite(cal->levels[q]) || (q > 0 && !(cal->levels[q] > cal->levels[q - 1])))
+            return fail(h, NCSB_EINVAL, "levels must be finite and ascending");
+    }
+    if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
+    if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
+        return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
+    if (n_frames == 0) return NCSB_OK;
+    ncsb::SolveArgs a{};
+    a.tile_mode = 0;
+    a.data = adu;
+    a.gamma = cal->variance;  // not read as gamma; kept non-null
+    a.out = out;
+    a.T = n_frames;
+    a.H = height;
+    a.W = width;
+    a.tiles_x = tiles_along(height);
+    a.tiles_y = tiles_along(width);
+    a.n_tiles = (long long)n_frames * a.tiles_x * a.tiles_y;
+    a.iters = tile_iters;
+    a.status = tile_status;
+    a.cost = tile_cost;
+    a.evals = tile_evals;
+    a.adu_offset = cal->offset;
+    a.adu_gain = cal->gain;
+    a.adu_var = cal->variance;
+    a.n_levels = cal->n_levels;
+    for (int q = 0; q < 3; ++q) a.levels[q] = cal->levels[q];
+    return launch(h, a, (cudaStream_t)stream);
+}
+
 int ncsb_solve_tiles(ncsb_handle* h, const float* data_in, const float* gamma_in, const float* u0,
                      int64_t n_tiles, float* data_out, int32_t* iters, int32_t* status,
                      double* cost, int32_t* evals, void* stream) {
@@ -313,6 +361,8 @@ int ncsb_batch_set(ncsb_handle* h, const ncsb_stack* stacks, int n_stacks) {
         return fail(h, NCSB_EINVAL, "need 1..NCSB_MAX_STACKS stacks");
     std::vector<ncsb::StackDesc> desc(n_stacks);
     std::vector<float> mk((size_t)n_stacks * 256);
+    std::vector<ncsb_optics> optics;  // stacks whose mask is built on the device
+    std::vector<int> slots;
     long long total = 0;
     for (int i = 0; i < n_stacks; ++i) {
         const ncsb_stack& st = stacks[i];
@@ -324,9 +374,16 @@ int ncsb_batch_set(ncsb_handle* h, const ncsb_stack* stacks, int n_stacks) {
             return fail(h, NCSB_ESIZE, at + "frames must be at least 14 x 14");
         if (!std::isfinite(st.alpha) || st.alpha < 0.0)
             return fail(h, NCSB_EINVAL, at + "alpha must be finite and >= 0");
-        float nat[256];
-        if (!build_msq(st.mask_shifted, nat)) return fail(h, NCSB_EINVAL, at + "non-finite mask");
-        lane_layout(nat, mk.data() + (size_t)i * 256);
+        if (st.mask_from_optics) {
+            if (!ncsb::masks::valid(st.optics)) return fail(h, NCSB_EINVAL, at + "bad optics");
+            optics.push_back(st.optics);
+            slots.push_back(i);
+        } else {
+            float nat[256];
+            if (!build_msq(st.mask_shifted, nat))
+                return fail(h, NCSB_EINVAL, at + "non-finite mask");
+            lane_layout(nat, mk.data() + (size_t)i * 256);
+        }
         ncsb::StackDesc& d = desc[i];
         d.data = st.images;
         d.gamma = st.gamma;
@@ -359,6 +416,25 @@ int ncsb_batch_set(ncsb_handle* h, const ncsb_stack* stacks, int n_stacks) {
     if (e == cudaSuccess)
         e = cudaMemcpy(h->d_mk_lane, mk.data(), sizeof(float) * mk.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpy(batch)");
+    if (!optics.empty()) {
+        // overwrite those stacks' tables with masks built on the device
+        const int no = (int)optics.size();
+        ncsb_optics* d_optics = nullptr;
+        int* d_slots = nullptr;
+        e = cudaMalloc(&d_optics, sizeof(ncsb_optics) * no);
+        if (e == cudaSuccess) e = cudaMalloc(&d_slots, sizeof(int) * no);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(d_optics, optics.data(), sizeof(ncsb_optics) * no,
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(d_slots, slots.data(), sizeof(int) * no, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = ncsb::masks::launch_masks(d_optics, no, nullptr, h->d_mk_lane, d_slots, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        cudaFree(d_optics);
+        cudaFree(d_slots);
+        if (e != cudaSuccess) return cuda_fail(h, e, "device masks");
+    }
     h->n_stacks = n_stacks;
     h->batch_tiles = total;
     // resolve the kernel variants' attributes now, outside any stream capture

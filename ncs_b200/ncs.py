@@ -189,6 +189,49 @@ class Solver:
                 ctypes.c_void_p(s.cuda_stream)))
         return out, iters, status, cost, evals, start
 
+    def reduce_noise_adu(self, adu, offset, gain, variance, levels=(), out=None,
+                         tile_stats=False, stream=None):
+        """Denoise raw camera frames: ``adu`` [T, H, W] counts, ``offset``
+        [H, W], ``gain`` and ``variance`` [H, W] or [L, H, W] (L gain
+        amplifiers, chosen per pixel by ADU level against the L - 1 ascending
+        ``levels``).  The conversion to photo-electrons (d = (ADU - offset) /
+        gain, non-positive d -> 1e-6, gamma = variance / gain^2) happens inside
+        the solver's tile gather.  Returns ``out`` in photo-electrons, or with
+        ``tile_stats`` (out, iters, status, cost, evals)."""
+        adu = self._tensor(adu, "adu")
+        if adu.dim() == 2:
+            adu = adu.unsqueeze(0)
+        T, H, W = adu.shape
+        offset = self._tensor(offset, "offset", (H, W))
+        gain = self._tensor(gain, "gain")
+        variance = self._tensor(variance, "variance")
+        if gain.dim() == 2:
+            gain = gain.unsqueeze(0)
+        if variance.dim() == 2:
+            variance = variance.unsqueeze(0)
+        L = gain.shape[0]
+        if tuple(gain.shape) != (L, H, W) or tuple(variance.shape) != (L, H, W):
+            raise ValueError("gain and variance must be [H, W] or [L, H, W] alike")
+        if not 1 <= L <= 4 or len(levels) != L - 1:
+            raise ValueError("need 1..4 map pairs and one threshold between each two")
+        cal = _lib.NcsbCalibration()
+        cal.offset, cal.gain, cal.variance = offset.data_ptr(), gain.data_ptr(), variance.data_ptr()
+        cal.n_levels = L
+        for q, v in enumerate(levels):
+            cal.levels[q] = float(v)
+        out = torch.empty_like(adu) if out is None else self._tensor(out, "out", (T, H, W))
+        n = self.num_tiles(T, H, W)
+        st = [torch.empty(n, dtype=torch.int32, device=self.device) for _ in range(3)]
+        cost = torch.empty(n, dtype=torch.float64, device=self.device)
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_reduce_noise_adu(
+                self._handle, _ptr(adu), T, H, W, ctypes.byref(cal), _ptr(out), _ptr(st[0]),
+                _ptr(st[1]), _ptr(cost), _ptr(st[2]), ctypes.c_void_p(s.cuda_stream)))
+        if tile_stats:
+            return out, st[0], st[1], cost, st[2]
+        return out
+
     # ---- batched launch: many stacks, each with its own alpha and mask ------
     def batch_set(self, stacks):
         """Register a batch of stacks for ``batch_reduce_noise``.  ``stacks`` is
@@ -216,17 +259,21 @@ class Solver:
                 raise ValueError("stack %d: gamma must be [H, W] or [T, H, W]" % i)
             out = st.get("out")
             out = torch.empty_like(images) if out is None else self._tensor(out, "out", (T, H, W))
-            if "mask_shifted" in st:
-                ms = numpy.asarray(st["mask_shifted"], dtype=numpy.float32)
-            else:
-                ms = numpy.fft.fftshift(numpy.asarray(st["mask"])).astype(numpy.float32)
-            if ms.shape != (16, 16):
-                raise ValueError("stack %d: OTF mask must be 16 x 16" % i)
             a = arr[i]
             a.images, a.gamma, a.out = images.data_ptr(), gamma.data_ptr(), out.data_ptr()
             a.n_frames, a.height, a.width, a.gamma_per_frame = T, H, W, per_frame
             a.alpha = float(st["alpha"])
-            ctypes.memmove(a.mask_shifted, numpy.ascontiguousarray(ms).ctypes.data, 1024)
+            if "optics" in st:   # mask built on the device from optics parameters
+                a.mask_from_optics = 1
+                a.optics = _lib.optics(**st["optics"])
+            else:
+                if "mask_shifted" in st:
+                    ms = numpy.asarray(st["mask_shifted"], dtype=numpy.float32)
+                else:
+                    ms = numpy.fft.fftshift(numpy.asarray(st["mask"])).astype(numpy.float32)
+                if ms.shape != (16, 16):
+                    raise ValueError("stack %d: OTF mask must be 16 x 16" % i)
+                ctypes.memmove(a.mask_shifted, numpy.ascontiguousarray(ms).ctypes.data, 1024)
             keep.append((images, gamma, out))
             outs.append(out)
         with torch.cuda.device(self.device):

@@ -54,3 +54,23 @@ def genfilter(R, pixelsize, NA, Lambda, Type="OTFweighted", w=1, h=0.7):
 
 def shifted(mask_centred):
     return numpy.fft.fftshift(numpy.asarray(mask_centred))
+
+
+def device_masks(optics_list, device="cuda"):
+    """Centred 16 x 16 masks built on the GPU (libncs_b200 ncsb_genfilter),
+    one per dict of ``ncs_b200._lib.optics`` keywords (type, pixel_size, NA,
+    wavelength, w, h).  Returns a float32 tensor [n, 16, 16] on ``device``."""
+    import ctypes
+    import torch
+    from . import _lib
+    n = len(optics_list)
+    arr = (_lib.NcsbOptics * max(n, 1))()
+    for i, o in enumerate(optics_list):
+        arr[i] = _lib.optics(**o)
+    out = torch.empty((n, 16, 16), dtype=torch.float32, device=device)
+    with torch.cuda.device(out.device):
+        rc = _lib.load().ncsb_genfilter(arr, n, ctypes.c_void_p(out.data_ptr()),
+                                        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    if rc != _lib.NCSB_OK:
+        raise ValueError("ncsb_genfilter failed with code %d (bad optics?)" % rc)
+    return out

@@ -182,3 +182,100 @@ def make_mixed(n_stacks=64, seed=4242, device="cuda", sides=(64, 128, 256, 512, 
                         alpha=alpha, NA=NA, wavelength=wl, kind=kind, side=side, T=T,
                         name="mixed[%d]" % k))
     return out
+
+
+# ---- the same physics on the GPU (libncs_b200 ncsb_sim_*) --------------------
+
+_CELL = 8
+
+
+def render_gpu(emitters_px, H, W, sigma_px, photons, bg, half=5, device="cuda"):
+    """``render`` on the device: [H, W] float32 tensor.  Emitters farther than
+    ``half`` pixels outside the frame cannot contribute and are dropped; the
+    rest are sorted by 8 x 8-pixel cell for the kernel's fixed-order gather."""
+    import ctypes
+    from . import _lib
+    em = numpy.asarray(emitters_px, dtype=numpy.float64).reshape(-1, 2)
+    ph = numpy.broadcast_to(numpy.asarray(photons, dtype=numpy.float64), (len(em),))
+    fx, fy = numpy.floor(em[:, 0]), numpy.floor(em[:, 1])
+    keep = (fx >= -half) & (fx <= W - 1 + half) & (fy >= -half) & (fy <= H - 1 + half)
+    em, ph, fx, fy = em[keep], ph[keep], fx[keep], fy[keep]
+    ncx, ncy = (W + _CELL - 1) // _CELL, (H + _CELL - 1) // _CELL
+    cx = numpy.clip(fx // _CELL, 0, ncx - 1).astype(numpy.int64)
+    cy = numpy.clip(fy // _CELL, 0, ncy - 1).astype(numpy.int64)
+    cell = cy * ncx + cx
+    order = numpy.argsort(cell, kind="stable")
+    start = numpy.zeros(ncx * ncy + 1, dtype=numpy.int32)
+    numpy.cumsum(numpy.bincount(cell, minlength=ncx * ncy), out=start[1:])
+    packed = numpy.stack([em[order, 0], em[order, 1], ph[order]], axis=1).astype(numpy.float32)
+    dev = torch.device(device)
+    t_em = torch.as_tensor(packed.reshape(-1), device=dev)
+    t_start = torch.as_tensor(start, device=dev)
+    ideal = torch.empty((H, W), dtype=torch.float32, device=dev)
+    with torch.cuda.device(dev):
+        rc = _lib.load().ncsb_sim_render(
+            ctypes.c_void_p(t_em.data_ptr() if len(packed) else 0),
+            ctypes.c_void_p(t_start.data_ptr()), H, W, float(sigma_px), int(half), float(bg),
+            ctypes.c_void_p(ideal.data_ptr()),
+            ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    if rc != _lib.NCSB_OK:
+        raise RuntimeError("ncsb_sim_render failed with code %d" % rc)
+    return ideal
+
+
+def camera_gpu(ideal, T, offset, gain, var, seed, adu=False, photons=True):
+    """T camera frames of ``ideal`` on its device: returns (photo-electrons,
+    ADU), each [T, H, W] float32 or None as requested."""
+    import ctypes
+    from . import _lib
+    H, W = ideal.shape
+    dev = ideal.device
+    maps = [torch.as_tensor(numpy.asarray(m), dtype=torch.float32, device=dev).contiguous()
+            for m in (offset, gain, var)]
+    ph = torch.empty((T, H, W), dtype=torch.float32, device=dev) if photons else None
+    ad = torch.empty((T, H, W), dtype=torch.float32, device=dev) if adu else None
+    vp = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else 0)
+    with torch.cuda.device(dev):
+        rc = _lib.load().ncsb_sim_camera(
+            vp(ideal.contiguous()), T, H, W, vp(maps[0]), vp(maps[1]), vp(maps[2]),
+            int(seed) & 0xFFFFFFFFFFFFFFFF, vp(ad), vp(ph),
+            ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    if rc != _lib.NCSB_OK:
+        raise RuntimeError("ncsb_sim_camera failed with code %d" % rc)
+    return ph, ad
+
+
+def make_stack_gpu(name="stack512", T=None, device="cuda", seed=1234, pixel=0.1, NA=1.4,
+                   wavelength=0.7, adu=False, **overrides):
+    """``make_stack`` with the rendering and the camera on the GPU (the
+    emitter positions, photon counts and camera maps are still drawn on the
+    host from the same numpy seed).  With ``adu`` the raw frames and the
+    calibration maps are returned too (keys adu, offset, gain, var)."""
+    cfg = dict(WORKLOADS[name])
+    if T is not None:
+        cfg["T"] = int(T)
+    for k, v in overrides.items():
+        if k not in cfg:
+            raise KeyError("unknown workload field %r" % (k,))
+        cfg[k] = v
+    rng = numpy.random.default_rng(seed)
+    H, W = cfg["H"], cfg["W"]
+    field = max(H, W) * pixel
+    em = wlc_emitters(cfg["chains"], field, rng) / pixel
+    sigma_px = 0.21 * wavelength / NA / pixel
+    photons = cfg["photons"]
+    if isinstance(photons, (tuple, list)):
+        photons = rng.uniform(photons[0], photons[1], size=len(em))
+    offset, gain, var = camera_maps(H, W, rng, cfg["hot"])
+    dev = torch.device(device)
+    ideal = render_gpu(em, H, W, sigma_px, photons, cfg["bg"], device=dev)
+    phot, raw = camera_gpu(ideal, cfg["T"], offset, gain, var, seed, adu=adu)
+    out = dict(images=phot, gamma=torch.as_tensor(var / gain ** 2, dtype=torch.float32, device=dev),
+               mask=otf_weighted_mask(16, pixel, NA, wavelength), alpha=cfg["alpha"],
+               max_iters=cfg["max_iters"], ideal=ideal, name=name, seed=seed, cfg=cfg)
+    if adu:
+        out.update(adu=raw,
+                   offset=torch.as_tensor(offset, dtype=torch.float32, device=dev),
+                   gain=torch.as_tensor(gain, dtype=torch.float32, device=dev),
+                   var=torch.as_tensor(var, dtype=torch.float32, device=dev))
+    return out

@@ -15,9 +15,10 @@ weights, ReLU backward, the MSE loss gradient, Adam and the fused inference
 kernel.  PyTorch only allocates buffers and does index plumbing for the
 training data.
 
-Training data: seeded 512 x 512 simulations with the full-sensor workload's
-structure density and camera (hot pixels included), per-emitter photons
-U(50, 400) and background U(2, 30) photons/px, cut into
+Training data: seeded 512 x 512 simulations (rendered and sampled on the GPU,
+ncs_b200/sim.py make_stack_gpu) with the full-sensor workload's structure
+density and camera (hot pixels included), per-emitter photons U(50, 400) and
+background U(2, 30) photons/px, cut into
 tiles with the solvers' segmentation and solved to convergence by the plain
 GPU kernel (epsilon 1e-6).  The regression target is the normalised
 correction y* = (u* - d) / s with s the tile's standard deviation + 1.
@@ -294,13 +295,13 @@ def simulate(seed, device, H=512, W=512, frames=3, chains=None):
     workload's structure density (60 chains per 2048 x 2048 field, so 4 per
     512 x 512) and camera (0.5 % hot pixels with x50 read variance), with
     per-emitter photons U(50, 400) and background U(2, 30) photons/px."""
-    from .sim import make_stack
+    from .sim import make_stack_gpu
     rng = numpy.random.default_rng(seed)
     bg = float(rng.uniform(2.0, 30.0))
     if chains is None:
         chains = max(1, int(round(60.0 * H * W / (2048.0 * 2048.0))))
-    return make_stack("sensor2048", T=frames, device=device, seed=int(seed), H=H, W=W,
-                      chains=chains, photons=(50.0, 400.0), bg=bg)
+    return make_stack_gpu("sensor2048", T=frames, device=device, seed=int(seed), H=H, W=W,
+                          chains=chains, photons=(50.0, 400.0), bg=bg)
 
 
 def training_tiles(n_tiles, seed=1000, device="cuda", frames=3, log=None):

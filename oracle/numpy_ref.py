@@ -210,3 +210,32 @@ def rel_cost_gap(f, fstar):
     """|f - f*| / max(|f*|, 1): the per-tile accuracy measure (tile costs can be
     negative, so the denominator is floored at 1)."""
     return numpy.abs(numpy.asarray(f) - numpy.asarray(fstar)) / numpy.maximum(numpy.abs(fstar), 1.0)
+
+
+def genmaps(adu, gain, var, levels):
+    """Per-frame gain and variance maps of a multi-amplifier camera: each pixel
+    takes pair 0 below levels[0], pair k for levels[k-1] <= ADU < levels[k], the
+    last pair above the last threshold (matlab/genmaps.m:29-62; with one pair
+    the maps are used as they are).  adu [T,H,W]; gain, var [L,H,W]."""
+    adu = numpy.asarray(adu, dtype=numpy.float64)
+    gain = numpy.asarray(gain, dtype=numpy.float64)
+    var = numpy.asarray(var, dtype=numpy.float64)
+    if gain.ndim == 2:
+        gain, var = gain[None], var[None]
+    lv = numpy.zeros(adu.shape, dtype=numpy.int64)
+    for t in levels:
+        lv += (adu >= t)
+    H, W = adu.shape[1:]
+    rows = numpy.arange(H)[:, None]
+    cols = numpy.arange(W)[None, :]
+    return gain[lv, rows, cols], var[lv, rows, cols]
+
+
+def adu_to_photons(adu, offset, gain, var, levels=()):
+    """(d, gamma) from raw frames: d = (ADU - offset) / gain with d <= 0 set to
+    1e-6 (python3-6/pyNCS/denoisetools.py:222-224), gamma = var / gain^2
+    (denoisetools.py:266), the maps picked per pixel by genmaps."""
+    g, v = genmaps(adu, gain, var, levels)
+    d = (numpy.asarray(adu, dtype=numpy.float64) - numpy.asarray(offset, dtype=numpy.float64)) / g
+    d[d <= 0] = 1e-6
+    return d, v / (g * g)

@@ -63,12 +63,18 @@ def test_null_handle_is_rejected(lib):
 
 
 def test_stack_descriptor_layout():
-    """ctypes mirror of ncsb_stack: 3 pointers, 4 int32, a double, 256 floats."""
+    """ctypes mirrors of ncsb_stack (3 pointers, 4 int32, a double, 256
+    floats, an int32 flag, ncsb_optics) and ncsb_optics (int32 + 5 doubles),
+    with C's alignment of the double members."""
     import ctypes
     from ncs_b200 import _lib
     S = _lib.NcsbStack
-    assert ctypes.sizeof(S) == 3 * 8 + 4 * 4 + 8 + 256 * 4
+    assert ctypes.sizeof(_lib.NcsbOptics) == 48 and _lib.NcsbOptics.pixel_size.offset == 8
     assert S.alpha.offset == 40 and S.mask_shifted.offset == 48
+    assert S.mask_from_optics.offset == 1072 and S.optics.offset == 1080
+    assert ctypes.sizeof(S) == 1128
+    C = _lib.NcsbCalibration
+    assert C.n_levels.offset == 24 and C.levels.offset == 28 and ctypes.sizeof(C) == 40
 
 
 def test_mixed_workload_parameters():

@@ -175,3 +175,20 @@ def test_masks_match_reference(gold):
     m = otf.otf_weighted_mask()
     assert checkOTFMask(m)
     assert m[8, 8] == 0.0 and m.max() == 1.0
+
+
+def test_genmaps_known_answer():
+    """Three amplifiers, thresholds 100 and 200: pixels below 100 use pair 0,
+    [100, 200) pair 1, >= 200 pair 2 (matlab/genmaps.m:36-58)."""
+    from oracle import numpy_ref as nr
+    adu = numpy.array([[[50.0, 100.0], [199.9, 200.0]]])
+    gain = numpy.stack([numpy.full((2, 2), 1.0), numpy.full((2, 2), 2.0), numpy.full((2, 2), 4.0)])
+    var = gain * 10.0
+    g, v = nr.genmaps(adu, gain, var, (100.0, 200.0))
+    assert numpy.array_equal(g[0], [[1.0, 2.0], [2.0, 4.0]])
+    assert numpy.array_equal(v[0], [[10.0, 20.0], [20.0, 40.0]])
+    off = numpy.full((2, 2), 100.0)
+    d, gam = nr.adu_to_photons(adu, off, gain, var, (100.0, 200.0))
+    # (50-100)/1 <= 0 -> 1e-6; (100-100)/2 = 0 -> 1e-6; 99.9/2; 100/4
+    assert numpy.allclose(d[0], [[1e-6, 1e-6], [49.95, 25.0]])
+    assert numpy.allclose(gam[0], [[10.0, 5.0], [5.0, 2.5]])

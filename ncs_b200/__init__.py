@@ -6,9 +6,10 @@ it; there is no CPU fallback.
 """
 from . import _lib
 from .ncs import (NCSCUDA, NCSCUDAException, Solver, cReduceNoise, checkOTFMask,
-                  reduceNoise)
+                  reduce_noise_normalized, reduceNoise)
 
 _lib.load()
 
 __all__ = ["Solver", "NCSCUDA", "NCSCUDAException", "reduceNoise", "cReduceNoise",
+           "reduce_noise_normalized",
            "checkOTFMask"]

@@ -111,7 +111,7 @@ EXPORTS = [
     "ncsb_net_infer_stack", "ncsb_net_infer_tiles", "ncsb_net_infer_batch",
     "ncsb_batch_set", "ncsb_batch_num_tiles", "ncsb_batch_reduce_noise",
     "ncsb_reduce_noise_adu", "ncsb_genfilter",
-    "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms",
+    "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms", "ncsb_reduce_noise_normalized",
 ]
 
 _lib = None
@@ -173,6 +173,10 @@ def load():
     lib.ncsb_sim_camera.restype = ctypes.c_int
     lib.ncsb_sim_uniforms.argtypes = [i64, ctypes.c_uint32, ctypes.c_uint64, vp, vp]
     lib.ncsb_sim_uniforms.restype = ctypes.c_int
+    lib.ncsb_reduce_noise_normalized.argtypes = [vp, ci, ci, ci, vp, ci, P(ctypes.c_float),
+                                                 ctypes.c_double, ci, ctypes.c_double, vp, vp,
+                                                 vp, vp, vp]
+    lib.ncsb_reduce_noise_normalized.restype = ctypes.c_int
     lib.ncsb_genfilter.argtypes = [P(NcsbOptics), ctypes.c_int, vp, vp]
     lib.ncsb_genfilter.restype = ctypes.c_int
     lib.ncsb_net_infer_batch.argtypes = [vp, vp, vp, vp]

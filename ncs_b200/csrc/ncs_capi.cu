@@ -148,7 +148,7 @@ void ncsb_default_params(ncsb_params* p) {
     if (!p) return;
     p->alpha = 0.2;
     p->max_iters = 200;
-    p->m = 2;
+    p->m = 1;
     p->epsilon = 1e-5;
     p->c1 = 1e-4;
     p->min_step = 1e-6;

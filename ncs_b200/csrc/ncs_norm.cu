@@ -1,0 +1,293 @@
+// ncs_norm.cu -- the normalised single-pixel NCS variant
+// ("matlab - single pixel with normalization/" in the reference): every pixel
+// is its own 3 x 3 segment (the pixel and its 8 neighbours, replicate-padded,
+// segpadimg.m with Rs = 1) minimising
+//     f(u) = (2/9) sum_i [u_i - c_i log(u_i + gamma_i)] + alpha P(u) / S(u),
+//     P(u) = sum_k (|fftshift(fft2(u))_k| / 3 * M_k)^2 = u' Q u,  S(u) = sum_i u_i
+// (calcost.m:38-56), from u = d, keeping the segment centre (stitchpadimg.m)
+// and setting negative results to 1e-6 (reducenoise.m, optimf).
+//
+// One thread per pixel: 9 unknowns, FP64 iterate, gradient and costs (the
+// cost is a sum of terms of order 100 whose differences near convergence are
+// of order 1e-5), BFGS with a dense 9 x 9 inverse-Hessian approximation kept
+// in shared memory (45 packed FP32 entries per thread), backtracking Armijo
+// line search with the fraction-to-barrier rule of the main solver.  The
+// reference minimises with MATLAB's fminunc quasi-Newton; the stopping rule
+// here is fminunc's first-order optimality test, ||g||_inf <= tol *
+// max(1, ||g_0||_inf), with its iteration cap.  Q (9 x 9, symmetric) is built
+// on the host from the 3 x 3 centred mask and passed packed.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "../../include/ncs_b200.h"
+
+namespace ncsb {
+namespace norm {
+
+constexpr int kThreads = 128;
+constexpr int kPacked = 45;  // upper triangle of a symmetric 9 x 9
+
+struct Args {
+    const float* data;
+    const float* gamma;
+    long long gstride;
+    float* out;
+    int T, H, W;
+    double q[kPacked];
+    double alpha, tol, c1, min_step;
+    int max_iters;
+    int32_t* iters;
+    int32_t* status;
+    double* cost;
+};
+
+__host__ __device__ constexpr int pk(int i, int j) {  // packed index, i <= j
+    return i * 9 - i * (i - 1) / 2 + (j - i);
+}
+
+__device__ __forceinline__ double qij(const Args& a, int i, int j) {
+    return i <= j ? a.q[pk(i, j)] : a.q[pk(j, i)];
+}
+
+// Per-thread constants of the segment in shared memory (c = d + gamma, gamma),
+// column t of each [9][kThreads] array.
+struct Seg {
+    const double (*c)[kThreads];
+    const double (*gm)[kThreads];
+    int t;
+    __device__ double C(int i) const { return c[i][t]; }
+    __device__ double G(int i) const { return gm[i][t]; }
+};
+
+// cost and (optionally) gradient; returns +inf outside the domain
+__device__ double evaluate(const Args& a, const double (&u)[9], const Seg& sg, double (&g)[9],
+                           bool want_grad) {
+    double S = 0.0, ll = 0.0, Qu[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        S += u[i];
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) acc = fma(qij(a, i, j), u[j], acc);
+        Qu[i] = acc;
+    }
+    double P = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) P = fma(u[i], Qu[i], P);
+    bool ok = S > 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const double ai = u[i] + sg.G(i);
+        ok = ok && ai > 0.0;
+        ll += u[i] - sg.C(i) * log(ai > 0.0 ? ai : 1.0);
+    }
+    if (!ok) return CUDART_INF;
+    if (want_grad) {
+        const double is = 1.0 / S, is2 = is * is;
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            g[i] = (2.0 / 9.0) * (1.0 - sg.C(i) / (u[i] + sg.G(i))) +
+                   a.alpha * (2.0 * Qu[i] * S - P) * is2;
+    }
+    return (2.0 / 9.0) * ll + a.alpha * P / S;
+}
+
+__global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
+    __shared__ float Hm[kPacked][kThreads];  // inverse-Hessian approximation, per thread
+    __shared__ double Cs[9][kThreads], Gs[9][kThreads];
+    const long long HW = (long long)a.H * a.W;
+    const long long idx = (long long)blockIdx.x * kThreads + threadIdx.x;
+    if (idx >= (long long)a.T * HW) return;
+    const int f = (int)(idx / HW);
+    const long long p = idx - (long long)f * HW;
+    const int y = (int)(p / a.W), x = (int)(p - (long long)y * a.W);
+    const float* img = a.data + (long long)f * HW;
+    const float* gmap = a.gamma + (long long)f * a.gstride;
+    const int t = threadIdx.x;
+    double u[9], g[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int yy = min(max(y + r - 1, 0), a.H - 1);
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const int xx = min(max(x + s - 1, 0), a.W - 1);
+            const double dv = img[(long long)yy * a.W + xx];
+            const double gv = gmap[(long long)yy * a.W + xx];
+            u[3 * r + s] = dv;
+            Gs[3 * r + s][t] = gv;
+            Cs[3 * r + s][t] = dv + gv;
+        }
+    }
+    const Seg sg{Cs, Gs, t};
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+#pragma unroll
+        for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0f : 0.0f;
+
+    double fu = evaluate(a, u, sg, g, true);
+    double g0 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) g0 = fmax(g0, fabs(g[i]));
+    int status = NCSB_REACHED_MAXITERS, it = 0;
+    if (!(fu < CUDART_INF)) status = NCSB_INCREASING_GRADIENT;  // infeasible start
+    for (; it < a.max_iters && status == NCSB_REACHED_MAXITERS; ++it) {
+        double gmax = 0.0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) gmax = fmax(gmax, fabs(g[i]));
+        if (gmax <= a.tol * fmax(1.0, g0)) { status = NCSB_SUCCESS; break; }
+        // direction p = -H g
+        double d[9], gd = 0.0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            double acc = 0.0;
+#pragma unroll
+            for (int j = 0; j < 9; ++j)
+                acc = fma((double)Hm[i <= j ? pk(i, j) : pk(j, i)][t], g[j], acc);
+            d[i] = -acc;
+            gd = fma(g[i], d[i], gd);
+        }
+        if (!(gd < 0.0)) {  // lost positive definiteness: restart from steepest descent
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+#pragma unroll
+                for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0f : 0.0f;
+            gd = 0.0;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                d[i] = -g[i];
+                gd = fma(g[i], d[i], gd);
+            }
+        }
+        // backtracking Armijo; trials keep u + gamma >= 1% of its value
+        double step = 1.0, un[9], gn[9], fn = CUDART_INF;
+        bool ok = false;
+        for (int trial = 0; trial < 64; ++trial) {
+            bool feas = true;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                un[i] = fma(step, d[i], u[i]);
+                feas = feas && (un[i] + sg.G(i) >= 0.01 * (u[i] + sg.G(i)));
+            }
+            if (feas) {
+                fn = evaluate(a, un, sg, gn, false);
+                if (fn <= fu + a.c1 * step * gd) { ok = true; break; }
+            }
+            step *= 0.5;
+            if (!(step >= a.min_step)) break;
+        }
+        if (!ok) { status = NCSB_MINIMUM_STEP; break; }
+        fn = evaluate(a, un, sg, gn, true);
+        // BFGS update of the inverse Hessian with s = un - u, y = gn - g
+        double s[9], yv[9], sy = 0.0, yy = 0.0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            s[i] = un[i] - u[i];
+            yv[i] = gn[i] - g[i];
+            sy = fma(s[i], yv[i], sy);
+            yy = fma(yv[i], yv[i], yy);
+        }
+        if (sy > 1e-300) {
+            if (it == 0) {  // scale the identity before the first update
+                const float sc = (float)(sy / yy);
+#pragma unroll
+                for (int i = 0; i < 9; ++i) Hm[pk(i, i)][t] = sc;
+            }
+            double v[9], yHy = 0.0;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                double acc = 0.0;
+#pragma unroll
+                for (int j = 0; j < 9; ++j)
+                    acc = fma((double)Hm[i <= j ? pk(i, j) : pk(j, i)][t], yv[j], acc);
+                v[i] = acc;
+                yHy = fma(yv[i], acc, yHy);
+            }
+            const double rho = 1.0 / sy, k2 = rho * rho * yHy + rho;
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+#pragma unroll
+                for (int j = i; j < 9; ++j) {
+                    const double h = Hm[pk(i, j)][t];
+                    Hm[pk(i, j)][t] =
+                        (float)(h - rho * (v[i] * s[j] + s[i] * v[j]) + k2 * s[i] * s[j]);
+                }
+        }
+        bool moved = false;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            moved = moved || (un[i] != u[i]);
+            u[i] = un[i];
+            g[i] = gn[i];
+        }
+        fu = fn;
+        if (!moved) { status = NCSB_REACHED_MAXPRECISION; ++it; break; }
+    }
+    const float centre = (float)u[4];
+    a.out[idx] = centre < 0.0f ? 1.0e-6f : centre;
+    if (a.iters) a.iters[idx] = it;
+    if (a.status) a.status[idx] = status;
+    if (a.cost) a.cost[idx] = fu;
+}
+
+}  // namespace norm
+}  // namespace ncsb
+
+using namespace ncsb::norm;
+
+extern "C" {
+
+int ncsb_reduce_noise_normalized(const float* images, int n_frames, int height, int width,
+                                 const float* gamma, int gamma_per_frame,
+                                 const float* mask3_centred, double alpha, int max_iters,
+                                 double tolerance, float* out, int32_t* px_iters,
+                                 int32_t* px_status, double* px_cost, void* stream) {
+    if (!images || !gamma || !out || !mask3_centred) return NCSB_EINVAL;
+    if (n_frames < 0 || height <= 0 || width <= 0 || max_iters < 0) return NCSB_EINVAL;
+    if (!(alpha >= 0.0) || !(tolerance >= 0.0)) return NCSB_EINVAL;
+    if (n_frames == 0) return NCSB_OK;
+    // Q[a][b] = (1/9) sum_k Mu_k^2 Re(conj(F_a[k]) F_b[k]), Mu = ifftshift(mask) (the mask
+    // multiplies fftshift(fft2(u))), symmetrised over k -> -k; F_a = fft2 of unit vector a
+    double mu[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const double m = mask3_centred[((i + 1) % 3) * 3 + (j + 1) % 3];
+            if (!(m == m) || m > 1e300 || m < -1e300) return NCSB_EINVAL;
+            mu[i][j] = m * m;
+        }
+    double sym[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) sym[i][j] = 0.5 * (mu[i][j] + mu[(3 - i) % 3][(3 - j) % 3]);
+    Args a{};
+    const double tw = 2.0 * 3.14159265358979323846 / 3.0;
+    for (int p = 0; p < 9; ++p)
+        for (int q = p; q < 9; ++q) {
+            const int p1 = p / 3, p2 = p % 3, q1 = q / 3, q2 = q % 3;
+            double acc = 0.0;
+            for (int k1 = 0; k1 < 3; ++k1)
+                for (int k2 = 0; k2 < 3; ++k2)  // Re(e^{+i th_p} e^{-i th_q}) = cos(th_p - th_q)
+                    acc += sym[k1][k2] * cos(tw * (k1 * (p1 - q1) + k2 * (p2 - q2)));
+            a.q[pk(p, q)] = acc / 9.0;
+        }
+    a.data = images;
+    a.gamma = gamma;
+    a.gstride = gamma_per_frame ? (long long)height * width : 0;
+    a.out = out;
+    a.T = n_frames;
+    a.H = height;
+    a.W = width;
+    a.alpha = alpha;
+    a.tol = tolerance;
+    a.c1 = 1e-4;
+    a.min_step = 1e-12;
+    a.max_iters = max_iters;
+    a.iters = px_iters;
+    a.status = px_status;
+    a.cost = px_cost;
+    const long long n = (long long)n_frames * height * width;
+    normalized_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0,
+                        (cudaStream_t)stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
+}
+
+}  // extern "C"

@@ -57,7 +57,7 @@ class Solver:
     group per tile).
     """
 
-    def __init__(self, alpha=0.2, max_iters=200, m=2, epsilon=1e-5, c1=1e-4, min_step=1e-6,
+    def __init__(self, alpha=0.2, max_iters=200, m=1, epsilon=1e-5, c1=1e-4, min_step=1e-6,
                  mode="spectral", ctas_per_sm=0, device=None):
         self.lib = _lib.load()
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None
@@ -555,3 +555,49 @@ def cReduceNoise(image, gamma, otf_mask, alpha, strict=True, **solver_kwargs):
     res = out[0].cpu().numpy().astype(numpy.float64)
     solver.close()
     return res
+
+
+def reduce_noise_normalized(images, gamma, mask3_centred, alpha=1.0, max_iters=15, tol=1e-6,
+                            stats=False, stream=None):
+    """The normalised single-pixel variant of NCS (the reference's MATLAB
+    package "single pixel with normalization"): 3 x 3 segment per pixel, cost
+    2 LL / 9 + alpha NC / sum(u), defaults alpha 1 and 15 iterations as its
+    demos.  ``images`` [T, H, W] (or [H, W]) and ``gamma`` ([H, W] or
+    [T, H, W]) float32 CUDA tensors; ``mask3_centred`` 3 x 3 (e.g.
+    ``otf.normalized_mask()``).  Returns the denoised stack, or with
+    ``stats`` (out, iters, status, cost) per pixel."""
+    lib = _lib.load()
+    if not isinstance(images, torch.Tensor) or not images.is_cuda or images.dtype != torch.float32:
+        raise TypeError("images must be a float32 CUDA tensor")
+    if images.dim() == 2:
+        images = images.unsqueeze(0)
+    images = images.contiguous()
+    T, H, W = images.shape
+    gamma = gamma.contiguous()
+    if tuple(gamma.shape) == (H, W):
+        per_frame = 0
+    elif tuple(gamma.shape) == (T, H, W):
+        per_frame = 1
+    else:
+        raise ValueError("gamma must be [H, W] or [T, H, W]")
+    m = numpy.ascontiguousarray(numpy.asarray(mask3_centred, dtype=numpy.float32))
+    if m.shape != (3, 3):
+        raise ValueError("the normalised variant takes a 3 x 3 mask")
+    out = torch.empty_like(images)
+    n = T * H * W
+    it = st = cost = None
+    if stats:
+        it = torch.empty(n, dtype=torch.int32, device=images.device)
+        st = torch.empty(n, dtype=torch.int32, device=images.device)
+        cost = torch.empty(n, dtype=torch.float64, device=images.device)
+    s = stream if stream is not None else torch.cuda.current_stream(images.device)
+    with torch.cuda.device(images.device):
+        rc = lib.ncsb_reduce_noise_normalized(
+            _ptr(images), T, H, W, _ptr(gamma), per_frame,
+            m.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(alpha), int(max_iters),
+            float(tol), _ptr(out), _ptr(it), _ptr(st), _ptr(cost), ctypes.c_void_p(s.cuda_stream))
+    if rc != _lib.NCSB_OK:
+        raise ValueError("ncsb_reduce_noise_normalized failed with code %d" % rc)
+    if stats:
+        return out, it.view(T, H, W), st.view(T, H, W), cost.view(T, H, W)
+    return out

@@ -74,3 +74,34 @@ def device_masks(optics_list, device="cuda"):
     if rc != _lib.NCSB_OK:
         raise ValueError("ncsb_genfilter failed with code %d (bad optics?)" % rc)
     return out
+
+
+def genfilter_odd(n, pixelsize, NA, Lambda, Type=None, w=1.0, h=0.7):
+    """Masks of the normalised single-pixel variant (odd n, centred): the
+    reference's "matlab - single pixel with normalization/genfilter.m":30-62,
+    grid -(n-1)/2 .. (n-1)/2, kmax = n / sqrt(2) / (n pixelsize); default type
+    T = lambda / 2 / NA / 1.4, beta = 1."""
+    r = numpy.arange(n) - (n - 1) / 2.0
+    X, Y = numpy.meshgrid(r, r)
+    kr = numpy.sqrt(X ** 2 + Y ** 2) / (n * pixelsize)
+    kmax = n / numpy.sqrt(2.0) / (n * pixelsize)
+    if Type == "pureN":
+        beta = 0.2
+        T = (1 - beta) * Lambda / 2 / NA
+    elif Type == "adjustable":
+        w0 = w * NA / Lambda
+        beta = numpy.pi / 2 * (kmax / w0 - 1) / (numpy.arccos(1 - 2 * h) + numpy.pi / 2 * (kmax / w0 - 1))
+        T = (1 - beta) / w0 / 2
+    else:
+        beta = 1.0
+        T = Lambda / 2 / NA / 1.4
+    rc = 0.5 * (1 + numpy.cos(numpy.pi * T / beta * (kr - (1 - beta) / 2 / T)))
+    rc[kr < (1 - beta) / 2 / T] = 1
+    rc[kr > (1 + beta) / 2 / T] = 0
+    return 1 - rc
+
+
+def normalized_mask(pixelsize=0.1, NA=1.4, Lambda=0.7):
+    """The 3 x 3 mask the normalised variant builds by default: genfilter of
+    the segment size Rs + 2 = 3 with twice the NA (reducenoise.m, otfsize = 2)."""
+    return genfilter_odd(3, pixelsize, 2.0 * NA, Lambda)

@@ -35,7 +35,7 @@ def test_default_params(lib):
     from ncs_b200 import _lib
     p = _lib.default_params()
     assert (p.alpha, p.max_iters, p.m, p.epsilon, p.c1, p.min_step, p.mode) == \
-        (0.2, 200, 2, 1e-5, 1e-4, 1e-6, 2)
+        (0.2, 200, 1, 1e-5, 1e-4, 1e-6, 2)
 
 
 def test_num_tiles_matches_oracle(lib):

@@ -357,6 +357,20 @@ int ncsb_net_infer_stack(const float *params, const float *images, int n_frames,
 int ncsb_net_infer_batch(const float *params, const ncsb_handle *h, float *u0_tiles,
                          void *stream);
 
+/* ncsb_net_infer_stack on the tensor cores (tcgen05): BF16 weights and
+ * activations, FP32 accumulation in tensor memory; the layers as implicit
+ * GEMMs over the zero-bordered 18 x 18 plane (M = 128, N = 32, K = 16).
+ * Results differ from the FP32 kernel by BF16 rounding (about 1e-2 of the
+ * tile's scale s at most).  status (optional, device int32): set to 1 if a
+ * wait for the tensor cores timed out (the kernel then ends early). */
+int ncsb_net_infer_stack_tc(const float *params, const float *images, int n_frames, int height,
+                            int width, const float *gamma, int gamma_per_frame, float *u0_tiles,
+                            int32_t *status, void *stream);
+
+/* The tensor-core inference on tiles d, gamma [n][16][16] -> u0 [n][16][16]. */
+int ncsb_net_infer_tiles_tc(const float *params, const float *d, const float *gamma,
+                            int64_t n_tiles, float *u0, int32_t *status, void *stream);
+
 /* The same inference on tiles d, gamma [n][16][16] -> u0 [n][16][16]. */
 int ncsb_net_infer_tiles(const float *params, const float *d, const float *gamma, int64_t n_tiles,
                          float *u0, void *stream);

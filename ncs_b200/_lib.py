@@ -112,6 +112,7 @@ EXPORTS = [
     "ncsb_batch_set", "ncsb_batch_num_tiles", "ncsb_batch_reduce_noise",
     "ncsb_reduce_noise_adu", "ncsb_genfilter",
     "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms", "ncsb_reduce_noise_normalized",
+    "ncsb_net_infer_stack_tc", "ncsb_net_infer_tiles_tc",
 ]
 
 _lib = None
@@ -179,6 +180,10 @@ def load():
     lib.ncsb_reduce_noise_normalized.restype = ctypes.c_int
     lib.ncsb_genfilter.argtypes = [P(NcsbOptics), ctypes.c_int, vp, vp]
     lib.ncsb_genfilter.restype = ctypes.c_int
+    lib.ncsb_net_infer_stack_tc.argtypes = [vp, vp, ci, ci, ci, vp, ci, vp, vp, vp]
+    lib.ncsb_net_infer_stack_tc.restype = ctypes.c_int
+    lib.ncsb_net_infer_tiles_tc.argtypes = [vp, vp, vp, i64, vp, vp, vp]
+    lib.ncsb_net_infer_tiles_tc.restype = ctypes.c_int
     lib.ncsb_net_infer_batch.argtypes = [vp, vp, vp, vp]
     lib.ncsb_batch_set.argtypes = [vp, P(NcsbStack), ctypes.c_int]
     lib.ncsb_batch_set.restype = ctypes.c_int

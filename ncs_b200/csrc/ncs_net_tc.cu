@@ -1,0 +1,487 @@
+// ncs_net_tc.cu -- warm-start network inference on the 5th-generation tensor
+// cores (tcgen05, sm_100a): the same network as ncs_net.cu's FP32 inference,
+// as implicit GEMMs with BF16 operands and FP32 accumulators in tensor memory.
+//
+// Per 16x16 tile, positions live on the zero-bordered 18 x 18 plane
+// (row-major, index P).  The outputs of a 3x3 layer at the 288 positions
+// P = 18..305 (plane rows 1..16, all 18 columns; the two border columns are
+// computed and discarded) are, for each tap (ky, kx), a GEMM
+//     D[q][co] += sum_ci A[q + 18 + (ky-1)*18 + (kx-1)][ci] * W[tap][ci][co]
+// so the tap is a shift of the A operand's start position: one shared-memory
+// matrix descriptor per tap over the same activation buffer.  M = 128
+// (3 blocks cover the 288 positions), N = 32 (N = 16 for the 1-channel last
+// layer, weights zero-padded), K = 16 per instruction, 2 per 32 channels.
+// The first layer (2 input channels) is one GEMM with an im2col operand,
+// K = 18 taps x channels padded to 32.
+//
+// Shared-memory operands are K-major without swizzle: 8 consecutive
+// positions x 8 channels (16 B each) form a core matrix, so an activation
+// buffer is [channel chunk][position][8] BF16 with the leading byte offset
+// (between K halves) = the chunk stride and the stride byte offset (between
+// 8-row groups) = 128 B.  The epilogue reads each accumulator row from tensor
+// memory (thread t of the 128 owns row t of every M block), adds the bias,
+// applies ReLU, rounds to BF16 and writes the next layer's operand -- zeros at
+// the plane's border positions, which are the next layer's zero padding.
+//
+// One CTA (4 warps) per SM, persistent over tiles; thread 0 issues the MMAs
+// and commits them to an mbarrier that all threads wait on.  Every wait is
+// bounded; a timed-out wait sets the caller's status flag, drains with a
+// second bounded wait, frees the tensor memory and ends the kernel.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/ncs_b200.h"
+
+namespace ncsb {
+namespace nettc {
+
+constexpr int kC = 32;
+constexpr int kThreads = 128;
+constexpr int kPlane = 18;
+constexpr int kQ = 384;                  // 3 M blocks of 128 output positions
+constexpr int kPos = 424;                // activation positions incl. shift margins
+constexpr int kChunkA = kPos * 16;       // bytes per 8-channel chunk of an activation buffer
+constexpr int kActBytes = 4 * kChunkA;   // 32 channels
+constexpr int kChunkI = kQ * 16;         // im2col chunk
+constexpr int kIm2colBytes = 4 * kChunkI;
+constexpr int kW1Bytes = 4 * 32 * 16;            // layer 1: K 32 x N 32
+constexpr int kWtapBytes = 4 * 32 * 16;          // layers 2, 3: per tap K 32 x N 32
+constexpr int kW4tapBytes = 4 * 16 * 16;         // layer 4: per tap K 32 x N 16
+constexpr float kStartFrac = 0.05f;
+constexpr unsigned kTmemCols = 128;
+constexpr long long kWaitLimit = 1ll << 22;  // mbarrier polls before giving up (seconds)
+
+// shared-memory plan (bytes, all 128-B aligned)
+constexpr int kOffW1 = 0;
+constexpr int kOffW2 = kOffW1 + kW1Bytes;
+constexpr int kOffW3 = kOffW2 + 9 * kWtapBytes;
+constexpr int kOffW4 = kOffW3 + 9 * kWtapBytes;
+constexpr int kOffAct0 = kOffW4 + 9 * kW4tapBytes;
+constexpr int kOffAct1 = kOffAct0 + kActBytes;
+constexpr int kOffIm2col = kOffAct1 + kActBytes;
+constexpr int kOffBias = kOffIm2col + kIm2colBytes;          // 3 x 32 + 1 floats
+constexpr int kOffTile = kOffBias + 128 * 4;                  // d, gamma, x0, x1: 4 x 256 floats
+constexpr int kSmemBytes = kOffTile + 4 * 256 * 4;
+
+struct Src {
+    int tile_mode;
+    const float* d;
+    const float* gamma;
+    long long gamma_frame_stride;
+    int H, W, tiles_x, tiles_y;
+    long long n_tiles;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// K-major, no swizzle (layout type 0), Blackwell descriptor version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: D F32, A and B BF16, both K-major.
+__host__ __device__ constexpr uint32_t idesc(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id,
+                                    uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void commit(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ bool try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool wait_bounded(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < kWaitLimit; ++i)
+        if (try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 32 consecutive FP32 accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+__device__ __forceinline__ int tile_origin(int i, int n) {
+    const int o = 14 * i, last = n + 2 - 16;
+    return o < last ? o : last;
+}
+
+// Store 32 channels of one position into a [chunk][pos][8] BF16 buffer.
+__device__ __forceinline__ void store_pos(unsigned char* buf, int chunk_bytes, int pos,
+                                          const float (&v)[32]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        uint4 w;
+        w.x = pack2(v[8 * k + 0], v[8 * k + 1]);
+        w.y = pack2(v[8 * k + 2], v[8 * k + 3]);
+        w.z = pack2(v[8 * k + 4], v[8 * k + 5]);
+        w.w = pack2(v[8 * k + 6], v[8 * k + 7]);
+        *reinterpret_cast<uint4*>(buf + k * chunk_bytes + pos * 16) = w;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    infer_tc(const Src src, const float* __restrict__ params, float* __restrict__ u0,
+             int32_t* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ float red[8];
+    const int t = threadIdx.x, warp = t >> 5;
+
+    // ---- weights -> BF16 operand layouts, biases, zeroed activations --------
+    const float* w1 = params;
+    const float* b1 = w1 + 2 * 9 * kC;
+    const float* w2 = b1 + kC;
+    const float* b2 = w2 + kC * 9 * kC;
+    const float* w3 = b2 + kC;
+    const float* b3 = w3 + kC * 9 * kC;
+    const float* w4 = b3 + kC;
+    const float* b4 = w4 + kC * 9;
+    __nv_bfloat16* sW1 = reinterpret_cast<__nv_bfloat16*>(sm + kOffW1);
+    // layer 1, B[k][co] with k = tap * 2 + ci (18 used of 32): [k chunk][co][8]
+    for (int i = t; i < 32 * 32; i += kThreads) {
+        const int k = i >> 5, co = i & 31;
+        const float v = k < 18 ? w1[((k & 1) * 9 + (k >> 1)) * kC + co] : 0.0f;
+        sW1[(k >> 3) * 256 + co * 8 + (k & 7)] = __float2bfloat16_rn(v);
+    }
+    for (int l = 0; l < 2; ++l) {
+        const float* w = l == 0 ? w2 : w3;
+        __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(sm + (l == 0 ? kOffW2 : kOffW3));
+        for (int i = t; i < 9 * 32 * 32; i += kThreads) {
+            const int tap = i / 1024, rem = i - tap * 1024, ci = rem >> 5, co = rem & 31;
+            sW[tap * 1024 + (ci >> 3) * 256 + co * 8 + (ci & 7)] =
+                __float2bfloat16_rn(w[(ci * 9 + tap) * kC + co]);
+        }
+    }
+    {
+        __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(sm + kOffW4);
+        for (int i = t; i < 9 * 32 * 16; i += kThreads) {
+            const int tap = i / 512, rem = i - tap * 512, ci = rem >> 4, co = rem & 15;
+            sW[tap * 512 + (ci >> 3) * 128 + co * 8 + (ci & 7)] =
+                __float2bfloat16_rn(co == 0 ? w4[ci * 9 + tap] : 0.0f);
+        }
+    }
+    float* sBias = reinterpret_cast<float*>(sm + kOffBias);
+    for (int i = t; i < 97; i += kThreads)
+        sBias[i] = i < 32 ? b1[i] : (i < 64 ? b2[i - 32] : (i < 96 ? b3[i - 64] : b4[0]));
+    for (int i = t; i < 2 * kActBytes / 16; i += kThreads)
+        reinterpret_cast<uint4*>(sm + kOffAct0)[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base_s)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_base_s;
+    const uint32_t bar_a = smem_u32(&bar);
+    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;  // this warp's TMEM lanes
+    uint32_t phase = 0;
+    bool alive = true;
+
+    float* sD = reinterpret_cast<float*>(sm + kOffTile);
+    float* sG = sD + 256;
+    float* sX0 = sG + 256;
+    float* sX1 = sX0 + 256;
+    unsigned char* act[2] = {sm + kOffAct0, sm + kOffAct1};
+    unsigned char* im2col = sm + kOffIm2col;
+    const uint32_t sW1a = smem_u32(sm + kOffW1), sW2a = smem_u32(sm + kOffW2);
+    const uint32_t sW3a = smem_u32(sm + kOffW3), sW4a = smem_u32(sm + kOffW4);
+    const uint32_t act_a[2] = {smem_u32(act[0]), smem_u32(act[1])};
+    const uint32_t im_a = smem_u32(im2col);
+    const long long per_frame = (long long)src.tiles_x * src.tiles_y;
+
+    // all threads: wait for the committed MMAs (block-uniform outcome)
+    // (on a timeout the phase stays, so the drain below waits on the same one)
+    auto sync_mma = [&]() -> bool {
+        const bool ok = wait_bounded(bar_a, phase);
+        const bool all = __syncthreads_and(ok) != 0;
+        if (all) phase ^= 1u;
+        fence_after();
+        return all;
+    };
+
+    for (long long tile = blockIdx.x; tile < src.n_tiles && alive; tile += gridDim.x) {
+        // ---- gather the tile, features, layer-1 im2col operand ---------------
+        float dv[2], gv[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int p = t + 128 * h, r = p >> 4, c = p & 15;
+            if (src.tile_mode) {
+                dv[h] = src.d[tile * 256 + p];
+                gv[h] = src.gamma[tile * 256 + p];
+            } else {
+                const int f = (int)(tile / per_frame);
+                const int rem = (int)(tile - (long long)f * per_frame);
+                const int ti = rem / src.tiles_y, tj = rem - ti * src.tiles_y;
+                const int yy = clampi(tile_origin(ti, src.H) + r - 1, 0, src.H - 1);
+                const int xx = clampi(tile_origin(tj, src.W) + c - 1, 0, src.W - 1);
+                dv[h] = src.d[(long long)f * src.H * src.W + (long long)yy * src.W + xx];
+                gv[h] = src.gamma[(long long)f * src.gamma_frame_stride + (long long)yy * src.W + xx];
+            }
+        }
+        float s1 = dv[0] + dv[1], s2 = dv[0] * dv[0] + dv[1] * dv[1];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        }
+        if ((t & 31) == 0) {
+            red[warp] = s1;
+            red[4 + warp] = s2;
+        }
+        __syncthreads();  // also: the previous tile's readers of sD / sX are done
+        const float mu = (red[0] + red[1] + red[2] + red[3]) * (1.0f / 256.0f);
+        const float sd = sqrtf(fmaxf((red[4] + red[5] + red[6] + red[7]) * (1.0f / 256.0f) -
+                                     mu * mu, 0.0f)) + 1.0f;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int p = t + 128 * h;
+            sD[p] = dv[h];
+            sG[p] = gv[h];
+            sX0[p] = (dv[h] - mu) / sd;
+            sX1[p] = sqrtf(fmaxf(dv[h], 0.0f) + fmaxf(gv[h], 0.0f)) / sd;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int m = 0; m < 3; ++m) {
+            const int q = 128 * m + t, P = q + kPlane;
+            const int R = P / kPlane, Cc = P - R * kPlane;
+            float v[32];
+#pragma unroll
+            for (int tap = 0; tap < 9; ++tap) {
+                const int rr = R + tap / 3 - 1, cc = Cc + tap % 3 - 1;
+                const bool in = rr >= 1 && rr <= 16 && cc >= 1 && cc <= 16;
+                const int px = in ? (rr - 1) * 16 + (cc - 1) : 0;
+                v[2 * tap] = in ? sX0[px] : 0.0f;
+                v[2 * tap + 1] = in ? sX1[px] : 0.0f;
+            }
+#pragma unroll
+            for (int k = 18; k < 32; ++k) v[k] = 0.0f;
+            store_pos(im2col, kChunkI, q, v);
+        }
+
+        // ---- the four layers ---------------------------------------------------
+        int cur = 0;  // activation buffer holding the current layer's input
+        for (int layer = 0; layer < 4 && alive; ++layer) {
+            fence_async_smem();
+            fence_before();
+            __syncthreads();
+            if (t == 0) {
+                fence_after();
+                if (layer == 0) {
+                    const uint32_t id = idesc(128, 32);
+                    for (int m = 0; m < 3; ++m)
+                        for (int ks = 0; ks < 2; ++ks)
+                            mma(tmem + m * 32,
+                                sdesc(im_a + (2 * ks) * kChunkI + 128 * m * 16, kChunkI, 128),
+                                sdesc(sW1a + (2 * ks) * 512, 512, 128), id, ks);
+                } else {
+                    const bool last = layer == 3;
+                    const uint32_t id = last ? idesc(128, 16) : idesc(128, 32);
+                    const uint32_t wa = layer == 1 ? sW2a : (layer == 2 ? sW3a : sW4a);
+                    const int tap_bytes = last ? kW4tapBytes : kWtapBytes;
+                    const int wchunk = last ? 256 : 512;
+                    for (int m = 0; m < 3; ++m)
+                        for (int tap = 0; tap < 9; ++tap)
+                            for (int ks = 0; ks < 2; ++ks) {
+                                const int pos = kPlane + 128 * m + (tap / 3 - 1) * kPlane +
+                                                (tap % 3 - 1) + 1;
+                                mma(tmem + m * (last ? 16 : 32),
+                                    sdesc(act_a[cur] + (2 * ks) * kChunkA + pos * 16, kChunkA, 128),
+                                    sdesc(wa + tap * tap_bytes + (2 * ks) * wchunk, wchunk, 128),
+                                    id, (tap | ks) != 0);
+                            }
+                }
+                commit(bar_a);
+            }
+            if (!sync_mma()) {
+                alive = false;
+                break;
+            }
+            // ---- epilogue: this thread's accumulator row of each M block ---------
+            if (layer < 3) {
+                const float* bias = sBias + 32 * layer;
+                unsigned char* dst = act[layer == 0 ? 0 : cur ^ 1];
+#pragma unroll 1
+                for (int m = 0; m < 3; ++m) {
+                    const int q = 128 * m + t, P = q + kPlane;
+                    const int R = P / kPlane, Cc = P - R * kPlane;
+                    const bool valid = q < 288 && Cc >= 1 && Cc <= 16;
+                    float v[32];
+                    tmem_ld32(tmem + lane_off + m * 32, v);
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) v[i] = valid ? fmaxf(v[i] + bias[i], 0.0f) : 0.0f;
+                    store_pos(dst, kChunkA, P + 1, v);
+                }
+                cur = layer == 0 ? 0 : cur ^ 1;
+            } else {
+#pragma unroll 1
+                for (int m = 0; m < 3; ++m) {
+                    const int q = 128 * m + t, P = q + kPlane;
+                    const int R = P / kPlane, Cc = P - R * kPlane;
+                    float v[32];
+                    tmem_ld32(tmem + lane_off + m * 16, v);  // columns 0..15 used (+16 unused)
+                    if (q < 288 && Cc >= 1 && Cc <= 16) {
+                        const int px = (R - 1) * 16 + (Cc - 1);
+                        const float y = v[0] + sBias[96];
+                        const float d = sD[px], g = sG[px];
+                        const float lo = kStartFrac * fmaxf(d + g, 1e-3f) - g;
+                        u0[tile * 256 + px] = fmaxf(fmaf(sd, y, d), lo);
+                    }
+                }
+            }
+        }
+    }
+
+    if (!alive) {
+        if (t == 0 && status) atomicExch(status, 1);
+        // drain: give the outstanding MMAs a bounded time to complete
+        wait_bounded(bar_a, phase);
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+int tiles_along(int n) {
+    const int last = n + 2 - 16;
+    int count = 0;
+    for (int b = 0;; b += 14) {
+        ++count;
+        if (b >= last) break;
+    }
+    return count;
+}
+
+int launch(const Src& src, const float* params, float* u0, int32_t* status, cudaStream_t s) {
+    if (cudaFuncSetAttribute(infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) !=
+        cudaSuccess)
+        return NCSB_ECUDA;
+    int dev = 0, sms = 1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NCSB_ECUDA;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long grid = sms;
+    if (grid > src.n_tiles) grid = src.n_tiles;
+    infer_tc<<<(unsigned)grid, kThreads, kSmemBytes, s>>>(src, params, u0, status);
+    return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
+}
+
+static_assert(kSmemBytes <= 200 * 1024, "shared-memory plan");
+static_assert(kOffAct0 % 1024 == 0 && kOffAct1 % 16 == 0 && kOffIm2col % 16 == 0, "alignment");
+
+}  // namespace nettc
+}  // namespace ncsb
+
+using namespace ncsb::nettc;
+
+extern "C" {
+
+int ncsb_net_infer_stack_tc(const float* params, const float* images, int n_frames, int height,
+                            int width, const float* gamma, int gamma_per_frame, float* u0,
+                            int32_t* status, void* stream) {
+    if (!params || !images || !gamma || !u0 || n_frames < 0 || height <= 0 || width <= 0)
+        return NCSB_EINVAL;
+    if (height < 14 || width < 14) return NCSB_ESIZE;
+    if (n_frames == 0) return NCSB_OK;
+    Src src{};
+    src.d = images;
+    src.gamma = gamma;
+    src.gamma_frame_stride = gamma_per_frame ? (long long)height * width : 0;
+    src.H = height;
+    src.W = width;
+    src.tiles_x = tiles_along(height);
+    src.tiles_y = tiles_along(width);
+    src.n_tiles = (long long)n_frames * src.tiles_x * src.tiles_y;
+    return launch(src, params, u0, status, (cudaStream_t)stream);
+}
+
+int ncsb_net_infer_tiles_tc(const float* params, const float* d, const float* gamma,
+                            int64_t n_tiles, float* u0, int32_t* status, void* stream) {
+    if (!params || !d || !gamma || !u0 || n_tiles < 0) return NCSB_EINVAL;
+    if (n_tiles == 0) return NCSB_OK;
+    Src src{};
+    src.tile_mode = 1;
+    src.d = d;
+    src.gamma = gamma;
+    src.tiles_x = 1;
+    src.tiles_y = 1;
+    src.H = 16;
+    src.W = 16;
+    src.n_tiles = n_tiles;
+    return launch(src, params, u0, status, (cudaStream_t)stream);
+}
+
+}  // extern "C"

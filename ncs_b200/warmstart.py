@@ -133,6 +133,33 @@ class WarmStartNet:
                 "ncsb_net_infer_batch")
         return out
 
+    def propose_stack_tc(self, images, gamma, out=None, stream=None):
+        """``propose_stack`` on the tensor cores (BF16 operands, FP32
+        accumulation).  Returns (proposals, status) with status a one-element
+        int32 device tensor, 1 if a tensor-core wait timed out."""
+        T, H, W = images.shape
+        per_frame = 1 if gamma.dim() == 3 else 0
+        n = _lib.num_tiles(T, H, W)
+        if out is None:
+            out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
+        status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_net_infer_stack_tc(
+                _ptr(self.params), _ptr(images.contiguous()), T, H, W, _ptr(gamma.contiguous()),
+                per_frame, _ptr(out), _ptr(status), _stream_ptr(stream, self.device)),
+                "ncsb_net_infer_stack_tc")
+        return out, status
+
+    def propose_tiles_tc(self, d, gamma, stream=None):
+        n = d.shape[0]
+        out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
+        status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_net_infer_tiles_tc(
+                _ptr(self.params), _ptr(d.contiguous()), _ptr(gamma.contiguous()), n, _ptr(out),
+                _ptr(status), _stream_ptr(stream, self.device)), "ncsb_net_infer_tiles_tc")
+        return out, status
+
     def propose_tiles(self, d, gamma, stream=None):
         n = d.shape[0]
         out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)

@@ -23,7 +23,8 @@
 // applies ReLU, rounds to BF16 and writes the next layer's operand -- zeros at
 // the plane's border positions, which are the next layer's zero padding.
 //
-// One CTA (4 warps) per SM, persistent over tiles; thread 0 issues the MMAs
+// Two CTAs (4 warps each) per SM, persistent over tiles, so one CTA's
+// epilogue overlaps the other's MMAs; thread 0 of a CTA issues its MMAs
 // and commits them to an mbarrier that all threads wait on.  Every wait is
 // bounded; a timed-out wait sets the caller's status flag, drains with a
 // second bounded wait, frees the tensor memory and ends the kernel.
@@ -43,14 +44,12 @@ constexpr int kQ = 384;                  // 3 M blocks of 128 output positions
 constexpr int kPos = 424;                // activation positions incl. shift margins
 constexpr int kChunkA = kPos * 16;       // bytes per 8-channel chunk of an activation buffer
 constexpr int kActBytes = 4 * kChunkA;   // 32 channels
-constexpr int kChunkI = kQ * 16;         // im2col chunk
-constexpr int kIm2colBytes = 4 * kChunkI;
 constexpr int kW1Bytes = 4 * 32 * 16;            // layer 1: K 32 x N 32
 constexpr int kWtapBytes = 4 * 32 * 16;          // layers 2, 3: per tap K 32 x N 32
 constexpr int kW4tapBytes = 4 * 16 * 16;         // layer 4: per tap K 32 x N 16
 constexpr float kStartFrac = 0.05f;
 constexpr unsigned kTmemCols = 128;
-constexpr long long kWaitLimit = 1ll << 22;  // mbarrier polls before giving up (seconds)
+constexpr long long kWaitTries = 1ll << 22;  // mbarrier polls before giving up (seconds)
 
 // shared-memory plan (bytes, all 128-B aligned)
 constexpr int kOffW1 = 0;
@@ -59,8 +58,11 @@ constexpr int kOffW3 = kOffW2 + 9 * kWtapBytes;
 constexpr int kOffW4 = kOffW3 + 9 * kWtapBytes;
 constexpr int kOffAct0 = kOffW4 + 9 * kW4tapBytes;
 constexpr int kOffAct1 = kOffAct0 + kActBytes;
-constexpr int kOffIm2col = kOffAct1 + kActBytes;
-constexpr int kOffBias = kOffIm2col + kIm2colBytes;          // 3 x 32 + 1 floats
+// the layer-1 im2col operand lives in activation buffer 1 at positions
+// 19..402 -- the range the later epilogue rewrites -- so the zero border
+// positions of that buffer are never touched
+constexpr int kIm2colPos = 19;
+constexpr int kOffBias = kOffAct1 + kActBytes;                // 3 x 32 + 1 floats
 constexpr int kOffTile = kOffBias + 128 * 4;                  // d, gamma, x0, x1: 4 x 256 floats
 constexpr int kSmemBytes = kOffTile + 4 * 256 * 4;
 
@@ -118,7 +120,7 @@ __device__ __forceinline__ bool try_wait(uint32_t bar, uint32_t parity) {
 }
 
 __device__ __forceinline__ bool wait_bounded(uint32_t bar, uint32_t parity) {
-    for (long long i = 0; i < kWaitLimit; ++i)
+    for (long long i = 0; i < kWaitTries; ++i)
         if (try_wait(bar, parity)) return true;
     return false;
 }
@@ -180,7 +182,7 @@ __device__ __forceinline__ void store_pos(unsigned char* buf, int chunk_bytes, i
     }
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 2)
     infer_tc(const Src src, const float* __restrict__ params, float* __restrict__ u0,
              int32_t* __restrict__ status) {
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -251,15 +253,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     float* sX0 = sG + 256;
     float* sX1 = sX0 + 256;
     unsigned char* act[2] = {sm + kOffAct0, sm + kOffAct1};
-    unsigned char* im2col = sm + kOffIm2col;
+    unsigned char* im2col = sm + kOffAct1 + kIm2colPos * 16;
     const uint32_t sW1a = smem_u32(sm + kOffW1), sW2a = smem_u32(sm + kOffW2);
     const uint32_t sW3a = smem_u32(sm + kOffW3), sW4a = smem_u32(sm + kOffW4);
     const uint32_t act_a[2] = {smem_u32(act[0]), smem_u32(act[1])};
-    const uint32_t im_a = smem_u32(im2col);
+    const uint32_t im_a = smem_u32(im2col);  // chunk stride kChunkA, like the activations
     const long long per_frame = (long long)src.tiles_x * src.tiles_y;
 
-    // all threads: wait for the committed MMAs (block-uniform outcome)
-    // (on a timeout the phase stays, so the drain below waits on the same one)
+    // all threads: wait for the layer's committed MMAs (block-uniform outcome;
+    // on a timeout the phase stays, so the drain below waits on the same one)
     auto sync_mma = [&]() -> bool {
         const bool ok = wait_bounded(bar_a, phase);
         const bool all = __syncthreads_and(ok) != 0;
@@ -268,9 +270,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         return all;
     };
 
-    for (long long tile = blockIdx.x; tile < src.n_tiles && alive; tile += gridDim.x) {
-        // ---- gather the tile, features, layer-1 im2col operand ---------------
-        float dv[2], gv[2];
+    // this thread's two pixels of a tile (the solvers' segmentation)
+    auto gather = [&](long long tile, float (&dv)[2], float (&gv)[2]) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int p = t + 128 * h, r = p >> 4, c = p & 15;
@@ -287,6 +288,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                 gv[h] = src.gamma[(long long)f * src.gamma_frame_stride + (long long)yy * src.W + xx];
             }
         }
+    };
+    float dv[2] = {0.0f, 0.0f}, gv[2] = {0.0f, 0.0f};
+    if ((long long)blockIdx.x < src.n_tiles) gather(blockIdx.x, dv, gv);
+
+    for (long long tile = blockIdx.x; tile < src.n_tiles && alive; tile += gridDim.x) {
+        // ---- features, layer-1 im2col operand ----------------------------------
         float s1 = dv[0] + dv[1], s2 = dv[0] * dv[0] + dv[1] * dv[1];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -325,8 +332,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
 #pragma unroll
             for (int k = 18; k < 32; ++k) v[k] = 0.0f;
-            store_pos(im2col, kChunkI, q, v);
+            store_pos(im2col, kChunkA, q, v);
         }
+
+        // the next tile's pixels load while this tile's layers run
+        float ndv[2] = {0.0f, 0.0f}, ngv[2] = {0.0f, 0.0f};
+        if (tile + gridDim.x < src.n_tiles) gather(tile + gridDim.x, ndv, ngv);
 
         // ---- the four layers ---------------------------------------------------
         int cur = 0;  // activation buffer holding the current layer's input
@@ -335,29 +346,34 @@ __global__ void __launch_bounds__(kThreads, 1)
             fence_before();
             __syncthreads();
             if (t == 0) {
+                // descriptors are built once per layer; an operand offset is
+                // added to the start-address field (shared addresses < 256 KB,
+                // so the 14-bit field never carries)
                 fence_after();
                 if (layer == 0) {
                     const uint32_t id = idesc(128, 32);
+                    const uint64_t a0 = sdesc(im_a, kChunkA, 128), b0 = sdesc(sW1a, 512, 128);
                     for (int m = 0; m < 3; ++m)
                         for (int ks = 0; ks < 2; ++ks)
-                            mma(tmem + m * 32,
-                                sdesc(im_a + (2 * ks) * kChunkI + 128 * m * 16, kChunkI, 128),
-                                sdesc(sW1a + (2 * ks) * 512, 512, 128), id, ks);
+                            mma(tmem + m * 32, a0 + (((2 * ks) * kChunkA + 128 * m * 16) >> 4),
+                                b0 + (((2 * ks) * 512) >> 4), id, ks);
                 } else {
                     const bool last = layer == 3;
                     const uint32_t id = last ? idesc(128, 16) : idesc(128, 32);
                     const uint32_t wa = layer == 1 ? sW2a : (layer == 2 ? sW3a : sW4a);
                     const int tap_bytes = last ? kW4tapBytes : kWtapBytes;
                     const int wchunk = last ? 256 : 512;
+                    const uint64_t a0 = sdesc(act_a[cur], kChunkA, 128);
+                    const uint64_t b0 = sdesc(wa, wchunk, 128);
                     for (int m = 0; m < 3; ++m)
                         for (int tap = 0; tap < 9; ++tap)
                             for (int ks = 0; ks < 2; ++ks) {
                                 const int pos = kPlane + 128 * m + (tap / 3 - 1) * kPlane +
                                                 (tap % 3 - 1) + 1;
                                 mma(tmem + m * (last ? 16 : 32),
-                                    sdesc(act_a[cur] + (2 * ks) * kChunkA + pos * 16, kChunkA, 128),
-                                    sdesc(wa + tap * tap_bytes + (2 * ks) * wchunk, wchunk, 128),
-                                    id, (tap | ks) != 0);
+                                    a0 + (((2 * ks) * kChunkA + pos * 16) >> 4),
+                                    b0 + ((tap * tap_bytes + (2 * ks) * wchunk) >> 4), id,
+                                    (tap | ks) != 0);
                             }
                 }
                 commit(bar_a);
@@ -399,6 +415,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             }
         }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            dv[h] = ndv[h];
+            gv[h] = ngv[h];
+        }
     }
 
     if (!alive) {
@@ -430,17 +451,26 @@ int launch(const Src& src, const float* params, float* u0, int32_t* status, cuda
     if (cudaFuncSetAttribute(infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) !=
         cudaSuccess)
         return NCSB_ECUDA;
+    // all of the unified L1 as shared memory, so two CTAs fit on an SM
+    cudaFuncSetAttribute(infer_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     int dev = 0, sms = 1;
     if (cudaGetDevice(&dev) != cudaSuccess) return NCSB_ECUDA;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    long long grid = sms;
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, infer_tc, kThreads, kSmemBytes) !=
+            cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    long long grid = (long long)sms * per_sm;
     if (grid > src.n_tiles) grid = src.n_tiles;
     infer_tc<<<(unsigned)grid, kThreads, kSmemBytes, s>>>(src, params, u0, status);
     return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
 }
 
-static_assert(kSmemBytes <= 200 * 1024, "shared-memory plan");
-static_assert(kOffAct0 % 1024 == 0 && kOffAct1 % 16 == 0 && kOffIm2col % 16 == 0, "alignment");
+static_assert(2 * (kSmemBytes + 2048) <= 228 * 1024, "two CTAs per SM");
+static_assert(kOffAct0 % 1024 == 0 && kOffAct1 % 16 == 0, "alignment");
+static_assert(kIm2colPos + kQ <= kPos - 21, "im2col rows stay inside the rewritten range");
 
 }  // namespace nettc
 }  // namespace ncsb

@@ -457,11 +457,13 @@ int launch(const Src& src, const float* params, float* u0, int32_t* status, cuda
     int dev = 0, sms = 1;
     if (cudaGetDevice(&dev) != cudaSuccess) return NCSB_ECUDA;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, infer_tc, kThreads, kSmemBytes) !=
-            cudaSuccess ||
-        per_sm < 1)
-        per_sm = 1;
+    // CTAs per SM from the shared-memory budget (the occupancy query assumes the
+    // default carveout); more CTAs than fit only queue, results do not change
+    int per_sm_bytes = 0, reserved = 0;
+    cudaDeviceGetAttribute(&per_sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    int per_sm = per_sm_bytes / (kSmemBytes + 1024 + reserved);  // + static shared memory
+    per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
     long long grid = (long long)sms * per_sm;
     if (grid > src.n_tiles) grid = src.n_tiles;
     infer_tc<<<(unsigned)grid, kThreads, kSmemBytes, s>>>(src, params, u0, status);

@@ -338,7 +338,9 @@ class Solver:
         if T == 0:
             return out
         if chunk_frames is None:
-            chunk_frames = max(1, -(-T // 8))
+            # 16 chunks: short pipeline fill and drain, chunks still large enough to
+            # fill the GPU (200 x 512 x 512 on B200: 5.1 ms vs 5.4 ms with 8 chunks)
+            chunk_frames = max(1, -(-T // 16))
         chunk_frames = max(1, min(int(chunk_frames), T))
         n_streams = max(1, int(n_streams))
         if self.mask_shifted is None:

@@ -511,8 +511,9 @@ KernelFn spectral_variant_m(int blocks, bool warm, bool batch, bool adu) {
 }
 
 KernelFn spectral_variant(int blocks, int m, bool warm, bool batch, bool adu = false) {
-    return m <= 2 ? spectral_variant_m<2>(blocks, warm, batch, adu)
-                  : spectral_variant_m<4>(blocks, warm, batch, adu);
+    return m <= 1 ? spectral_variant_m<1>(blocks, warm, batch, adu)
+                  : (m <= 2 ? spectral_variant_m<2>(blocks, warm, batch, adu)
+                            : spectral_variant_m<4>(blocks, warm, batch, adu));
 }
 
 int spectral_default_blocks(int m) {

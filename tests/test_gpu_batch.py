@@ -153,3 +153,25 @@ def test_batch_errors(ncs, stacks):
     p.batch_set([stacks[1]])
     with pytest.raises(RuntimeError):
         p.batch_reduce_noise()                     # spectral form only
+
+
+def test_autotuner_picks_a_timed_candidate_and_caches(ncs, stacks, tmp_path):
+    from ncs_b200 import tune
+    s = ncs.Solver()
+    outs = s.batch_set(stacks)
+    key = tune.batch_key(s) + "/test"
+    cands = ({"ctas_per_sm": 3, "m": 1}, {"ctas_per_sm": 1, "m": 2})
+    path = str(tmp_path / "tune.json")
+    best, tried = tune.autotune(s, lambda: s.batch_reduce_noise(), key, candidates=cands,
+                                path=path)
+    assert best in cands and len(tried) == 2
+    assert best == min(tried, key=lambda x: x[0])[1]
+    assert (s.params.ctas_per_sm, s.params.m) == (best["ctas_per_sm"], best["m"])
+    # whichever candidate wins, the stopping rule is the same: every tile converges
+    stats = s.batch_stats()
+    s.batch_reduce_noise(stats=stats)
+    torch.cuda.synchronize()
+    assert (stats["status"] == 0).all()
+    # cached: a second call returns the stored choice without timing
+    best2, _ = tune.autotune(s, lambda: 1 / 0, key, candidates=cands, path=path)
+    assert best2 == best

@@ -22,6 +22,7 @@ all host cores instead.
 """
 import argparse
 import ctypes
+import datetime
 import json
 import os
 import statistics
@@ -74,8 +75,9 @@ def fp32_peak_tflops(sm_mhz, n_sms):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (200 ms period)."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi sampling (20 ms period) around the timed region; the samples
+    whose timestamps fall inside it are the ones reported."""
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -83,22 +85,35 @@ class Clocks:
         self.index = index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def start(self):
+        """Start sampling; returns once the first sample has been written."""
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        deadline = time.time() + 5.0
+        while time.time() < deadline and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
+
+    def begin(self):
+        self.t0 = time.time()
+
+    def end(self):
+        self.t1 = time.time()
 
     def stop(self):
         if self.proc is None:
             return None
+        time.sleep(0.05)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -109,18 +124,29 @@ class Clocks:
         with open(self.path) as f:
             for line in f:
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
+                if len(parts) >= 10:
+                    try:
+                        parts[0] = datetime.datetime.strptime(
+                            parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    except ValueError:
+                        continue
                     rows.append(parts)
         os.unlink(self.path)
-        if not rows:
+        inside = rows
+        if self.t0 is not None and self.t1 is not None:
+            inside = [r for r in rows if self.t0 - 0.02 <= r[0] <= self.t1 + 0.02]
+        window = "timed region"
+        if not inside:  # region shorter than the sampling period: nearest samples
+            inside, window = rows, "sampling run around the timed region"
+        if not inside:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        sm = [float(r[2]) for r in inside if r[2].replace(".", "", 1).isdigit()]
+        mx = [float(r[3]) for r in inside if r[3].replace(".", "", 1).isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        reasons = sorted({names[i] for r in inside for i in range(4) if r[6 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(inside), "window": window}
 
 
 def dist_setup():
@@ -334,15 +360,16 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     clocks = Clocks(local)
     clocks.start()
-    time.sleep(0.3)
     barrier(world)
     torch.cuda.synchronize()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    clocks.begin()
     ev[0].record(stream)
     for k in range(args.steps):
         solver.reduce_noise(images, gamma, out=out)
         ev[k + 1].record(stream)
     torch.cuda.synchronize()
+    clocks.end()
     barrier(world)
     clk = clocks.stop()
     per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
@@ -579,15 +606,16 @@ def run_mixed(args, world, rank, local):
     stream = torch.cuda.current_stream(dev)
     clocks = Clocks(local)
     clocks.start()
-    time.sleep(0.3)
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.begin()
     e0.record(stream)
     for _ in range(args.steps):
         graph.replay()
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks.end()
     barrier(world)
     clk = clocks.stop()
     total_ms = max_over_ranks(e0.elapsed_time(e1), world)

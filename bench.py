@@ -37,7 +37,7 @@ import torch
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic FP32 work per tile ("Roofline").  A real 16x16
+# Algorithmic FP32 work per tile, the roofline numerator.  A real 16x16
 # 2-D FFT is counted as 2.5 N log2 N = 5,120 flops (N = 256).
 #   start (both forms): Q u by a forward + inverse FFT and the spectrum
 #     weighting (11,264), gradient and norms (3,328)              14,592

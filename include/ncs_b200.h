@@ -204,6 +204,14 @@ typedef struct {
  * device.  NCSB_EINVAL for an unknown type or non-positive parameters. */
 int ncsb_genfilter(const ncsb_optics *optics, int n, float *masks_centred, void *stream);
 
+/* genpsfparam of the reference (python3-6/pyNCS/denoisetools.py:103-115) on
+ * the device, FP64: pupil = |k| on the centred R x R grid (genkspace), 0 above
+ * NA / lambda; PSF = |fftshift(fft2(pupil))|^2 normalised to unit sum;
+ * OTF = |fftshift(ifft2(PSF))| normalised to unit maximum.  Outputs are device
+ * [R][R] FP32 arrays, any of them NULL to skip; 2 <= R <= 256. */
+int ncsb_genpsfparam(int R, double pixel_size, double na, double wavelength, float *psf,
+                     float *pupil, float *otf, void *stream);
+
 /* ---- simulator: synthetic sCMOS stacks generated on the device ------------
  * Replaces the reference's host-side simulation loops (python3-6/pyNCS/
  * denoisetools.py:118-186 genidealimage / SRhist, :205-225 addnoise /

@@ -112,7 +112,7 @@ EXPORTS = [
     "ncsb_batch_set", "ncsb_batch_num_tiles", "ncsb_batch_reduce_noise",
     "ncsb_reduce_noise_adu", "ncsb_genfilter",
     "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms", "ncsb_reduce_noise_normalized",
-    "ncsb_net_infer_stack_tc", "ncsb_net_infer_tiles_tc",
+    "ncsb_net_infer_stack_tc", "ncsb_net_infer_tiles_tc", "ncsb_genpsfparam",
 ]
 
 _lib = None
@@ -178,6 +178,9 @@ def load():
                                                  ctypes.c_double, ci, ctypes.c_double, vp, vp,
                                                  vp, vp, vp]
     lib.ncsb_reduce_noise_normalized.restype = ctypes.c_int
+    lib.ncsb_genpsfparam.argtypes = [ci, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                     vp, vp, vp, vp]
+    lib.ncsb_genpsfparam.restype = ctypes.c_int
     lib.ncsb_genfilter.argtypes = [P(NcsbOptics), ctypes.c_int, vp, vp]
     lib.ncsb_genfilter.restype = ctypes.c_int
     lib.ncsb_net_infer_stack_tc.argtypes = [vp, vp, ci, ci, ci, vp, ci, vp, vp, vp]

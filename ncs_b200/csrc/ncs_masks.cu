@@ -9,7 +9,7 @@
 // one CTA builds one mask in FP64: as a centred 16x16 image for callers, and/or
 // directly as the solver's M^2/256 table in the spectral kernel's lane layout,
 // so a batch of stacks with different optics never round-trips masks through
-// the host.
+// the host.  genpsfparam (the reference's pupil -> PSF -> OTF) is here too.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <stdint.h>
@@ -90,10 +90,108 @@ cudaError_t launch_masks(const ncsb_optics* d_optics, int n, float* centred, flo
     return cudaGetLastError();
 }
 
+// ---- genpsfparam (denoisetools.py:103-115) ----------------------------------
+// pupil = |k| on the centred grid (genkspace), 0 above NA / lambda;
+// PSF = |fftshift(fft2(pupil))|^2 / its sum; OTF = |fftshift(ifft2(PSF))| / its max.
+// Separable DFTs in FP64, one thread per output element (R <= 256).
+
+__global__ void psf_pupil(int R, double px, double fmax, double2* __restrict__ z,
+                          float* __restrict__ pupil) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R * R) return;
+    const int y = i / R, x = i - y * R;
+    const double X = x - R / 2.0, Y = y - R / 2.0;
+    double kr = sqrt(X * X + Y * Y) / (R * px);
+    if (kr > fmax) kr = 0.0;
+    z[i] = make_double2(kr, 0.0);
+    if (pupil) pupil[i] = (float)kr;
+}
+
+// out[r][v] = sum_c in[r][c] exp(sign 2 pi i v c / R)   (rows), or the same
+// along columns (cols = 1): out[u][c] = sum_r in[r][c] exp(sign 2 pi i u r / R)
+__global__ void psf_dft(const double2* __restrict__ in, double2* __restrict__ out, int R,
+                        double sign, int cols) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R * R) return;
+    const int a = i / R, b = i - a * R;  // output (row, col)
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < R; ++k) {
+        const double2 v = cols ? in[k * R + b] : in[a * R + k];
+        const int ph = ((cols ? a : b) * k) % R;
+        double sn, cs;
+        sincospi(2.0 * ph / R, &sn, &cs);
+        sn *= sign;
+        re += v.x * cs - v.y * sn;
+        im += v.x * sn + v.y * cs;
+    }
+    out[i] = make_double2(re, im);
+}
+
+// dst[u][v] = |src[(u - R/2) mod R][(v - R/2) mod R]|^power (fftshift), power 1 or 2
+__global__ void psf_shift_abs(const double2* __restrict__ src, double2* __restrict__ dst, int R,
+                              int power) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R * R) return;
+    const int u = i / R, v = i - u * R, h = R / 2;
+    const double2 s = src[((u - h + R) % R) * R + (v - h + R) % R];
+    const double m2 = s.x * s.x + s.y * s.y;
+    dst[i] = make_double2(power == 2 ? m2 : sqrt(m2), 0.0);
+}
+
+// one CTA: out = in.x / (sum or max of in.x)
+__global__ void psf_normalise(const double2* __restrict__ in, int n, int by_max,
+                              float* __restrict__ out) {
+    __shared__ double red[1024];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        acc = by_max ? fmax(acc, in[i].x) : acc + in[i].x;
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            red[threadIdx.x] = by_max ? fmax(red[threadIdx.x], red[threadIdx.x + s])
+                                      : red[threadIdx.x] + red[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double d = red[0];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) out[i] = (float)(in[i].x / d);
+}
+
 }  // namespace masks
 }  // namespace ncsb
 
 extern "C" {
+
+int ncsb_genpsfparam(int R, double pixel_size, double na, double wavelength, float* psf,
+                     float* pupil, float* otf, void* stream) {
+    if (R < 2 || R > 256 || !(pixel_size > 0.0) || !(na > 0.0) || !(wavelength > 0.0))
+        return NCSB_EINVAL;
+    if (!psf && !pupil && !otf) return NCSB_EINVAL;
+    using namespace ncsb::masks;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = R * R, blocks = (n + 255) / 256;
+    double2 *a = nullptr, *b = nullptr;
+    if (cudaMallocAsync(&a, sizeof(double2) * n, s) != cudaSuccess) return NCSB_ECUDA;
+    if (cudaMallocAsync(&b, sizeof(double2) * n, s) != cudaSuccess) {
+        cudaFreeAsync(a, s);
+        return NCSB_ECUDA;
+    }
+    psf_pupil<<<blocks, 256, 0, s>>>(R, pixel_size, na / wavelength, a, pupil);
+    psf_dft<<<blocks, 256, 0, s>>>(a, b, R, -1.0, 0);   // fft2: rows,
+    psf_dft<<<blocks, 256, 0, s>>>(b, a, R, -1.0, 1);   //       columns
+    psf_shift_abs<<<blocks, 256, 0, s>>>(a, b, R, 2);   // PSF = |fftshift(.)|^2
+    if (psf) psf_normalise<<<1, 1024, 0, s>>>(b, n, 0, psf);
+    if (otf) {
+        psf_dft<<<blocks, 256, 0, s>>>(b, a, R, 1.0, 0);  // ifft2 (unscaled: the max
+        psf_dft<<<blocks, 256, 0, s>>>(a, b, R, 1.0, 1);  // normalisation removes 1/R^2)
+        psf_shift_abs<<<blocks, 256, 0, s>>>(b, a, R, 1);
+        psf_normalise<<<1, 1024, 0, s>>>(a, n, 1, otf);
+    }
+    cudaFreeAsync(a, s);
+    cudaFreeAsync(b, s);
+    return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
+}
+
 
 int ncsb_genfilter(const ncsb_optics* optics, int n, float* masks_centred, void* stream) {
     if (!optics || !masks_centred || n < 0) return NCSB_EINVAL;

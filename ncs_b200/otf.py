@@ -105,3 +105,20 @@ def normalized_mask(pixelsize=0.1, NA=1.4, Lambda=0.7):
     """The 3 x 3 mask the normalised variant builds by default: genfilter of
     the segment size Rs + 2 = 3 with twice the NA (reducenoise.m, otfsize = 2)."""
     return genfilter_odd(3, pixelsize, 2.0 * NA, Lambda)
+
+
+def device_psf(R, pixelsize, NA, wavelength, device="cuda"):
+    """genpsfparam of the reference (denoisetools.py:103-115) computed on the GPU
+    (ncsb_genpsfparam): returns (PSFn, pupil, OTFn), float32 [R, R] tensors."""
+    import ctypes
+    import torch
+    from . import _lib
+    outs = [torch.empty((R, R), dtype=torch.float32, device=device) for _ in range(3)]
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+    with torch.cuda.device(outs[0].device):
+        rc = _lib.load().ncsb_genpsfparam(int(R), float(pixelsize), float(NA), float(wavelength),
+                                          vp(outs[0]), vp(outs[1]), vp(outs[2]),
+                                          ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    if rc != _lib.NCSB_OK:
+        raise ValueError("ncsb_genpsfparam failed with code %d" % rc)
+    return tuple(outs)

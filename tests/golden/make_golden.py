@@ -15,7 +15,9 @@ written here.  Sources used (paths in the HuanglabPurdue/NCS tree):
   * clib/pyCNCS/ncs_c.py           cReduceNoise / pyReduceNoise, run through
                                    the reference's own Python wrapper over the
                                    reference ncs.c compiled by oracle/Makefile
-  * python3-6/pyNCS/denoisetools.py genfilter (all three filter types)
+  * python3-6/pyNCS/denoisetools.py genfilter (all three filter types) and
+                                   genpsfparam (genpsfparam_vectors.npz;
+                                   ``--psf-only`` writes just that file)
 """
 import importlib.util
 import os
@@ -136,5 +138,30 @@ def main(ref):
     print("wrote", len(out), "arrays")
 
 
+def psf_vectors(ref):
+    """genpsfparam (denoisetools.py:103-115) for a few grids -> genpsfparam_vectors.npz.
+    The module imports plotting and HDF5 packages at the top, so the function is
+    taken from its source text with genkspace and run with numpy and
+    scipy.fftpack, as the module itself does."""
+    import scipy.fftpack
+    dt_src = open(os.path.join(ref, "python3-6/pyNCS/denoisetools.py")).read()
+    ns = {"ft": scipy.fftpack}
+    start = dt_src.index("def genkspace")
+    stop = dt_src.index("def SRhist")
+    exec("import numpy as np\n" + dt_src[start:stop], ns)
+    out = {}
+    for R, px, na, lam in ((16, 0.1, 1.4, 0.7), (32, 0.05, 1.2, 0.52), (33, 0.1, 1.49, 0.6)):
+        psf, pupil, otf = ns["genpsfparam"](R, px, na, lam)
+        key = "R%d" % R
+        out[key + "_params"] = numpy.array([R, px, na, lam])
+        out[key + "_psf"], out[key + "_pupil"], out[key + "_otf"] = psf, pupil, otf
+    numpy.savez_compressed(os.path.join(HERE, "genpsfparam_vectors.npz"), **out)
+    print("wrote", len(out), "arrays")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref_root = args[0] if args else "/root/reference"
+    if "--psf-only" not in sys.argv:
+        main(ref_root)
+    psf_vectors(ref_root)

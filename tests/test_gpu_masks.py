@@ -72,3 +72,16 @@ def test_batch_with_device_masks_equals_host_masks(ncs):
     for x, y in zip(oa, ob):
         assert ((x - y).abs() / y.abs().clamp(min=1.0)).max().item() <= 1e-4
     assert abs(sa["iters"].double().mean().item() - sb["iters"].double().mean().item()) <= 0.01
+
+
+def test_device_genpsfparam_matches_reference_vectors(ncs):
+    """The reference's own genpsfparam output (tests/golden/genpsfparam_vectors.npz,
+    written by make_golden.py from denoisetools.py:103-115) on even and odd grids."""
+    from ncs_b200 import otf
+    gold = numpy.load(os.path.join(os.path.dirname(GOLD), "genpsfparam_vectors.npz"))
+    for R in (16, 32, 33):
+        _, px, na, lam = gold["R%d_params" % R]
+        psf, pupil, o = (t.cpu().numpy() for t in otf.device_psf(R, px, na, lam))
+        assert numpy.allclose(pupil, gold["R%d_pupil" % R], rtol=1e-6, atol=1e-6)
+        assert numpy.allclose(psf, gold["R%d_psf" % R], rtol=1e-5, atol=1e-9)
+        assert numpy.allclose(o, gold["R%d_otf" % R], rtol=1e-5, atol=1e-7)

@@ -30,6 +30,8 @@ int launch_infer_batch(const float* params, const StackDesc* stacks, int n_stack
 }  // namespace net
 }  // namespace ncsb
 
+using ncsb::tiles_along;
+
 struct ncsb_handle {
     ncsb_params p;
     int device = 0;
@@ -94,18 +96,6 @@ void lane_layout(const float nat[256], float* out) {
         const int L = idx >> 3, i = idx & 7;
         out[idx] = nat[(2 * bitrev3_host(i) + (L & 1)) * 16 + (L >> 1)];
     }
-}
-
-int tiles_along(int n) {
-    // len(range(0, n + 2, 14)) with the last origin clamped to n + 2 - 16
-    // and the walk stopped after it (ncs.c:71-86, :136-142).
-    const int last = n + 2 - NCSB_TILE;
-    int count = 0;
-    for (int b = 0;; b += 14) {
-        ++count;
-        if (b >= last) break;
-    }
-    return count;
 }
 
 int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s) {

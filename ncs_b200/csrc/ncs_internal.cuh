@@ -75,6 +75,30 @@ struct SolveArgs {
     float levels[3];               // ascending ADU thresholds between the pairs
 };
 
+// ---- tile geometry (segmentation of ncs.c:66-113, shared by every kernel) ----
+// Origin of tile i along an axis of n pixels: 14 i, the last one shifted back to
+// n + 2 - 16 so that it ends at the far edge of the 1-px padded frame.
+__host__ __device__ __forceinline__ int tile_origin(int i, int n) {
+    const int o = 14 * i, last = n + 2 - kTile;
+    return o < last ? o : last;
+}
+
+__host__ __device__ __forceinline__ int clampi(int v, int lo, int hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+// Tiles along an axis: len(range(0, n + 2, 14)) with the last origin clamped to
+// n + 2 - 16 and the walk stopped there (ncs.c:71-86, :136-142).
+__host__ __device__ inline int tiles_along(int n) {
+    const int last = n + 2 - kTile;
+    int count = 0;
+    for (int b = 0;; b += 14) {
+        ++count;
+        if (b >= last) break;
+    }
+    return count;
+}
+
 __device__ __forceinline__ int bitrev4(int v) {
     return ((v & 1) << 3) | ((v & 2) << 1) | ((v & 4) >> 1) | ((v & 8) >> 3);
 }

@@ -33,10 +33,6 @@ constexpr float kStartFrac = 0.05f;
 
 __host__ __device__ constexpr int round4(int v) { return (v + 3) & ~3; }
 
-__device__ __forceinline__ int clampi(int v, int lo, int hi) {
-    return v < lo ? lo : (v > hi ? hi : v);
-}
-
 // Stage CIN channels of one tile into zero-bordered planes.
 template <int CIN>
 __device__ __forceinline__ void stage_planes(float* xs, const float* __restrict__ xt) {
@@ -277,11 +273,6 @@ __global__ void __launch_bounds__(256) features(const float* __restrict__ d,
 
 // ---- fused inference -------------------------------------------------------
 
-__device__ __forceinline__ int tile_origin(int i, int n) {
-    const int o = 14 * i, last = n + 2 - 16;
-    return o < last ? o : last;
-}
-
 // One conv layer from planes xin to planes yout (interior), shared memory only.
 template <int CIN, int COUT, bool RELU>
 __device__ __forceinline__ void layer_smem(const float* xin, float* yout, const float* wt,
@@ -385,16 +376,6 @@ __global__ void __launch_bounds__(256) infer(const InferSrc src, const float* __
     }
 }
 
-int tiles_along(int n) {
-    const int last = n + 2 - 16;
-    int count = 0;
-    for (int b = 0;; b += 14) {
-        ++count;
-        if (b >= last) break;
-    }
-    return count;
-}
-
 int launch_infer(const InferSrc& src, const float* params, float* u0, cudaStream_t s) {
     const size_t smem = infer_smem_bytes();
     if (cudaFuncSetAttribute(infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -454,6 +435,7 @@ int launch_infer_batch(const float* params, const StackDesc* stacks, int n_stack
 }  // namespace ncsb
 
 using namespace ncsb::net;
+using ncsb::tiles_along;
 
 extern "C" {
 

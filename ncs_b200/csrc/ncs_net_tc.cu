@@ -33,6 +33,7 @@
 #include <stdint.h>
 
 #include "../../include/ncs_b200.h"
+#include "ncs_internal.cuh"
 
 namespace ncsb {
 namespace nettc {
@@ -157,15 +158,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<const uint32_t*>(&h);
-}
-
-__device__ __forceinline__ int clampi(int v, int lo, int hi) {
-    return v < lo ? lo : (v > hi ? hi : v);
-}
-
-__device__ __forceinline__ int tile_origin(int i, int n) {
-    const int o = 14 * i, last = n + 2 - 16;
-    return o < last ? o : last;
 }
 
 // Store 32 channels of one position into a [chunk][pos][8] BF16 buffer.
@@ -437,16 +429,6 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 }
 
-int tiles_along(int n) {
-    const int last = n + 2 - 16;
-    int count = 0;
-    for (int b = 0;; b += 14) {
-        ++count;
-        if (b >= last) break;
-    }
-    return count;
-}
-
 int launch(const Src& src, const float* params, float* u0, int32_t* status, cudaStream_t s) {
     if (cudaFuncSetAttribute(infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) !=
         cudaSuccess)
@@ -478,6 +460,7 @@ static_assert(kIm2colPos + kQ <= kPos - 21, "im2col rows stay inside the rewritt
 }  // namespace ncsb
 
 using namespace ncsb::nettc;
+using ncsb::tiles_along;
 
 extern "C" {
 

@@ -29,6 +29,8 @@ cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStr
 int spectral_max_ctas_per_sm(int m, int blocks, bool warm, bool batch);
 }  // namespace ncsb
 
+using ncsb::tiles_along;
+
 namespace {
 
 // Layout of the static scratch: [0, 8) work counter, [256, 1280) the
@@ -76,16 +78,6 @@ int setup_current_device(DeviceSetup** out) {
     }
     *out = &s;
     return NCSB_OK;
-}
-
-int tiles_along(int n) {
-    const int last = n + 2 - NCSB_TILE;
-    int count = 0;
-    for (int b = 0;; b += 14) {
-        ++count;
-        if (b >= last) break;
-    }
-    return count;
 }
 
 bool params_ok(const ncsb_params* p) {

@@ -89,16 +89,6 @@ __device__ __forceinline__ void apply_q(float x0, float x1, float& y0, float& y1
     y1 = z.y;
 }
 
-// Frame coordinates helpers (stack mode).
-__device__ __forceinline__ int tile_origin(int i, int n) {
-    const int o = 14 * i, last = n + 2 - kTile;
-    return o < last ? o : last;
-}
-
-__device__ __forceinline__ int clampi(int v, int lo, int hi) {
-    return v < lo ? lo : (v > hi ? hi : v);
-}
-
 }  // namespace
 
 __global__ void __launch_bounds__(kThreads, 8) ncs_plain_kernel(const SolveArgs a) {

@@ -295,15 +295,6 @@ __device__ __forceinline__ float warp_sum_f(float v) {
     return v;
 }
 
-__device__ __forceinline__ int tile_origin(int i, int n) {
-    const int o = 14 * i, last = n + 2 - kTile;
-    return o < last ? o : last;
-}
-
-__device__ __forceinline__ int clampi(int v, int lo, int hi) {
-    return v < lo ? lo : (v > hi ? hi : v);
-}
-
 __device__ __forceinline__ void load8(const float4* h, float (&x)[8]) {
     const float4 a = h[0], b = h[1];
     x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;

@@ -375,6 +375,11 @@ int ncsb_net_infer_stack_tc(const float *params, const float *images, int n_fram
                             int width, const float *gamma, int gamma_per_frame, float *u0_tiles,
                             int32_t *status, void *stream);
 
+/* The tensor-core inference over the handle's current batch (ncsb_batch_set):
+ * u0_tiles [ncsb_batch_num_tiles()][16][16] in the batch's tile order. */
+int ncsb_net_infer_batch_tc(const float *params, const ncsb_handle *h, float *u0_tiles,
+                            int32_t *status, void *stream);
+
 /* The tensor-core inference on tiles d, gamma [n][16][16] -> u0 [n][16][16]. */
 int ncsb_net_infer_tiles_tc(const float *params, const float *d, const float *gamma,
                             int64_t n_tiles, float *u0, int32_t *status, void *stream);

@@ -113,6 +113,7 @@ EXPORTS = [
     "ncsb_reduce_noise_adu", "ncsb_genfilter",
     "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms", "ncsb_reduce_noise_normalized",
     "ncsb_net_infer_stack_tc", "ncsb_net_infer_tiles_tc", "ncsb_genpsfparam",
+    "ncsb_net_infer_batch_tc",
 ]
 
 _lib = None
@@ -187,6 +188,8 @@ def load():
     lib.ncsb_net_infer_stack_tc.restype = ctypes.c_int
     lib.ncsb_net_infer_tiles_tc.argtypes = [vp, vp, vp, i64, vp, vp, vp]
     lib.ncsb_net_infer_tiles_tc.restype = ctypes.c_int
+    lib.ncsb_net_infer_batch_tc.argtypes = [vp, vp, vp, vp, vp]
+    lib.ncsb_net_infer_batch_tc.restype = ctypes.c_int
     lib.ncsb_net_infer_batch.argtypes = [vp, vp, vp, vp]
     lib.ncsb_batch_set.argtypes = [vp, P(NcsbStack), ctypes.c_int]
     lib.ncsb_batch_set.restype = ctypes.c_int

@@ -28,6 +28,10 @@ namespace net {
 int launch_infer_batch(const float* params, const StackDesc* stacks, int n_stacks,
                        long long n_tiles, float* u0, cudaStream_t s);
 }  // namespace net
+namespace nettc {
+int launch_batch(const float* params, const StackDesc* stacks, int n_stacks, long long n_tiles,
+                 float* u0, int32_t* status, cudaStream_t s);
+}  // namespace nettc
 }  // namespace ncsb
 
 using ncsb::tiles_along;
@@ -467,6 +471,14 @@ int ncsb_net_infer_batch(const float* params, const ncsb_handle* h, float* u0_ti
     if (h->n_stacks < 1) return NCSB_EINVAL;
     return ncsb::net::launch_infer_batch(params, h->d_stacks, h->n_stacks, h->batch_tiles,
                                          u0_tiles, (cudaStream_t)stream);
+}
+
+int ncsb_net_infer_batch_tc(const float* params, const ncsb_handle* h, float* u0_tiles,
+                            int32_t* status, void* stream) {
+    if (!params || !h || !u0_tiles) return NCSB_EINVAL;
+    if (h->n_stacks < 1) return NCSB_EINVAL;
+    return ncsb::nettc::launch_batch(params, h->d_stacks, h->n_stacks, h->batch_tiles, u0_tiles,
+                                     status, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -74,6 +74,8 @@ struct Src {
     long long gamma_frame_stride;
     int H, W, tiles_x, tiles_y;
     long long n_tiles;
+    const StackDesc* stacks;  // batched stacks (stack mode), else null
+    int n_stacks;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -271,13 +273,34 @@ __global__ void __launch_bounds__(kThreads, 2)
                 dv[h] = src.d[tile * 256 + p];
                 gv[h] = src.gamma[tile * 256 + p];
             } else {
-                const int f = (int)(tile / per_frame);
-                const int rem = (int)(tile - (long long)f * per_frame);
-                const int ti = rem / src.tiles_y, tj = rem - ti * src.tiles_y;
-                const int yy = clampi(tile_origin(ti, src.H) + r - 1, 0, src.H - 1);
-                const int xx = clampi(tile_origin(tj, src.W) + c - 1, 0, src.W - 1);
-                dv[h] = src.d[(long long)f * src.H * src.W + (long long)yy * src.W + xx];
-                gv[h] = src.gamma[(long long)f * src.gamma_frame_stride + (long long)yy * src.W + xx];
+                const float* sd = src.d;
+                const float* sgam = src.gamma;
+                long long gstride = src.gamma_frame_stride, lt = tile, pf = per_frame;
+                int H = src.H, W = src.W, ty = src.tiles_y;
+                if (src.stacks) {  // batched: the last stack whose first tile is <= tile
+                    int lo = 0, hi = src.n_stacks - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (src.stacks[mid].tile_begin <= tile) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    const StackDesc& st = src.stacks[lo];
+                    sd = st.data;
+                    sgam = st.gamma;
+                    gstride = st.gamma_frame_stride;
+                    lt = tile - st.tile_begin;
+                    H = st.H;
+                    W = st.W;
+                    ty = st.tiles_y;
+                    pf = (long long)st.tiles_x * st.tiles_y;
+                }
+                const int f = (int)(lt / pf);
+                const int rem = (int)(lt - (long long)f * pf);
+                const int ti = rem / ty, tj = rem - ti * ty;
+                const int yy = clampi(tile_origin(ti, H) + r - 1, 0, H - 1);
+                const int xx = clampi(tile_origin(tj, W) + c - 1, 0, W - 1);
+                dv[h] = sd[(long long)f * H * W + (long long)yy * W + xx];
+                gv[h] = sgam[(long long)f * gstride + (long long)yy * W + xx];
             }
         }
     };
@@ -450,6 +473,18 @@ int launch(const Src& src, const float* params, float* u0, int32_t* status, cuda
     if (grid > src.n_tiles) grid = src.n_tiles;
     infer_tc<<<(unsigned)grid, kThreads, kSmemBytes, s>>>(src, params, u0, status);
     return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
+}
+
+int launch_batch(const float* params, const StackDesc* stacks, int n_stacks, long long n_tiles,
+                 float* u0, int32_t* status, cudaStream_t s) {
+    if (n_tiles == 0) return NCSB_OK;
+    Src src{};
+    src.stacks = stacks;
+    src.n_stacks = n_stacks;
+    src.tiles_x = 1;
+    src.tiles_y = 1;
+    src.n_tiles = n_tiles;
+    return launch(src, params, u0, status, s);
 }
 
 static_assert(2 * (kSmemBytes + 2048) <= 228 * 1024, "two CTAs per SM");

@@ -150,6 +150,22 @@ class WarmStartNet:
                 "ncsb_net_infer_stack_tc")
         return out, status
 
+    def propose_batch_tc(self, solver, out=None, status=None, stream=None):
+        """``propose_batch`` on the tensor cores; returns (proposals, status).
+        With ``out`` and ``status`` (int32 [1], zeroed by the caller) given,
+        one kernel is issued and nothing is allocated, so the call can be
+        captured in a CUDA graph; status stays non-zero once a wait times out."""
+        n = solver.batch_tiles
+        if out is None:
+            out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
+        if status is None:
+            status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_net_infer_batch_tc(
+                _ptr(self.params), solver._handle, _ptr(out), _ptr(status),
+                _stream_ptr(stream, self.device)), "ncsb_net_infer_batch_tc")
+        return out, status
+
     def propose_tiles_tc(self, d, gamma, stream=None):
         n = d.shape[0]
         out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)

@@ -6,8 +6,9 @@ The batched kernel reads each tile's stack descriptor instead of kernel
 parameters and otherwise runs the single-stack arithmetic, so every stack's
 result, per-tile iterations, status and cost must equal (bit for bit) a
 single-stack solve with that stack's alpha and mask.  Also: proposals from
-the batched network inference equal the per-stack ones, the launch can be
-captured in a CUDA graph and replayed, and bad batches are refused.
+the batched network inference (FP32 and tensor-core) equal the per-stack
+ones, the launch can be captured in a CUDA graph and replayed, and bad
+batches are refused.
 """
 import numpy
 import pytest
@@ -115,6 +116,25 @@ def test_batch_proposals_and_warm_solve(ncs, stacks):
         assert torch.equal(stats["start"][off:off + n], rfb)
         off += n
         ss.close()
+
+
+def test_batch_tensor_core_proposals_equal_per_stack(ncs, stacks):
+    """The tensor-core inference over a batch reads each tile's stack descriptor
+    and otherwise runs the per-stack arithmetic: equal bit for bit."""
+    from ncs_b200 import warmstart
+    net = warmstart.WarmStartNet.load()
+    s = ncs.Solver()
+    s.batch_set(stacks)
+    u0, status = net.propose_batch_tc(s)
+    per = []
+    for st in stacks:
+        u, st_status = net.propose_stack_tc(st["images"], st["gamma"])
+        assert int(st_status.item()) == 0
+        per.append(u)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    assert u0.shape[0] == s.batch_tiles
+    assert torch.equal(u0, torch.cat(per))
 
 
 def test_batch_launch_replays_from_a_cuda_graph(ncs, stacks):

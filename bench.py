@@ -322,6 +322,7 @@ def workload_config(w, args):
                                            w["max_iters"]),
             "frames": T, "height": H, "width": W, "alpha": w["alpha"],
             "max_iters": w["max_iters"], "seed": w["seed"], "form": args.form,
+            "ctas_per_sm": args.ctas_per_sm or "library default",
             "l2": "inputs+outputs %.0f MB > 126 MB L2, no flush" % (2 * T * H * W * 4 / 1e6),
             "parallelism": "replicas by frame (one stack per rank)"}
 
@@ -334,7 +335,8 @@ def run_ours(args, world, rank, local):
     w = sim.make_stack(args.workload, T=args.frames, device=dev, seed=1234 + rank)
     images, gamma = w["images"], w["gamma"]
     T, H, W = images.shape
-    solver = ncs_b200.Solver(alpha=w["alpha"], max_iters=w["max_iters"], mode=args.form)
+    solver = ncs_b200.Solver(alpha=w["alpha"], max_iters=w["max_iters"], mode=args.form,
+                             ctas_per_sm=args.ctas_per_sm)
     solver.set_otf_mask(w["mask"])
     out = torch.empty_like(images)
     stream = torch.cuda.current_stream(dev)
@@ -747,6 +749,8 @@ def main():
                     help="skip the learned warm-start leg")
     ap.add_argument("--accuracy-tiles", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ctas-per-sm", type=int, default=0,
+                    help="resident CTAs per SM of the solve (0: the library's default)")
     ap.add_argument("--stacks", type=int, default=64,
                     help="stacks in the mixed workload (--workload mixed)")
     args = ap.parse_args()

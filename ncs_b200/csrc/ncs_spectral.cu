@@ -14,8 +14,9 @@
 // one line-search trial per iteration), so each solve does less work although
 // an iteration now applies two Fourier-diagonal operators:
 //   * the first half of the two-loop leaves q; one forward 16x16 FFT of q and
-//     two inverse FFTs give H0 q and Q H0 q (spectral weights
-//     1/(lambda + 2 alpha M^2) and M^2 / (lambda + 2 alpha M^2));
+//     one complex inverse FFT give H0 q (real part) and Q H0 q (imaginary
+//     part), spectral weights 1/(lambda + 2 alpha M^2) and
+//     M^2 / (lambda + 2 alpha M^2);
 //   * the second half adds coef_i s_i to the direction and coef_i Q s_i to
 //     w = Q p, with Q s_i = t_i w_i stored with each pair -- so w = Q p, which
 //     the exact line search needs (ncs_plain.cu), costs no extra transform.
@@ -84,7 +85,9 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 
     __shared__ StackDesc sdesc[kWarps];  // Batch: each warp's current stack
     const LaneGeo G = lane_geo(lane);
-    float mk[8];  // M^2/256 at this lane's 8 spectral positions
+    // M^2/256 at this lane's 8 spectral positions: the CTA's shared table, or
+    // the current stack's lane-layout table (Batch); read once per pass
+    const float4* mkp = reinterpret_cast<const float4*>(mtab) + lane * 2;
     float alpha = a.alpha, two_alpha = 2.0f * a.alpha, two_alpha_256 = 512.0f * a.alpha;
     if constexpr (!Batch) {
         for (int idx = threadIdx.x; idx < 256; idx += blockDim.x) {
@@ -92,10 +95,6 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             mtab[idx] = a.msq[(2 * bitrev3(i) + (L & 1)) * 16 + (L >> 1)];
         }
         __syncthreads();
-        const float4 m0 = *reinterpret_cast<const float4*>(mtab + lane * 8);
-        const float4 m1 = *reinterpret_cast<const float4*>(mtab + lane * 8 + 4);
-        mk[0] = m0.x; mk[1] = m0.y; mk[2] = m0.z; mk[3] = m0.w;
-        mk[4] = m1.x; mk[5] = m1.y; mk[6] = m1.z; mk[7] = m1.w;
     }
 
     for (;;) {
@@ -118,10 +117,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             alpha = sdesc[wid].alpha;
             two_alpha = 2.0f * alpha;
             two_alpha_256 = 512.0f * alpha;
-            const float4* mt = reinterpret_cast<const float4*>(a.mk_lane + (size_t)lo * 256) + lane * 2;
-            const float4 m0 = __ldg(mt), m1 = __ldg(mt + 1);
-            mk[0] = m0.x; mk[1] = m0.y; mk[2] = m0.z; mk[3] = m0.w;
-            mk[4] = m1.x; mk[5] = m1.y; mk[6] = m1.z; mk[7] = m1.w;
+            mkp = reinterpret_cast<const float4*>(a.mk_lane + (size_t)lo * 256) + lane * 2;
         }
 
         // ---- gather the tile (segmentation, ncs.c:66-113) ---------------------
@@ -256,27 +252,30 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     }
                 }
             }
-            // spectral step: one forward transform, one or two inverse ones
+            // spectral step: one forward transform and one complex inverse one,
+            // whose real part is H0 q and imaginary part Q H0 q (pass 0: Q u
+            // alone).  Both spectral weights are real and symmetric in k.
             float2 spec[8];
             warp_fft_fwd(q, spec, ws, G);
-            const int n_out = first ? 1 : 2;
-#pragma unroll 1
-            for (int o = 0; o < n_out; ++o) {
-                float2 e2[8];
+            float mk[8];
+            {
+                const float4 m0 = Batch ? __ldg(mkp) : mkp[0], m1 = Batch ? __ldg(mkp + 1) : mkp[1];
+                mk[0] = m0.x; mk[1] = m0.y; mk[2] = m0.z; mk[3] = m0.w;
+                mk[4] = m1.x; mk[5] = m1.y; mk[6] = m1.z; mk[7] = m1.w;
+            }
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    // pass 0: Q;  then H0 (o = 0) and Q H0 (o = 1)
-                    const float hq = __fdividef(1.0f, fmaf(two_alpha_256, mk[i], lam));
-                    const float wgt = first ? mk[i] : (o == 0 ? hq * (1.0f / 256.0f) : mk[i] * hq);
-                    e2[i] = make_float2(spec[i].x * wgt, spec[i].y * wgt);
-                }
-                float y[8];
-                warp_fft_inv(e2, y, ws, G);
+            for (int i = 0; i < 8; ++i) {
+                const float hq = __fdividef(1.0f, fmaf(two_alpha_256, mk[i], lam));
+                const float w0 = first ? mk[i] : hq * (1.0f / 256.0f);
+                const float w1 = first ? 0.0f : mk[i] * hq;
+                spec[i] = make_float2(fmaf(spec[i].x, w0, -spec[i].y * w1),
+                                      fmaf(spec[i].y, w0, spec[i].x * w1));
+            }
+            float y1[8];
+            warp_fft_inv2(spec, p, y1, ws, G);
+            if (!first) {  // a start pass keeps w (Q u0 of a proposal)
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    if (o == 0) p[i] = y[i];
-                    else w[i] = y[i];
-                }
+                for (int i = 0; i < 8; ++i) w[i] = y1[i];
             }
             if (first) {
                 if (start_pass == 2) {  // keep Q u0, transform d next
@@ -317,12 +316,12 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
                     v[i] = p[i];
-                    const float ag = fmaxf(u[i] + gm[i], kFitMin);
-                    const float r = __fdividef(c[i], ag);
+                    const float ia = __fdividef(1.0f, fmaxf(u[i] + gm[i], kFitMin));
+                    const float r = c[i] * ia;
                     g[i] = 1.0f - r + two_alpha * v[i];
                     uu = fmaf(u[i], u[i], uu);
                     gg = fmaf(g[i], g[i], gg);
-                    ll = fmaf(r, __fdividef(1.0f, ag), ll);
+                    ll = fmaf(r, ia, ll);
                 }
                 uu = warp_sum_f(uu);
                 gg = warp_sum_f(gg);
@@ -406,8 +405,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 const float un = fmaf(t, p[i], u[i]);
                 w[i] *= t;
                 v[i] += w[i];
-                const float ag = fmaxf(un + gm[i], kFitMin);
-                const float r = __fdividef(c[i], ag);
+                const float ia = __fdividef(1.0f, fmaxf(un + gm[i], kFitMin));
+                const float r = c[i] * ia;
                 const float gn = 1.0f - r + two_alpha * v[i];
                 s[i] = un - u[i];
                 y[i] = gn - g[i];
@@ -417,7 +416,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 sy = fmaf(s[i], y[i], sy);
                 uu = fmaf(un, un, uu);
                 gg = fmaf(gn, gn, gg);
-                ll = fmaf(r, __fdividef(1.0f, ag), ll);
+                ll = fmaf(r, ia, ll);
             }
             {
                 float vals[16] = {sy, uu, gg, ll, mv};
@@ -496,13 +495,20 @@ size_t spectral_smem_bytes(int m) {
     return kTableBytes + (size_t)kWarps * spec_warp_bytes(mc);
 }
 
+template <int B, int MaxM>
+KernelFn spectral_special(bool warm, bool batch, bool adu) {
+    if (adu) return ncs_spectral_kernel<B, MaxM, false, false, true>;
+    if (batch) return warm ? ncs_spectral_kernel<B, MaxM, true, true>
+                           : ncs_spectral_kernel<B, MaxM, false, true>;
+    return ncs_spectral_kernel<B, MaxM, true, false>;
+}
+
 template <int MaxM>
 KernelFn spectral_variant_m(int blocks, bool warm, bool batch, bool adu) {
-    // proposals, batches and raw-ADU input: the default grid only
-    if (adu) return ncs_spectral_kernel<3, MaxM, false, false, true>;
-    if (batch) return warm ? ncs_spectral_kernel<3, MaxM, true, true>
-                           : ncs_spectral_kernel<3, MaxM, false, true>;
-    if (warm) return ncs_spectral_kernel<3, MaxM, true, false>;
+    // proposals, batches and raw-ADU input: 3 or 4 CTAs per SM
+    if (adu || batch || warm)
+        return blocks >= 4 ? spectral_special<4, MaxM>(warm, batch, adu)
+                           : spectral_special<3, MaxM>(warm, batch, adu);
     switch (blocks <= 3 ? 3 : (blocks >= 5 ? 5 : blocks)) {
         case 3: return ncs_spectral_kernel<3, MaxM, false, false>;
         case 4: return ncs_spectral_kernel<4, MaxM, false, false>;
@@ -522,10 +528,10 @@ int spectral_default_blocks(int m) {
     if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
         cudaSuccess)
         per_sm = 228 * 1024;
-    // 3 CTAs (12 warps) per SM measured fastest: the 4- and 5-CTA register
-    // budgets spill
+    // 4 CTAs (16 warps, 128 registers, at most a few words spilled) measured
+    // fastest; the 5-CTA budget (96 registers) spills heavily
     const int b = (int)(per_sm / (spectral_smem_bytes(m) + 1024));
-    return b < 3 ? b : 3;
+    return b < 4 ? b : 4;
 }
 
 }  // namespace

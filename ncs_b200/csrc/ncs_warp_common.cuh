@@ -192,10 +192,10 @@ __device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8]
     fft8_fwd(e);
 }
 
-// Inverse half: from a spectrum in the layout warp_fft_fwd leaves, the real
-// tile back in this lane's 8 pixels (unnormalised inverse: x 256).
-__device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float (&y)[8], WarpSmem& ws,
-                                             const LaneGeo& L) {
+// Column stage of the inverse: from a spectrum in the layout warp_fft_fwd
+// leaves, fb[r][KC] = the row spectrum (horizontal frequency KC) of spatial
+// row r, for all 16 rows.
+__device__ __forceinline__ void warp_ifft_cols(float2 (&e)[8], WarpSmem& ws, const LaneGeo& L) {
     fft8_inv(e);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
@@ -213,14 +213,11 @@ __device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float (&y)[8], Warp
 #pragma unroll
     for (int r = 0; r < 8; ++r) ws.fb[r + 8 * L.H][L.KC] = out[r];
     __syncwarp();
+}
 
-    // inverse rows: pack the two real output rows, inverse transforms
-    float2 V[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float2 a = ws.fb[L.P][L.k0 + k], b = ws.fb[L.P + 8][L.k0 + k];
-        V[k] = make_float2(a.x - b.y, a.y + b.x);
-    }
+// Row stage of the inverse: V[k] = one row's spectrum at frequencies k0 + k
+// (this lane's four); z[j] = that row at column Qd + 4j (unnormalised).
+__device__ __forceinline__ void warp_ifft_row(float2 (&V)[4], float2 (&z)[4], const LaneGeo& L) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float2 p = shfl_xor2(V[k], 1);
@@ -238,12 +235,51 @@ __device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float (&y)[8], Warp
     V[1] = conjmul(V[1], L.tw1);
     V[2] = conjmul(V[2], L.tw2);
     V[3] = conjmul(V[3], L.tw3);
-    {
-        const float2 s02 = V[0] + V[2], d02 = V[0] - V[2], s13 = V[1] + V[3], d13 = V[1] - V[3];
-        const float2 z0 = s02 + s13, z2 = s02 - s13;
-        const float2 z1 = d02 + mul_i(d13), z3 = d02 + mul_mi(d13);
-        y[0] = z0.x; y[1] = z0.y; y[2] = z1.x; y[3] = z1.y;
-        y[4] = z2.x; y[5] = z2.y; y[6] = z3.x; y[7] = z3.y;
+    const float2 s02 = V[0] + V[2], d02 = V[0] - V[2], s13 = V[1] + V[3], d13 = V[1] - V[3];
+    z[0] = s02 + s13;
+    z[2] = s02 - s13;
+    z[1] = d02 + mul_i(d13);
+    z[3] = d02 + mul_mi(d13);
+}
+
+// Inverse half: from a spectrum in the layout warp_fft_fwd leaves, the real
+// tile back in this lane's 8 pixels (unnormalised inverse: x 256).  The two
+// real rows P and P + 8 share one complex row transform.
+__device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float (&y)[8], WarpSmem& ws,
+                                             const LaneGeo& L) {
+    warp_ifft_cols(e, ws, L);
+    float2 V[4], z[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 a = ws.fb[L.P][L.k0 + k], b = ws.fb[L.P + 8][L.k0 + k];
+        V[k] = make_float2(a.x - b.y, a.y + b.x);
+    }
+    warp_ifft_row(V, z, L);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        y[2 * j] = z[j].x;
+        y[2 * j + 1] = z[j].y;
+    }
+}
+
+// Two real tiles from one complex inverse: e = A + i B with A and B spectra
+// of real tiles (Hermitian) gives y0 = the tile of A and y1 = that of B
+// (unnormalised).  One column stage serves both; rows P and P + 8 each take
+// a complex row transform.
+__device__ __forceinline__ void warp_fft_inv2(float2 (&e)[8], float (&y0)[8], float (&y1)[8],
+                                              WarpSmem& ws, const LaneGeo& L) {
+    warp_ifft_cols(e, ws, L);
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        float2 V[4], z[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) V[k] = ws.fb[L.P + 8 * s][L.k0 + k];
+        warp_ifft_row(V, z, L);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            y0[2 * j + s] = z[j].x;
+            y1[2 * j + s] = z[j].y;
+        }
     }
 }
 

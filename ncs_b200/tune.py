@@ -16,7 +16,7 @@ import os
 
 import torch
 
-DEFAULT_CANDIDATES = tuple({"ctas_per_sm": c, "m": m} for c in (1, 2, 3) for m in (1, 2, 4))
+DEFAULT_CANDIDATES = tuple({"ctas_per_sm": c, "m": m} for c in (2, 3, 4) for m in (1, 2, 4))
 
 _cache = {}
 

@@ -125,6 +125,26 @@ int ncsb_reduce_noise(ncsb_handle *h, const float *images, int n_frames, int hei
                       void *stream);
 
 /*
+ * ncsb_reduce_noise from and to HOST memory, the form of the reference's
+ * Python entries (cuda/pyCUDANCS/ncs.py:137-147 copies the tiles to the
+ * device, launches, and copies the result back; clib/pyCNCS/ncs_c.py:250-276
+ * works on host arrays).  images, gamma (shared or per frame, as in
+ * ncsb_reduce_noise) and out are host pointers; page-locked memory lets the
+ * copies overlap the solve.  The stack is cut into chunks of chunk_frames
+ * frames (<= 0: about 8 MB); chunk i is copied in, solved and copied out on
+ * the handle's stream i % n_streams (<= 0: 4; at most 8), each stream with its own
+ * device buffers and work counter, so one chunk's copies overlap other
+ * chunks' copies and solves.  The streams start after the work already
+ * queued on `stream`, and `stream` waits for them.  The call returns once
+ * `out` holds the result.  The handle's streams, events and buffers are
+ * created on the first call and kept until ncsb_destroy; calls on one
+ * handle must not overlap.  Results equal ncsb_reduce_noise bit for bit.
+ */
+int ncsb_reduce_noise_host(ncsb_handle *h, const float *images, int n_frames, int height,
+                           int width, const float *gamma, int gamma_per_frame, float *out,
+                           int chunk_frames, int n_streams, void *stream);
+
+/*
  * Tile-level solve with the reference kernel's data layout: data_in and
  * gamma_in are [n_tiles][16][16] FP32 (gamma per tile, ncs.cu:931),
  * data_out [n_tiles][16][16]; iters / status / cost / evals optional [n_tiles].

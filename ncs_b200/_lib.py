@@ -113,7 +113,7 @@ EXPORTS = [
     "ncsb_reduce_noise_adu", "ncsb_genfilter",
     "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms", "ncsb_reduce_noise_normalized",
     "ncsb_net_infer_stack_tc", "ncsb_net_infer_tiles_tc", "ncsb_genpsfparam",
-    "ncsb_net_infer_batch_tc",
+    "ncsb_net_infer_batch_tc", "ncsb_reduce_noise_host",
 ]
 
 _lib = None
@@ -190,6 +190,8 @@ def load():
     lib.ncsb_net_infer_tiles_tc.restype = ctypes.c_int
     lib.ncsb_net_infer_batch_tc.argtypes = [vp, vp, vp, vp, vp]
     lib.ncsb_net_infer_batch_tc.restype = ctypes.c_int
+    lib.ncsb_reduce_noise_host.argtypes = [vp, vp, i32, i32, i32, vp, i32, vp, i32, i32, vp]
+    lib.ncsb_reduce_noise_host.restype = ctypes.c_int
     lib.ncsb_net_infer_batch.argtypes = [vp, vp, vp, vp]
     lib.ncsb_batch_set.argtypes = [vp, P(NcsbStack), ctypes.c_int]
     lib.ncsb_batch_set.restype = ctypes.c_int

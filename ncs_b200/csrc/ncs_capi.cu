@@ -36,6 +36,58 @@ int launch_batch(const float* params, const StackDesc* stacks, int n_stacks, lon
 
 using ncsb::tiles_along;
 
+namespace {
+
+// State of ncsb_reduce_noise_host, created on its first call: up to
+// kMaxStreams streams, each with its own chunk buffers and work counter.
+// Chunk i goes to stream i % n, which copies it in, solves it and copies it
+// out, so stream order alone protects each buffer and the copies of
+// different streams interleave on the host link in both directions.
+struct HostPipe {
+    static constexpr int kMaxStreams = 8;
+    int n = 0;            // streams with buffers
+    size_t chunk_px = 0;  // pixels per chunk buffer
+    bool per_frame = false;
+    size_t gamma_px = 0;  // pixels of the shared gamma buffer
+    float* d_in[kMaxStreams] = {};
+    float* d_out[kMaxStreams] = {};
+    float* d_gf[kMaxStreams] = {};  // per-frame gamma chunks
+    float* d_gamma = nullptr;       // shared gamma map
+    unsigned long long* d_queues = nullptr;  // [kMaxStreams]
+    cudaStream_t st[kMaxStreams] = {};
+    cudaEvent_t start = nullptr, gamma_in = nullptr, done[kMaxStreams] = {};
+};
+
+void free_buffers(HostPipe* q) {
+    for (int b = 0; b < HostPipe::kMaxStreams; ++b) {
+        cudaFree(q->d_in[b]);
+        cudaFree(q->d_out[b]);
+        cudaFree(q->d_gf[b]);
+        q->d_in[b] = q->d_out[b] = q->d_gf[b] = nullptr;
+    }
+    q->n = 0;
+    q->chunk_px = 0;
+    q->per_frame = false;
+}
+
+void destroy_pipe(HostPipe* q) {
+    if (!q) return;
+    for (cudaStream_t st : q->st)
+        if (st) cudaStreamSynchronize(st);
+    free_buffers(q);
+    cudaFree(q->d_gamma);
+    cudaFree(q->d_queues);
+    for (cudaStream_t st : q->st)
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : {q->start, q->gamma_in})
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : q->done)
+        if (ev) cudaEventDestroy(ev);
+    delete q;
+}
+
+}  // namespace
+
 struct ncsb_handle {
     ncsb_params p;
     int device = 0;
@@ -50,6 +102,7 @@ struct ncsb_handle {
     int batch_cap = 0;
     int n_stacks = 0;
     long long batch_tiles = 0;
+    HostPipe* pipe = nullptr;  // ncsb_reduce_noise_host
     std::string err;
 };
 
@@ -102,10 +155,12 @@ void lane_layout(const float nat[256], float* out) {
     }
 }
 
-int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(h->d_queue, 0, sizeof(unsigned long long), s);
+// queue: the work counter of this launch (default: the handle's own)
+int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s, unsigned long long* queue = nullptr) {
+    if (!queue) queue = h->d_queue;
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemsetAsync(queue)");
-    a.queue = h->d_queue;
+    a.queue = queue;
     a.msq = h->d_msq;
     a.alpha = (float)h->p.alpha;
     a.eps = (float)h->p.epsilon;
@@ -185,6 +240,7 @@ int ncsb_set_params(ncsb_handle* h, const ncsb_params* p) {
 
 int ncsb_destroy(ncsb_handle* h) {
     if (!h) return NCSB_EINVAL;
+    destroy_pipe(h->pipe);
     cudaFree(h->d_msq);
     cudaFree(h->d_queue);
     cudaFree(h->d_stacks);
@@ -246,6 +302,136 @@ int ncsb_reduce_noise(ncsb_handle* h, const float* images, int n_frames, int hei
     a.cost = tile_cost;
     a.evals = tile_evals;
     return launch(h, a, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Create the pipeline's streams and events, and (re)size its buffers.
+cudaError_t prepare_pipe(ncsb_handle* h, int n, size_t chunk_px, size_t gamma_px,
+                         bool per_frame) {
+    if (!h->pipe) {
+        HostPipe* q = new (std::nothrow) HostPipe();
+        if (!q) return cudaErrorMemoryAllocation;
+        h->pipe = q;
+        cudaError_t e = cudaMalloc(&q->d_queues, HostPipe::kMaxStreams * sizeof(unsigned long long));
+        for (int k = 0; k < HostPipe::kMaxStreams && e == cudaSuccess; ++k) {
+            e = cudaStreamCreateWithFlags(&q->st[k], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&q->done[k], cudaEventDisableTiming);
+        }
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&q->start, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&q->gamma_in, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            destroy_pipe(q);
+            h->pipe = nullptr;
+            return e;
+        }
+    }
+    HostPipe* q = h->pipe;
+    if (q->n != n || q->chunk_px < chunk_px || (per_frame && !q->per_frame)) {
+        // the previous call has finished: every call waits for all its streams
+        free_buffers(q);
+        const size_t bytes = chunk_px * sizeof(float);
+        for (int k = 0; k < n; ++k) {
+            cudaError_t e = cudaMalloc(&q->d_in[k], bytes);
+            if (e == cudaSuccess) e = cudaMalloc(&q->d_out[k], bytes);
+            if (e == cudaSuccess && per_frame) e = cudaMalloc(&q->d_gf[k], bytes);
+            if (e != cudaSuccess) {
+                free_buffers(q);
+                return e;
+            }
+        }
+        q->n = n;
+        q->chunk_px = chunk_px;
+        q->per_frame = per_frame;
+    }
+    if (!per_frame && q->gamma_px < gamma_px) {
+        cudaFree(q->d_gamma);
+        q->d_gamma = nullptr;
+        q->gamma_px = 0;
+        cudaError_t e = cudaMalloc(&q->d_gamma, gamma_px * sizeof(float));
+        if (e != cudaSuccess) return e;
+        q->gamma_px = gamma_px;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ncsb_reduce_noise_host(ncsb_handle* h, const float* images, int n_frames, int height,
+                           int width, const float* gamma, int gamma_per_frame, float* out,
+                           int chunk_frames, int n_streams, void* stream) {
+    if (!h) return NCSB_EINVAL;
+    if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
+    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
+    if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
+    if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
+        return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
+    if (n_frames == 0) return NCSB_OK;
+    const size_t frame_px = (size_t)height * width;
+    if (chunk_frames <= 0) {  // about 8 MB per chunk
+        const double f = 8.0e6 / (4.0 * (double)frame_px);
+        chunk_frames = f < 1.0 ? 1 : (int)(f + 0.5);
+    }
+    if (chunk_frames > n_frames) chunk_frames = n_frames;
+    if (n_streams <= 0) n_streams = 4;
+    if (n_streams > HostPipe::kMaxStreams) n_streams = HostPipe::kMaxStreams;
+    cudaError_t e = prepare_pipe(h, n_streams, (size_t)chunk_frames * frame_px, frame_px,
+                                 gamma_per_frame != 0);
+    if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline set-up");
+    HostPipe* q = h->pipe;
+    cudaStream_t caller = (cudaStream_t)stream;
+    const size_t fb = frame_px * sizeof(float);
+    // every stream starts after the caller's earlier work and, for a shared
+    // gamma map, after its copy in
+    e = cudaEventRecord(q->start, caller);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(q->st[0], q->start, 0);
+    if (e == cudaSuccess && !gamma_per_frame) {
+        e = cudaMemcpyAsync(q->d_gamma, gamma, fb, cudaMemcpyHostToDevice, q->st[0]);
+        if (e == cudaSuccess) e = cudaEventRecord(q->gamma_in, q->st[0]);
+    }
+    for (int k = 1; k < n_streams && e == cudaSuccess; ++k)
+        e = cudaStreamWaitEvent(q->st[k], gamma_per_frame ? q->start : q->gamma_in, 0);
+    if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline start");
+    for (int i = 0, f0 = 0; f0 < n_frames; ++i, f0 += chunk_frames) {
+        const int n = n_frames - f0 < chunk_frames ? n_frames - f0 : chunk_frames;
+        const int k = i % n_streams;
+        cudaStream_t st = q->st[k];
+        e = cudaMemcpyAsync(q->d_in[k], images + (size_t)f0 * frame_px, (size_t)n * fb,
+                            cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && gamma_per_frame)
+            e = cudaMemcpyAsync(q->d_gf[k], gamma + (size_t)f0 * frame_px, (size_t)n * fb,
+                                cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline copy in");
+        ncsb::SolveArgs a{};
+        a.tile_mode = 0;
+        a.data = q->d_in[k];
+        a.gamma = gamma_per_frame ? q->d_gf[k] : q->d_gamma;
+        a.gamma_frame_stride = gamma_per_frame ? (long long)frame_px : 0;
+        a.out = q->d_out[k];
+        a.T = n;
+        a.H = height;
+        a.W = width;
+        a.tiles_x = tiles_along(height);
+        a.tiles_y = tiles_along(width);
+        a.n_tiles = (long long)n * a.tiles_x * a.tiles_y;
+        const int rc = launch(h, a, st, q->d_queues + k);
+        if (rc != NCSB_OK) return rc;
+        e = cudaMemcpyAsync(out + (size_t)f0 * frame_px, q->d_out[k], (size_t)n * fb,
+                            cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline copy out");
+    }
+    // the caller's stream, and this call's return, wait for every stream
+    for (int k = 0; k < n_streams && e == cudaSuccess; ++k) {
+        e = cudaEventRecord(q->done[k], q->st[k]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(caller, q->done[k], 0);
+    }
+    for (int k = 0; k < n_streams && e == cudaSuccess; ++k) e = cudaEventSynchronize(q->done[k]);
+    if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline finish");
+    return NCSB_OK;
 }
 
 int ncsb_reduce_noise_start(ncsb_handle* h, const float* images, int n_frames, int height,

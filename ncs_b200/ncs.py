@@ -311,18 +311,23 @@ class Solver:
                 "evals": torch.empty(n, **i32), "start": torch.empty(n, **i32),
                 "cost": torch.empty(n, dtype=torch.float64, device=self.device)}
 
-    def reduce_noise_host(self, images, gamma, out=None, chunk_frames=None, n_streams=3):
-        """Host stack in, host stack out, with the copies hidden behind the solve.
+    def reduce_noise_host(self, images, gamma, out=None, chunk_frames=None, n_streams=None,
+                          stream=None):
+        """Host stack in, host stack out, with the copies hidden behind the solve
+        (``ncsb_reduce_noise_host``).
 
         ``images`` [T, H, W] and ``gamma`` [H, W] or [T, H, W] are float32 CPU
-        tensors (pinned memory lets the copies run asynchronously; numpy arrays
-        are accepted and pinned here).  The frames are cut into chunks; chunk i
-        is copied in, solved and copied out on stream i % n_streams, each
-        stream with its own solver handle (its own work counter), so one
-        chunk's host-device copies overlap another chunk's solve.  Returns the
-        pinned [T, H, W] result after all streams finish."""
+        tensors or numpy arrays, page-locked here if they are not already.
+        The library cuts the stack into chunks (``chunk_frames`` frames,
+        default about 8 MB); chunk i is copied in, solved and copied out on
+        stream i % ``n_streams``
+        (default 4), so both directions of the host link and the solve run at
+        once.  Returns the pinned [T, H, W] result, bit-identical to
+        ``reduce_noise``."""
         def pinned(x):
             t = x if isinstance(x, torch.Tensor) else torch.from_numpy(numpy.asarray(x))
+            if t.device.type != "cpu":
+                raise TypeError("reduce_noise_host takes host arrays")
             if t.dtype != torch.float32:
                 t = t.float()
             t = t.contiguous()
@@ -330,76 +335,26 @@ class Solver:
         h_in = pinned(images)
         if h_in.dim() == 2:
             h_in = h_in.unsqueeze(0)
+        if h_in.dim() != 3:
+            raise ValueError("images must be [T, H, W] or [H, W]")
         T, H, W = h_in.shape
         h_g = pinned(gamma)
-        per_frame = h_g.dim() == 3
+        if tuple(h_g.shape) == (H, W):
+            per_frame = 0
+        elif tuple(h_g.shape) == (T, H, W):
+            per_frame = 1
+        else:
+            raise ValueError("gamma must be [H, W] or [T, H, W]")
         if out is None:
             out = torch.empty((T, H, W), dtype=torch.float32).pin_memory()
-        if T == 0:
-            return out
-        if chunk_frames is None:
-            # 16 chunks: short pipeline fill and drain, chunks still large enough to
-            # fill the GPU (200 x 512 x 512 on B200: 5.1 ms vs 5.4 ms with 8 chunks)
-            chunk_frames = max(1, -(-T // 16))
-        chunk_frames = max(1, min(int(chunk_frames), T))
-        n_streams = max(1, int(n_streams))
-        if self.mask_shifted is None:
-            raise RuntimeError("set an OTF mask first")
-        # Streams, handles and device chunk buffers persist across calls, so a
-        # repeated call allocates nothing (new streams would defeat the caching
-        # allocator, which keeps blocks per stream).
-        pipe = getattr(self, "_pipe", None)
-        if pipe is None or len(pipe["solvers"]) != n_streams:
-            pipe = {"solvers": [Solver(device=self.device) for _ in range(n_streams)],
-                    "streams": [torch.cuda.Stream(device=self.device) for _ in range(n_streams)],
-                    "bufs": None, "key": None}
-            self._pipe = pipe
-        for sv in pipe["solvers"]:
-            sv.params = _lib.NcsbParams.from_buffer_copy(self.params)
-            sv._check(sv.lib.ncsb_set_params(sv._handle, ctypes.byref(sv.params)))
-            if sv.mask_shifted is None or not numpy.array_equal(sv.mask_shifted, self.mask_shifted):
-                sv.set_otf_mask_shifted(self.mask_shifted)
-        solvers, streams = pipe["solvers"], pipe["streams"]
-        key = (chunk_frames, H, W, per_frame)
-        cur = torch.cuda.current_stream(self.device)
+        elif (out.device.type != "cpu" or out.dtype != torch.float32
+              or tuple(out.shape) != (T, H, W) or not out.is_contiguous()):
+            raise ValueError("out must be a contiguous float32 host tensor [T, H, W]")
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
         with torch.cuda.device(self.device):
-            if pipe["key"] != key:
-                pipe["bufs"] = [
-                    (torch.empty((chunk_frames, H, W), dtype=torch.float32, device=self.device),
-                     torch.empty((chunk_frames, H, W), dtype=torch.float32, device=self.device),
-                     torch.empty((chunk_frames, H, W), dtype=torch.float32, device=self.device)
-                     if per_frame else None)
-                    for _ in streams]
-                pipe["key"] = key
-            bufs = pipe["bufs"]
-            d_g = None if per_frame else h_g.to(self.device, non_blocking=True)
-            ready = torch.cuda.Event()
-            ready.record(cur)
-            for st in streams:
-                st.wait_event(ready)
-            for i, f0 in enumerate(range(0, T, chunk_frames)):
-                n = min(chunk_frames, T - f0)
-                k = i % n_streams
-                st, (d_in, d_out, d_gf) = streams[k], bufs[k]
-                with torch.cuda.stream(st):
-                    d_in[:n].copy_(h_in[f0:f0 + n], non_blocking=True)
-                    g = d_g
-                    if per_frame:
-                        d_gf[:n].copy_(h_g[f0:f0 + n], non_blocking=True)
-                        g = d_gf[:n]
-                    solvers[k].reduce_noise(d_in[:n], g, out=d_out[:n], stream=st)
-                    out[f0:f0 + n].copy_(d_out[:n], non_blocking=True)
-            done = []
-            for st in streams:
-                ev = torch.cuda.Event()
-                ev.record(st)
-                done.append(ev)
-            for ev in done:
-                cur.wait_event(ev)  # the caller's stream orders after the whole pipeline
-            for st in streams:
-                st.synchronize()
-            if d_g is not None:
-                d_g.record_stream(cur)
+            self._check(self.lib.ncsb_reduce_noise_host(
+                self._handle, _ptr(h_in), T, H, W, _ptr(h_g), per_frame, _ptr(out),
+                int(chunk_frames or 0), int(n_streams or 0), ctypes.c_void_p(s.cuda_stream)))
         return out
 
     def solve_tiles(self, data, gamma, u0=None, stream=None):

@@ -233,9 +233,11 @@ def test_accuracy_gate_on_synthetic_frames(ncs, mode):
 
 
 def test_host_pipeline_equals_device_solve(ncs, mode):
-    """Solver.reduce_noise_host (chunks over 3 streams, one handle each) gives
+    """Solver.reduce_noise_host (ncsb_reduce_noise_host: chunks, each copied
+    in, solved and copied out on one of the handle's streams) gives
     bit-identical frames to the device-resident solve, for shared and
-    per-frame gamma and for a chunk size that does not divide the stack."""
+    per-frame gamma, chunk sizes that do not divide the stack, more chunks
+    than streams, and a handle reused for a larger frame."""
     rng = numpy.random.default_rng(11)
     T, H, W = 7, 40, 52
     images = rng.uniform(1.0, 90.0, size=(T, H, W)).astype(numpy.float32)
@@ -245,5 +247,12 @@ def test_host_pipeline_equals_device_solve(ncs, mode):
     s.set_otf_mask_shifted(create_otf_mask_shifted())
     for g in (gamma, gframes):
         ref = s.reduce_noise(torch.from_numpy(images).cuda(), torch.from_numpy(g).cuda()).cpu()
-        got = s.reduce_noise_host(images, g, chunk_frames=3)
-        assert torch.equal(got, ref)
+        for chunk, ns in ((3, 2), (3, 4), (None, None), (1, 8), (2, 3), (2, 1)):
+            got = s.reduce_noise_host(images, g, chunk_frames=chunk, n_streams=ns)
+            assert torch.equal(got, ref)
+    big = rng.uniform(1.0, 90.0, size=(3, 70, 45)).astype(numpy.float32)
+    gbig = rng.uniform(1.0, 20.0, size=(70, 45)).astype(numpy.float32)
+    ref = s.reduce_noise(torch.from_numpy(big).cuda(), torch.from_numpy(gbig).cuda()).cpu()
+    assert torch.equal(s.reduce_noise_host(big, gbig, chunk_frames=1), ref)
+    with pytest.raises(ValueError):
+        s.reduce_noise_host(images, gamma[:10])

@@ -13,13 +13,14 @@
 // ||g|| <= epsilon max(1, ||u||) about threefold (stack512: 14.6 -> 5.0 mean,
 // one line-search trial per iteration), so each solve does less work although
 // an iteration now applies two Fourier-diagonal operators:
-//   * the first half of the two-loop leaves q; one forward 16x16 FFT of q and
-//     one complex inverse FFT give H0 q (real part) and Q H0 q (imaginary
-//     part), spectral weights 1/(lambda + 2 alpha M^2) and
-//     M^2 / (lambda + 2 alpha M^2);
+//   * the first half of the two-loop leaves q; one forward 16x16 FFT of q,
+//     the spectral weight 1/(lambda + 2 alpha M^2) and one inverse FFT give
+//     H0 q.  Because (lambda + 2 alpha M^2) h = 1 in every bin,
+//     2 alpha Q H0 q = q - lambda H0 q needs no transform of its own;
 //   * the second half adds coef_i s_i to the direction and coef_i Q s_i to
-//     w = Q p, with Q s_i = t_i w_i stored with each pair -- so w = Q p, which
-//     the exact line search needs (ncs_plain.cu), costs no extra transform.
+//     w = 2 alpha Q p, with 2 alpha Q s_i = t_i w_i stored with each pair --
+//     so w, which the exact line search needs (ncs_plain.cu), costs no
+//     extra transform.  v = 2 alpha Q u is kept the same way.
 // Everything else -- FP64 cost-difference Armijo test with the fraction-to-
 // barrier rule, stopping rules, status codes, device segmentation and owner-
 // rule stitching -- is that of the other solvers.  The first trial step is 1
@@ -209,8 +210,9 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
         for (int i = 0; i < 8; ++i) c[i] = d[i] + gm[i];
 
         // ---- preconditioned L-BFGS ---------------------------------------------
-        // Pass 0 transforms u (v = Q u, initial gradient); later passes
+        // Pass 0 transforms u (v = 2 alpha Q u, initial gradient); later passes
         // transform the two-loop vector q.  One call site for each FFT half.
+        // v = 2 alpha Q u and w = 2 alpha Q p carry the factor 2 alpha.
         float v[8], g[8], p[8], w[8];
         float rho[MaxM], al[MaxM];
         int status = kUnstarted, iters = 0, evals = 1, k = 0, newest = -1;
@@ -252,9 +254,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     }
                 }
             }
-            // spectral step: one forward transform and one complex inverse one,
-            // whose real part is H0 q and imaginary part Q H0 q (pass 0: Q u
-            // alone).  Both spectral weights are real and symmetric in k.
+            // spectral step: p = H0 q (pass 0: 2 alpha Q u) by one forward and
+            // one inverse transform; the weights are real and symmetric in k.
             float2 spec[8];
             warp_fft_fwd(q, spec, ws, G);
             float mk[8];
@@ -265,20 +266,22 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             }
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                const float hq = __fdividef(1.0f, fmaf(two_alpha_256, mk[i], lam));
-                const float w0 = first ? mk[i] : hq * (1.0f / 256.0f);
-                const float w1 = first ? 0.0f : mk[i] * hq;
-                spec[i] = make_float2(fmaf(spec[i].x, w0, -spec[i].y * w1),
-                                      fmaf(spec[i].y, w0, spec[i].x * w1));
+                const float wgt = first ? two_alpha * mk[i]
+                                        : __fdividef(1.0f / 256.0f, fmaf(two_alpha_256, mk[i], lam));
+                spec[i] = make_float2(spec[i].x * wgt, spec[i].y * wgt);
             }
-            float y1[8];
-            warp_fft_inv2(spec, p, y1, ws, G);
-            if (!first) {  // a start pass keeps w (Q u0 of a proposal)
+            warp_fft_inv(spec, p, ws, G);
+            if (!first) {  // w = 2 alpha Q H0 q = q - lambda H0 q
+                if (two_alpha > 0.0f) {
 #pragma unroll
-                for (int i = 0; i < 8; ++i) w[i] = y1[i];
+                    for (int i = 0; i < 8; ++i) w[i] = fmaf(-lam, p[i], q[i]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) w[i] = 0.0f;
+                }
             }
             if (first) {
-                if (start_pass == 2) {  // keep Q u0, transform d next
+                if (start_pass == 2) {  // keep 2 alpha Q u0, transform d next
 #pragma unroll
                     for (int i = 0; i < 8; ++i) w[i] = p[i];
                     start_pass = 1;
@@ -286,7 +289,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 }
                 if (start_pass == 1) {
                     // f(u0) - f(d) = sum[(u0 - d) - c (log(u0 + gamma) - log(d + gamma))]
-                    //                + alpha (u0'Q u0 - d'Q d);  p = Q d, w = Q u0
+                    //                + alpha (u0'Q u0 - d'Q d);  p = 2 alpha Q d,
+                    //                w = 2 alpha Q u0
                     float dd[8];
                     load_d(dd);
                     float dl = 0.0f, dq = 0.0f;
@@ -300,7 +304,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                         dl += fmaf(-c[i], lr, u[i] - dd[i]);
                         dq += __fsub_rn(__fmul_rn(u[i], w[i]), __fmul_rn(dd[i], p[i]));
                     }
-                    const double delta = warp_sum_d((double)dl + (double)alpha * (double)dq);
+                    const double delta = warp_sum_d((double)dl + 0.5 * (double)dq);
                     if (delta <= 0.0) {
 #pragma unroll
                         for (int i = 0; i < 8; ++i) p[i] = w[i];
@@ -318,7 +322,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     v[i] = p[i];
                     const float ia = __fdividef(1.0f, fmaxf(u[i] + gm[i], kFitMin));
                     const float r = c[i] * ia;
-                    g[i] = 1.0f - r + two_alpha * v[i];
+                    g[i] = 1.0f - r + v[i];
                     uu = fmaf(u[i], u[i], uu);
                     gg = fmaf(g[i], g[i], gg);
                     ll = fmaf(r, ia, ll);
@@ -390,7 +394,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 ++evals;
                 const double td = (double)t;
                 const double delta = any_cross ? CUDART_INF
-                                               : dl + (double)alpha * (2.0 * td * dpv + td * td * dpw);
+                                               : dl + td * dpv + 0.5 * td * td * dpw;
                 if (delta <= (double)a.c1 * td * gd) { ok = true; break; }
                 t *= 0.5f;
                 if (!(t >= a.min_step)) break;  // also stops on NaN
@@ -407,7 +411,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 v[i] += w[i];
                 const float ia = __fdividef(1.0f, fmaxf(un + gm[i], kFitMin));
                 const float r = c[i] * ia;
-                const float gn = 1.0f - r + two_alpha * v[i];
+                const float gn = 1.0f - r + v[i];
                 s[i] = un - u[i];
                 y[i] = gn - g[i];
                 mv += (s[i] != 0.0f) ? 1.0f : 0.0f;
@@ -453,7 +457,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             }
             e0 = warp_sum_d(e0);
             e1 = warp_sum_d(e1);
-            if (lane == 0) a.cost[tile] = e0 + (double)alpha * e1;
+            if (lane == 0) a.cost[tile] = e0 + 0.5 * e1;  // v = 2 alpha Q u
         }
         if (lane == 0) {
             if (a.iters) a.iters[tile] = iters;

@@ -262,27 +262,6 @@ __device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float (&y)[8], Warp
     }
 }
 
-// Two real tiles from one complex inverse: e = A + i B with A and B spectra
-// of real tiles (Hermitian) gives y0 = the tile of A and y1 = that of B
-// (unnormalised).  One column stage serves both; rows P and P + 8 each take
-// a complex row transform.
-__device__ __forceinline__ void warp_fft_inv2(float2 (&e)[8], float (&y0)[8], float (&y1)[8],
-                                              WarpSmem& ws, const LaneGeo& L) {
-    warp_ifft_cols(e, ws, L);
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-        float2 V[4], z[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) V[k] = ws.fb[L.P + 8 * s][L.k0 + k];
-        warp_ifft_row(V, z, L);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            y0[2 * j + s] = z[j].x;
-            y1[2 * j + s] = z[j].y;
-        }
-    }
-}
-
 // y = Q x for the 8 pixels of this lane; mt = this lane's 8 values of
 // M^2/256 in the column-pass layout.
 __device__ __forceinline__ void warp_apply_q(const float (&x)[8], float (&y)[8], WarpSmem& ws,

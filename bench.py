@@ -384,7 +384,9 @@ def run_ours(args, world, rank, local):
     h_in = images.cpu().pin_memory()
     h_gamma = gamma.cpu().pin_memory()
     h_out = torch.empty_like(h_in).pin_memory()
-    e2e_steps = max(1, min(args.steps, 5))
+    # at least ~20 stacks: the host link is shared with the machine's other
+    # GPUs, so a short window is noisy
+    e2e_steps = max(1, min(2 * args.steps, 20))
     solver.reduce_noise_host(h_in, h_gamma, out=h_out)  # warm-up: streams, handles, buffers
     barrier(world)
     torch.cuda.synchronize()

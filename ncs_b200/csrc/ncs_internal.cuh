@@ -210,11 +210,11 @@ __device__ __forceinline__ float warp_transpose_sum32(float (&v)[32], int lane) 
     return v[0];
 }
 
-// Same for N = 16 or 32 values: lane v ends with the warp total of value
-// v & (N - 1) (the two half-warps are combined last when N = 16).
+// Same for N = 8, 16 or 32 values: lane v ends with the warp total of value
+// v & (N - 1) (lanes that differ only above bit log2 N are combined last).
 template <int N>
 __device__ __forceinline__ float warp_transpose_sum(float (&v)[N], int lane) {
-    static_assert(N == 16 || N == 32, "16 or 32 values");
+    static_assert(N == 8 || N == 16 || N == 32, "8, 16 or 32 values");
 #pragma unroll
     for (int h = N / 2; h >= 1; h >>= 1) {
         const bool up = (lane & h) != 0;
@@ -225,7 +225,8 @@ __device__ __forceinline__ float warp_transpose_sum(float (&v)[N], int lane) {
             v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
         }
     }
-    if (N == 16) v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
+#pragma unroll
+    for (int o = N; o < 32; o <<= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
     return v[0];
 }
 

@@ -215,6 +215,10 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
         // v = 2 alpha Q u and w = 2 alpha Q p carry the factor 2 alpha.
         float v[8], g[8], p[8], w[8];
         float rho[MaxM], al[MaxM];
+        // s'g of the newest pair at the gradient it was stored with: the first
+        // two-loop dot of the next iteration, s'(-g), without a reduction
+        float sg_newest = 0.0f;
+        bool sg_fresh = false;
         int status = kUnstarted, iters = 0, evals = 1, k = 0, newest = -1;
         float lam = 1.0f;
         bool first = true;
@@ -242,11 +246,17 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                         int slot = newest - i;
                         if (slot < 0) slot += mcap;
                         float hv[8];
-                        load8(hs + slot * 64 + lane * 2, hv);
-                        float acc = 0.0f;
+                        float dot;
+                        if (i == 0 && sg_fresh) {
+                            dot = -sg_newest;  // q = -g here
+                        } else {
+                            load8(hs + slot * 64 + lane * 2, hv);
+                            float acc = 0.0f;
 #pragma unroll
-                        for (int e = 0; e < 8; ++e) acc = fmaf(hv[e], q[e], acc);
-                        const float ai = rho[i] * warp_sum_f(acc);
+                            for (int e = 0; e < 8; ++e) acc = fmaf(hv[e], q[e], acc);
+                            dot = warp_sum_f(acc);
+                        }
+                        const float ai = rho[i] * dot;
                         al[i] = ai;
                         load8(hy + slot * 64 + lane * 2, hv);
 #pragma unroll
@@ -257,7 +267,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             // spectral step: p = H0 q (pass 0: 2 alpha Q u) by one forward and
             // one inverse transform; the weights are real and symmetric in k.
             float2 spec[8];
-            warp_fft_fwd(q, spec, ws, G);
+            warp_fft_fwd<false>(q, spec, ws, G);  // 2 F q: the weights hold the 1/2
             float mk[8];
             {
                 const float4 m0 = Batch ? __ldg(mkp) : mkp[0], m1 = Batch ? __ldg(mkp + 1) : mkp[1];
@@ -266,8 +276,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             }
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                const float wgt = first ? two_alpha * mk[i]
-                                        : __fdividef(1.0f / 256.0f, fmaf(two_alpha_256, mk[i], lam));
+                const float wgt = first ? alpha * mk[i]
+                                        : __fdividef(1.0f / 512.0f, fmaf(two_alpha_256, mk[i], lam));
                 spec[i] = make_float2(spec[i].x * wgt, spec[i].y * wgt);
             }
             warp_fft_inv(spec, p, ws, G);
@@ -361,14 +371,15 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 pv = fmaf(p[i], v[i], pv);
                 pw = fmaf(p[i], w[i], pw);
             }
-            const double gd = warp_sum_d((double)gp);
-            const double dpv = warp_sum_d((double)pv), dpw = warp_sum_d((double)pw);
+            double gd = (double)gp, dpv = (double)pv, dpw = (double)pw;
+            warp_sum3_d(gd, dpv, dpw, lane);
             if (!(gd < 0.0)) {
                 // not a descent direction: drop the history (H0 alone is positive
                 // definite); fail only if even that does not descend
                 if (k == 0) { status = kIncreasingGradient; break; }
                 k = 0;
                 newest = -1;
+                sg_fresh = false;
                 continue;
             }
 
@@ -403,7 +414,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 
             // accept; new pair (s, y, Q s = t w)
             float s[8], y[8];
-            float sy = 0.0f, uu = 0.0f, gg = 0.0f, ll = 0.0f, mv = 0.0f;
+            float sy = 0.0f, uu = 0.0f, gg = 0.0f, ll = 0.0f, mv = 0.0f, sg = 0.0f;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const float un = fmaf(t, p[i], u[i]);
@@ -418,24 +429,28 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 u[i] = un;
                 g[i] = gn;
                 sy = fmaf(s[i], y[i], sy);
+                sg = fmaf(s[i], gn, sg);
                 uu = fmaf(un, un, uu);
                 gg = fmaf(gn, gn, gg);
                 ll = fmaf(r, ia, ll);
             }
             {
-                float vals[16] = {sy, uu, gg, ll, mv};
-                const float tot = warp_transpose_sum<16>(vals, lane);
+                float vals[8] = {sy, uu, gg, ll, mv, sg};
+                const float tot = warp_transpose_sum<8>(vals, lane);
                 sy = __shfl_sync(kFull, tot, 0);
                 uu = __shfl_sync(kFull, tot, 1);
                 gg = __shfl_sync(kFull, tot, 2);
                 ll = __shfl_sync(kFull, tot, 3);
                 mv = __shfl_sync(kFull, tot, 4);
+                sg = __shfl_sync(kFull, tot, 5);
             }
             ++iters;
             lam = ll * (1.0f / 256.0f);
             if (sqrtf(gg) <= a.eps * fmaxf(sqrtf(uu), 1.0f)) { status = kSuccess; break; }
             if (mv == 0.0f) { status = kReachedMaxPrecision; break; }
+            sg_fresh = sy > 0.0f;
             if (sy > 0.0f) {
+                sg_newest = sg;
                 newest = newest + 1 == mcap ? 0 : newest + 1;
                 store8(hs + newest * 64 + lane * 2, s);
                 store8(hy + newest * 64 + lane * 2, y);

@@ -146,7 +146,10 @@ __device__ __forceinline__ LaneGeo lane_geo(int lane) {
 
 // Forward half of the 16x16 transform: lane (KC = L>>1, H = L&1) ends with
 // the spectrum X[2 bitrev3(i) + H][KC] of its 8 pixels' tile in e[i]
-// (unnormalised).  Input: x[2j] = row P, x[2j+1] = row P+8, column Qd + 4j.
+// (unnormalised; with Halve = false, 2 X, for callers that fold the factor
+// 1/2 of the row-pair separation into a later scaling).  Input: x[2j] = row
+// P, x[2j+1] = row P+8, column Qd + 4j.
+template <bool Halve = true>
 __device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8], WarpSmem& ws,
                                              const LaneGeo& L) {
     // rows: 4-point DFT over j in the lane, twiddle, 4-point DFT across lanes
@@ -185,7 +188,8 @@ __device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8]
     for (int p = 0; p < 8; ++p) {
         const float2 Z = ws.fb[p][L.KC], Zm = ws.fb[p][kneg];
         const float sx = Z.x + Zm.x, dx = Z.x - Zm.x, sy = Z.y + Zm.y, dy = Z.y - Zm.y;
-        float2 ev = make_float2(0.5f * fmaf(L.sH, sy, sx), 0.5f * fmaf(-L.sH, dx, dy));
+        float2 ev = make_float2(fmaf(L.sH, sy, sx), fmaf(-L.sH, dx, dy));
+        if (Halve) ev = make_float2(0.5f * ev.x, 0.5f * ev.y);
         const float2 w = w16(p);
         e[p] = L.H ? cmul(ev, w) : ev;
     }
@@ -302,6 +306,22 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
     return v;
+}
+
+// Warp totals of three FP64 values: the first two levels exchange halves of
+// a 4-slot vector (slot 3 empty), so lane L & 3 = j ends with total j after
+// 6 double shuffles; 3 more broadcast them (15 for three plain sums).
+__device__ __forceinline__ void warp_sum3_d(double& a, double& b, double& c, int lane) {
+    const bool up2 = (lane & 2) != 0, up1 = (lane & 1) != 0;
+    const double s0 = up2 ? a : c, s1 = up2 ? b : 0.0;
+    double v0 = (up2 ? c : a) + __shfl_xor_sync(kFull, s0, 2);
+    double v1 = (up2 ? 0.0 : b) + __shfl_xor_sync(kFull, s1, 2);
+    v0 = (up1 ? v1 : v0) + __shfl_xor_sync(kFull, up1 ? v0 : v1, 1);
+#pragma unroll
+    for (int o = 4; o < 32; o <<= 1) v0 += __shfl_xor_sync(kFull, v0, o);
+    a = __shfl_sync(kFull, v0, 0);
+    b = __shfl_sync(kFull, v0, 1);
+    c = __shfl_sync(kFull, v0, 2);
 }
 
 __device__ __forceinline__ float warp_sum_f(float v) {

@@ -76,6 +76,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
     static_assert(MaxM >= 1 && MaxM <= kMaxM, "history capacity");
     extern __shared__ __align__(16) unsigned char dsm[];
     const int mcap = a.m < 1 ? 1 : (a.m > MaxM ? MaxM : a.m);
+    // stopping rule ||g|| <= eps max(||u||, 1), compared squared
+    const float eps2 = a.eps * a.eps;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* mtab = reinterpret_cast<float*>(dsm);
     unsigned char* wbase = dsm + kTableBytes + (size_t)wid * spec_warp_bytes(mcap);
@@ -277,7 +279,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const float wgt = first ? alpha * mk[i]
-                                        : __fdividef(1.0f / 512.0f, fmaf(two_alpha_256, mk[i], lam));
+                                        : (1.0f / 512.0f) * rcp_fast(fmaf(two_alpha_256, mk[i], lam));
                 spec[i] = make_float2(spec[i].x * wgt, spec[i].y * wgt);
             }
             warp_fft_inv(spec, p, ws, G);
@@ -330,7 +332,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
                     v[i] = p[i];
-                    const float ia = __fdividef(1.0f, fmaxf(u[i] + gm[i], kFitMin));
+                    const float ia = rcp_fast(fmaxf(u[i] + gm[i], kFitMin));
                     const float r = c[i] * ia;
                     g[i] = 1.0f - r + v[i];
                     uu = fmaf(u[i], u[i], uu);
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 uu = warp_sum_f(uu);
                 gg = warp_sum_f(gg);
                 lam = warp_sum_f(ll) * (1.0f / 256.0f);
-                if (sqrtf(gg) <= a.eps * fmaxf(sqrtf(uu), 1.0f)) { status = kSuccess; break; }
+                if (gg <= eps2 * fmaxf(uu, 1.0f)) { status = kSuccess; break; }
                 continue;
             }
             // two-loop, second half (oldest pair first): p += coef s, w += coef Q s
@@ -391,12 +393,15 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 bool cross = false;
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
+                    // log(max(ni, F)) - log(max(ai, F)) = log1p((max(ni, F) - A) / A),
+                    // A = max(ai, F); above the floor the numerator is the exact
+                    // step tp (branch free: one select instead of a branch)
                     const float ai = u[i] + gm[i];
                     const float tp = t * p[i];
                     const float ni = ai + tp;
-                    float l;
-                    if (ai >= kFitMin && ni >= kFitMin) l = log1p_ls(__fdividef(tp, ai));
-                    else l = __logf(fmaxf(ni, kFitMin)) - __logf(fmaxf(ai, kFitMin));
+                    const bool in_dom = ai >= kFitMin && ni >= kFitMin;
+                    const float A = fmaxf(ai, kFitMin);
+                    const float l = log1p_ls((in_dom ? tp : fmaxf(ni, kFitMin) - A) * rcp_fast(A));
                     cross |= (ai >= kFitMin) && (ni < kBarrierFrac * ai);
                     term += fmaf(-c[i], l, tp);
                 }
@@ -420,7 +425,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 const float un = fmaf(t, p[i], u[i]);
                 w[i] *= t;
                 v[i] += w[i];
-                const float ia = __fdividef(1.0f, fmaxf(un + gm[i], kFitMin));
+                const float ia = rcp_fast(fmaxf(un + gm[i], kFitMin));
                 const float r = c[i] * ia;
                 const float gn = 1.0f - r + v[i];
                 s[i] = un - u[i];
@@ -446,7 +451,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             }
             ++iters;
             lam = ll * (1.0f / 256.0f);
-            if (sqrtf(gg) <= a.eps * fmaxf(sqrtf(uu), 1.0f)) { status = kSuccess; break; }
+            if (gg <= eps2 * fmaxf(uu, 1.0f)) { status = kSuccess; break; }
             if (mv == 0.0f) { status = kReachedMaxPrecision; break; }
             sg_fresh = sy > 0.0f;
             if (sy > 0.0f) {
@@ -457,7 +462,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 store8(hq + newest * 64 + lane * 2, w);
 #pragma unroll
                 for (int i = MaxM - 1; i > 0; --i) rho[i] = rho[i - 1];
-                rho[0] = 1.0f / sy;
+                rho[0] = rcp_fast(sy);
                 if (k < mcap) ++k;
             }
         }

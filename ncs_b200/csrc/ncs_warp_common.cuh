@@ -286,12 +286,22 @@ __device__ __forceinline__ void warp_apply_q(const float (&x)[8], float (&y)[8],
     warp_fft_inv(e, y, ws, L);
 }
 
+// 1/x from the hardware reciprocal (PTX rcp.approx.ftz.f32: one MUFU
+// operation, relative error about 2^-23, subnormals flushed).  The solvers
+// only take reciprocals of values >= 1e-6 or of sums that are bounded away
+// from 0, where it matches 1/x to FP32 precision.
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // log1p(x) for x > -1: 2 atanh(y), y = x / (2 + x), by the odd series
 // 2y (1 + y^2/3 + ... + y^10/11) when |x| <= 1/2 (|y| <= 1/5, truncation
 // < 1e-9 relative); otherwise log(1 + x) from the hardware log2, whose
 // absolute error is small against |log(1 + x)| >= 0.4 there.
 __device__ __forceinline__ float log1p_ls(float x) {
-    const float y = __fdividef(x, 2.0f + x);
+    const float y = x * rcp_fast(2.0f + x);
     const float y2 = y * y;
     float s = fmaf(y2, 1.0f / 11.0f, 1.0f / 9.0f);
     s = fmaf(y2, s, 1.0f / 7.0f);

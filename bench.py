@@ -522,7 +522,7 @@ def run_ours(args, world, rank, local):
                 "h2d_bytes_per_step": int(h_in.numel() * 4 + h_gamma.numel() * 4),
                 "d2h_bytes_per_step": int(h_out.numel() * 4),
                 "api": "ncs_b200.Solver.reduce_noise_host -> ncsb_reduce_noise_host: pinned "
-                       "host buffers; T/25-frame chunks round-robin over 4 streams, each copying "
+                       "host buffers; T/40-frame chunks round-robin over 4 streams, each copying "
                        "in, solving and copying out"},
         "gpu_launches": args.steps,
         "clocks": clk,

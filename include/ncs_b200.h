@@ -131,7 +131,7 @@ int ncsb_reduce_noise(ncsb_handle *h, const float *images, int n_frames, int hei
  * works on host arrays).  images, gamma (shared or per frame, as in
  * ncsb_reduce_noise) and out are host pointers; page-locked memory lets the
  * copies overlap the solve.  The stack is cut into chunks of chunk_frames
- * frames (<= 0: n_frames / 25, at most 64 MB); chunk i is copied in, solved
+ * frames (<= 0: n_frames / 40, at most 64 MB); chunk i is copied in, solved
  * and copied out on
  * the handle's stream i % n_streams (<= 0: 4; at most 8), each stream with its own
  * device buffers and work counter, so one chunk's copies overlap other

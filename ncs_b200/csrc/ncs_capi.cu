@@ -373,11 +373,11 @@ int ncsb_reduce_noise_host(ncsb_handle* h, const float* images, int n_frames, in
     if (n_frames == 0) return NCSB_OK;
     const size_t frame_px = (size_t)height * width;
     if (chunk_frames <= 0) {
-        // about 25 chunks per stack (fastest on B200 for 200 x 512^2 and
-        // 100 x 2048^2: short fill and drain, few per-chunk gaps), at most
-        // 64 MB each
+        // about 40 chunks per stack (fastest on B200 for 200 x 512^2 and
+        // close to it for 100 x 2048^2: short fill and drain, few per-chunk
+        // gaps), at most 64 MB each
         const int cap = (int)(64.0e6 / (4.0 * (double)frame_px));
-        chunk_frames = (n_frames + 12) / 25;
+        chunk_frames = (n_frames + 20) / 40;
         if (chunk_frames > cap) chunk_frames = cap;
         if (chunk_frames < 1) chunk_frames = 1;
     }

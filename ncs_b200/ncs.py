@@ -319,7 +319,7 @@ class Solver:
         ``images`` [T, H, W] and ``gamma`` [H, W] or [T, H, W] are float32 CPU
         tensors or numpy arrays, page-locked here if they are not already.
         The library cuts the stack into chunks (``chunk_frames`` frames,
-        default T / 25, at most 64 MB); chunk i is copied in, solved and
+        default T / 40, at most 64 MB); chunk i is copied in, solved and
         copied out on stream i % ``n_streams`` (default 4), so both directions
         of the host link and the solve run at once.  Returns the pinned
         [T, H, W] result, bit-identical to ``reduce_noise``."""

@@ -45,14 +45,14 @@ sys.path.insert(0, ROOT)
 # plain form (scalar initial matrix), per iteration: Q p (11,264),
 #   directional dots (1,536), accepted point + gradient (2,304), norms and
 #   curvature dots (2,048), plus 2,048 per stored pair (2 dots, 2 axpys)
-# spectral form, per iteration: one forward + two inverse FFTs and two
-#   spectrum weightings (17,408), directional dots (1,536), accepted point
-#   + gradient + curvature (2,816), norms and lambda (2,048), plus 2,560 per
-#   stored pair (2 dots, 3 axpys)
+# spectral form, per iteration: one forward + one inverse FFT, the spectrum
+#   weighting and w = q - lambda p (11,776), directional dots (1,536),
+#   accepted point + gradient + curvature (2,816), norms and lambda (2,048),
+#   plus 2,560 per stored pair (2 dots, 3 axpys)
 FLOP_INIT = 11264 + 3328
 FLOP_TRIAL = 2048
 FLOP_ITER_BASE = {"plain": 11264 + 1536 + 2304 + 2048, "plain_wg": 11264 + 1536 + 2304 + 2048,
-                  "spectral": 17408 + 1536 + 2816 + 2048}
+                  "spectral": 11776 + 1536 + 2816 + 2048}
 FLOP_PER_PAIR = {"plain": 4 * 256 * 2, "plain_wg": 4 * 256 * 2, "spectral": 5 * 256 * 2}
 # multiply-adds x 2 of the warm-start network per 16x16 tile:
 # 256 px x 9 taps x (2*32 + 32*32 + 32*32 + 32*1)

@@ -23,11 +23,17 @@
 // applies ReLU, rounds to BF16 and writes the next layer's operand -- zeros at
 // the plane's border positions, which are the next layer's zero padding.
 //
-// Two CTAs (4 warps each) per SM, persistent over tiles, so one CTA's
-// epilogue overlaps the other's MMAs; thread 0 of a CTA issues its MMAs
-// and commits them to an mbarrier that all threads wait on.  Every wait is
-// bounded; a timed-out wait sets the caller's status flag, drains with a
-// second bounded wait, frees the tensor memory and ends the kernel.
+// A layer's MMAs have finished reading their input before its epilogue
+// runs, so the epilogue overwrites that input in place: one activation
+// buffer per tile.  A CTA (4 warps) keeps two tiles in flight in two slots,
+// each with its buffer, 128 tensor-memory columns and an mbarrier, and
+// alternates between them: wait for a slot's MMAs, run its epilogue, issue
+// its next layer (or start its next tile), turn to the other slot -- so one
+// slot's epilogue runs while the other slot's MMAs do.  Two such CTAs share
+// an SM, persistent over tiles.  Thread 0 issues the MMAs and commits them
+// to the slot's mbarrier, which all threads wait on.  Every wait is bounded;
+// a timed-out wait sets the caller's status flag, drains the outstanding
+// MMAs with bounded waits, frees the tensor memory and ends the kernel.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -49,7 +55,8 @@ constexpr int kW1Bytes = 4 * 32 * 16;            // layer 1: K 32 x N 32
 constexpr int kWtapBytes = 4 * 32 * 16;          // layers 2, 3: per tap K 32 x N 32
 constexpr int kW4tapBytes = 4 * 16 * 16;         // layer 4: per tap K 32 x N 16
 constexpr float kStartFrac = 0.05f;
-constexpr unsigned kTmemCols = 128;
+constexpr int kSlots = 2;                // tiles in flight per CTA
+constexpr unsigned kTmemCols = 256;      // 128 columns per slot
 constexpr long long kWaitTries = 1ll << 22;  // mbarrier polls before giving up (seconds)
 
 // shared-memory plan (bytes, all 128-B aligned)
@@ -57,15 +64,15 @@ constexpr int kOffW1 = 0;
 constexpr int kOffW2 = kOffW1 + kW1Bytes;
 constexpr int kOffW3 = kOffW2 + 9 * kWtapBytes;
 constexpr int kOffW4 = kOffW3 + 9 * kWtapBytes;
-constexpr int kOffAct0 = kOffW4 + 9 * kW4tapBytes;
-constexpr int kOffAct1 = kOffAct0 + kActBytes;
-// the layer-1 im2col operand lives in activation buffer 1 at positions
-// 19..402 -- the range the later epilogue rewrites -- so the zero border
-// positions of that buffer are never touched
+constexpr int kOffAct = kOffW4 + 9 * kW4tapBytes;             // one buffer per slot
+// the layer-1 im2col operand lives in the slot's activation buffer at
+// positions 19..402 -- the range every epilogue rewrites -- so the zero
+// border positions of the buffer are never touched
 constexpr int kIm2colPos = 19;
-constexpr int kOffBias = kOffAct1 + kActBytes;                // 3 x 32 + 1 floats
-constexpr int kOffTile = kOffBias + 128 * 4;                  // d, gamma, x0, x1: 4 x 256 floats
-constexpr int kSmemBytes = kOffTile + 4 * 256 * 4;
+constexpr int kOffBias = kOffAct + kSlots * kActBytes;        // 3 x 32 + 1 floats
+constexpr int kOffTile = kOffBias + 128 * 4;                  // per slot d, gamma, x0, x1
+constexpr int kTileBytes = 4 * 256 * 4;
+constexpr int kSmemBytes = kOffTile + kSlots * kTileBytes;
 
 struct Src {
     int tile_mode;
@@ -176,11 +183,32 @@ __device__ __forceinline__ void store_pos(unsigned char* buf, int chunk_bytes, i
     }
 }
 
+// The 54 MMAs of a 3x3 layer over one slot: 3 M blocks x 9 taps x 2 K steps,
+// every operand offset and accumulate flag a compile-time constant (the
+// issuing thread is on the critical path: the other threads wait at the next
+// barrier while it issues).  NOut = 32, or 16 for the last layer.
+template <int NOut>
+__device__ __forceinline__ void issue_taps(uint32_t td, uint64_t a0, uint64_t b0) {
+    constexpr uint32_t id = idesc(128, NOut);
+    constexpr int tap_bytes = NOut == 32 ? kWtapBytes : kW4tapBytes;
+    constexpr int wchunk = NOut * 16;
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                const int pos = kPlane + 128 * m + (tap / 3 - 1) * kPlane + (tap % 3 - 1) + 1;
+                mma(td + m * NOut, a0 + (((2 * ks) * kChunkA + pos * 16) >> 4),
+                    b0 + ((tap * tap_bytes + (2 * ks) * wchunk) >> 4), id, (tap | ks) != 0);
+            }
+}
+
 __global__ void __launch_bounds__(kThreads, 2)
     infer_tc(const Src src, const float* __restrict__ params, float* __restrict__ u0,
              int32_t* __restrict__ status) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bar[kSlots];
     __shared__ uint32_t tmem_base_s;
     __shared__ float red[8];
     const int t = threadIdx.x, warp = t >> 5;
@@ -221,10 +249,12 @@ __global__ void __launch_bounds__(kThreads, 2)
     float* sBias = reinterpret_cast<float*>(sm + kOffBias);
     for (int i = t; i < 97; i += kThreads)
         sBias[i] = i < 32 ? b1[i] : (i < 64 ? b2[i - 32] : (i < 96 ? b3[i - 64] : b4[0]));
-    for (int i = t; i < 2 * kActBytes / 16; i += kThreads)
-        reinterpret_cast<uint4*>(sm + kOffAct0)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = t; i < kSlots * kActBytes / 16; i += kThreads)
+        reinterpret_cast<uint4*>(sm + kOffAct)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (t == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+        for (int sl = 0; sl < kSlots; ++sl)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[sl]))
+                         : "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -237,41 +267,29 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
     fence_after();
     const uint32_t tmem = tmem_base_s;
-    const uint32_t bar_a = smem_u32(&bar);
     const uint32_t lane_off = (uint32_t)(warp * 32) << 16;  // this warp's TMEM lanes
-    uint32_t phase = 0;
-    bool alive = true;
-
-    float* sD = reinterpret_cast<float*>(sm + kOffTile);
-    float* sG = sD + 256;
-    float* sX0 = sG + 256;
-    float* sX1 = sX0 + 256;
-    unsigned char* act[2] = {sm + kOffAct0, sm + kOffAct1};
-    unsigned char* im2col = sm + kOffAct1 + kIm2colPos * 16;
     const uint32_t sW1a = smem_u32(sm + kOffW1), sW2a = smem_u32(sm + kOffW2);
     const uint32_t sW3a = smem_u32(sm + kOffW3), sW4a = smem_u32(sm + kOffW4);
-    const uint32_t act_a[2] = {smem_u32(act[0]), smem_u32(act[1])};
-    const uint32_t im_a = smem_u32(im2col);  // chunk stride kChunkA, like the activations
     const long long per_frame = (long long)src.tiles_x * src.tiles_y;
+    const long long stride = (long long)kSlots * gridDim.x;  // tiles between a slot's tiles
 
-    // all threads: wait for the layer's committed MMAs (block-uniform outcome;
-    // on a timeout the phase stays, so the drain below waits on the same one)
-    auto sync_mma = [&]() -> bool {
-        const bool ok = wait_bounded(bar_a, phase);
-        const bool all = __syncthreads_and(ok) != 0;
-        if (all) phase ^= 1u;
-        fence_after();
-        return all;
-    };
+    // per-slot state, block-uniform: current tile, next layer to wait for,
+    // mbarrier phase, feature scale; and this thread's prefetched pixels
+    long long tile_s[kSlots] = {};
+    int layer_s[kSlots] = {};
+    uint32_t phase_s[kSlots] = {};
+    float scale_s[kSlots] = {};
+    float dv[kSlots][2] = {}, gv[kSlots][2] = {};
+    bool alive = true;
 
     // this thread's two pixels of a tile (the solvers' segmentation)
-    auto gather = [&](long long tile, float (&dv)[2], float (&gv)[2]) {
+    auto gather = [&](long long tile, float (&dvo)[2], float (&gvo)[2]) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int p = t + 128 * h, r = p >> 4, c = p & 15;
             if (src.tile_mode) {
-                dv[h] = src.d[tile * 256 + p];
-                gv[h] = src.gamma[tile * 256 + p];
+                dvo[h] = src.d[tile * 256 + p];
+                gvo[h] = src.gamma[tile * 256 + p];
             } else {
                 const float* sd = src.d;
                 const float* sgam = src.gamma;
@@ -299,39 +317,46 @@ __global__ void __launch_bounds__(kThreads, 2)
                 const int ti = rem / ty, tj = rem - ti * ty;
                 const int yy = clampi(tile_origin(ti, H) + r - 1, 0, H - 1);
                 const int xx = clampi(tile_origin(tj, W) + c - 1, 0, W - 1);
-                dv[h] = sd[(long long)f * H * W + (long long)yy * W + xx];
-                gv[h] = sgam[(long long)f * gstride + (long long)yy * W + xx];
+                dvo[h] = sd[(long long)f * H * W + (long long)yy * W + xx];
+                gvo[h] = sgam[(long long)f * gstride + (long long)yy * W + xx];
             }
         }
     };
-    float dv[2] = {0.0f, 0.0f}, gv[2] = {0.0f, 0.0f};
-    if ((long long)blockIdx.x < src.n_tiles) gather(blockIdx.x, dv, gv);
 
-    for (long long tile = blockIdx.x; tile < src.n_tiles && alive; tile += gridDim.x) {
-        // ---- features, layer-1 im2col operand ----------------------------------
-        float s1 = dv[0] + dv[1], s2 = dv[0] * dv[0] + dv[1] * dv[1];
+    // features of slot sl's tile from the gathered pixels, and the layer-1
+    // im2col operand in the slot's activation buffer (whose previous reader,
+    // the slot's last layer, has completed)
+    auto build = [&](int sl) {
+        float* sD = reinterpret_cast<float*>(sm + kOffTile + sl * kTileBytes);
+        float* sG = sD + 256;
+        float* sX0 = sG + 256;
+        float* sX1 = sX0 + 256;
+        float s1 = dv[sl][0] + dv[sl][1], s2 = dv[sl][0] * dv[sl][0] + dv[sl][1] * dv[sl][1];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             s1 += __shfl_xor_sync(0xffffffffu, s1, o);
             s2 += __shfl_xor_sync(0xffffffffu, s2, o);
         }
+        __syncthreads();  // earlier readers of red and of this slot's tile data are done
         if ((t & 31) == 0) {
             red[warp] = s1;
             red[4 + warp] = s2;
         }
-        __syncthreads();  // also: the previous tile's readers of sD / sX are done
+        __syncthreads();
         const float mu = (red[0] + red[1] + red[2] + red[3]) * (1.0f / 256.0f);
         const float sd = sqrtf(fmaxf((red[4] + red[5] + red[6] + red[7]) * (1.0f / 256.0f) -
                                      mu * mu, 0.0f)) + 1.0f;
+        scale_s[sl] = sd;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int p = t + 128 * h;
-            sD[p] = dv[h];
-            sG[p] = gv[h];
-            sX0[p] = (dv[h] - mu) / sd;
-            sX1[p] = sqrtf(fmaxf(dv[h], 0.0f) + fmaxf(gv[h], 0.0f)) / sd;
+            sD[p] = dv[sl][h];
+            sG[p] = gv[sl][h];
+            sX0[p] = (dv[sl][h] - mu) / sd;
+            sX1[p] = sqrtf(fmaxf(dv[sl][h], 0.0f) + fmaxf(gv[sl][h], 0.0f)) / sd;
         }
         __syncthreads();
+        unsigned char* im2col = sm + kOffAct + sl * kActBytes + kIm2colPos * 16;
 #pragma unroll 1
         for (int m = 0; m < 3; ++m) {
             const int q = 128 * m + t, P = q + kPlane;
@@ -349,98 +374,141 @@ __global__ void __launch_bounds__(kThreads, 2)
             for (int k = 18; k < 32; ++k) v[k] = 0.0f;
             store_pos(im2col, kChunkA, q, v);
         }
+    };
 
-        // the next tile's pixels load while this tile's layers run
-        float ndv[2] = {0.0f, 0.0f}, ngv[2] = {0.0f, 0.0f};
-        if (tile + gridDim.x < src.n_tiles) gather(tile + gridDim.x, ndv, ngv);
-
-        // ---- the four layers ---------------------------------------------------
-        int cur = 0;  // activation buffer holding the current layer's input
-        for (int layer = 0; layer < 4 && alive; ++layer) {
-            fence_async_smem();
-            fence_before();
-            __syncthreads();
-            if (t == 0) {
-                // descriptors are built once per layer; an operand offset is
-                // added to the start-address field (shared addresses < 256 KB,
-                // so the 14-bit field never carries)
-                fence_after();
-                if (layer == 0) {
-                    const uint32_t id = idesc(128, 32);
-                    const uint64_t a0 = sdesc(im_a, kChunkA, 128), b0 = sdesc(sW1a, 512, 128);
-                    for (int m = 0; m < 3; ++m)
-                        for (int ks = 0; ks < 2; ++ks)
-                            mma(tmem + m * 32, a0 + (((2 * ks) * kChunkA + 128 * m * 16) >> 4),
-                                b0 + (((2 * ks) * 512) >> 4), id, ks);
-                } else {
-                    const bool last = layer == 3;
-                    const uint32_t id = last ? idesc(128, 16) : idesc(128, 32);
-                    const uint32_t wa = layer == 1 ? sW2a : (layer == 2 ? sW3a : sW4a);
-                    const int tap_bytes = last ? kW4tapBytes : kWtapBytes;
-                    const int wchunk = last ? 256 : 512;
-                    const uint64_t a0 = sdesc(act_a[cur], kChunkA, 128);
-                    const uint64_t b0 = sdesc(wa, wchunk, 128);
-                    for (int m = 0; m < 3; ++m)
-                        for (int tap = 0; tap < 9; ++tap)
-                            for (int ks = 0; ks < 2; ++ks) {
-                                const int pos = kPlane + 128 * m + (tap / 3 - 1) * kPlane +
-                                                (tap % 3 - 1) + 1;
-                                mma(tmem + m * (last ? 16 : 32),
-                                    a0 + (((2 * ks) * kChunkA + pos * 16) >> 4),
-                                    b0 + ((tap * tap_bytes + (2 * ks) * wchunk) >> 4), id,
-                                    (tap | ks) != 0);
-                            }
-                }
-                commit(bar_a);
+    // make the slot's operand writes visible to the tensor core, then thread
+    // 0 issues the layer's MMAs and commits them to the slot's mbarrier
+    auto issue = [&](int sl, int layer) {
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        if (t == 0) {
+            // descriptors are built once per layer; an operand offset is added
+            // to the start-address field (shared addresses < 256 KB, so the
+            // 14-bit field never carries)
+            fence_after();
+            const uint32_t act_a = smem_u32(sm + kOffAct + sl * kActBytes);
+            const uint32_t td = tmem + (uint32_t)(sl * 128);
+            if (layer == 0) {
+                constexpr uint32_t id = idesc(128, 32);
+                const uint64_t a0 = sdesc(act_a + kIm2colPos * 16, kChunkA, 128);
+                const uint64_t b0 = sdesc(sW1a, 512, 128);
+#pragma unroll
+                for (int m = 0; m < 3; ++m)
+#pragma unroll
+                    for (int ks = 0; ks < 2; ++ks)
+                        mma(td + m * 32, a0 + (((2 * ks) * kChunkA + 128 * m * 16) >> 4),
+                            b0 + (((2 * ks) * 512) >> 4), id, ks);
+            } else if (layer < 3) {
+                issue_taps<32>(td, sdesc(act_a, kChunkA, 128),
+                               sdesc(layer == 1 ? sW2a : sW3a, 512, 128));
+            } else {
+                issue_taps<16>(td, sdesc(act_a, kChunkA, 128), sdesc(sW4a, 256, 128));
             }
-            if (!sync_mma()) {
+            commit(smem_u32(&bar[sl]));
+        }
+    };
+
+    // all threads: wait for the slot's committed MMAs (block-uniform outcome;
+    // on a timeout the phase stays, so the drain below waits on the same one)
+    auto sync_mma = [&](int sl) -> bool {
+        const bool ok = wait_bounded(smem_u32(&bar[sl]), phase_s[sl]);
+        const bool all = __syncthreads_and(ok) != 0;
+        if (all) phase_s[sl] ^= 1u;
+        fence_after();
+        return all;
+    };
+
+    // epilogue of slot sl's layer: this thread's accumulator row of each M block
+    auto epilogue = [&](int sl, int layer) {
+        const uint32_t td = tmem + lane_off + (uint32_t)(sl * 128);
+        if (layer < 3) {
+            const float* bias = sBias + 32 * layer;
+            unsigned char* dst = sm + kOffAct + sl * kActBytes;  // in place
+#pragma unroll 1
+            for (int m = 0; m < 3; ++m) {
+                const int q = 128 * m + t, P = q + kPlane;
+                const int R = P / kPlane, Cc = P - R * kPlane;
+                const bool valid = q < 288 && Cc >= 1 && Cc <= 16;
+                float v[32];
+                tmem_ld32(td + m * 32, v);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) v[i] = valid ? fmaxf(v[i] + bias[i], 0.0f) : 0.0f;
+                store_pos(dst, kChunkA, P + 1, v);
+            }
+        } else {
+            const float* sD = reinterpret_cast<const float*>(sm + kOffTile + sl * kTileBytes);
+            const float* sG = sD + 256;
+            const long long tile = tile_s[sl];
+            const float sd = scale_s[sl];
+#pragma unroll 1
+            for (int m = 0; m < 3; ++m) {
+                const int q = 128 * m + t, P = q + kPlane;
+                const int R = P / kPlane, Cc = P - R * kPlane;
+                float v[32];
+                tmem_ld32(td + m * 16, v);  // columns 0..15 used (+16 unused)
+                if (q < 288 && Cc >= 1 && Cc <= 16) {
+                    const int px = (R - 1) * 16 + (Cc - 1);
+                    const float y = v[0] + sBias[96];
+                    const float d = sD[px], g = sG[px];
+                    const float lo = kStartFrac * fmaxf(d + g, 1e-3f) - g;
+                    u0[tile * 256 + px] = fmaxf(fmaf(sd, y, d), lo);
+                }
+            }
+        }
+    };
+
+    // ---- start: each slot's first tile -------------------------------------
+#pragma unroll
+    for (int sl = 0; sl < kSlots; ++sl) {
+        tile_s[sl] = (long long)blockIdx.x + (long long)sl * gridDim.x;
+        scale_s[sl] = 1.0f;
+        if (tile_s[sl] < src.n_tiles) gather(tile_s[sl], dv[sl], gv[sl]);
+    }
+#pragma unroll
+    for (int sl = 0; sl < kSlots; ++sl) {
+        if (tile_s[sl] >= src.n_tiles) continue;
+        build(sl);
+        issue(sl, 0);
+        if (tile_s[sl] + stride < src.n_tiles) gather(tile_s[sl] + stride, dv[sl], gv[sl]);
+    }
+
+    // ---- alternate between the slots until both run out of tiles ------------
+    for (;;) {
+        bool any = false;
+#pragma unroll
+        for (int sl = 0; sl < kSlots; ++sl) {
+            if (!alive || tile_s[sl] >= src.n_tiles) continue;
+            any = true;
+            if (!sync_mma(sl)) {
                 alive = false;
                 break;
             }
-            // ---- epilogue: this thread's accumulator row of each M block ---------
-            if (layer < 3) {
-                const float* bias = sBias + 32 * layer;
-                unsigned char* dst = act[layer == 0 ? 0 : cur ^ 1];
-#pragma unroll 1
-                for (int m = 0; m < 3; ++m) {
-                    const int q = 128 * m + t, P = q + kPlane;
-                    const int R = P / kPlane, Cc = P - R * kPlane;
-                    const bool valid = q < 288 && Cc >= 1 && Cc <= 16;
-                    float v[32];
-                    tmem_ld32(tmem + lane_off + m * 32, v);
-#pragma unroll
-                    for (int i = 0; i < 32; ++i) v[i] = valid ? fmaxf(v[i] + bias[i], 0.0f) : 0.0f;
-                    store_pos(dst, kChunkA, P + 1, v);
-                }
-                cur = layer == 0 ? 0 : cur ^ 1;
+            epilogue(sl, layer_s[sl]);
+            if (layer_s[sl] < 3) {
+                ++layer_s[sl];
+                issue(sl, layer_s[sl]);
             } else {
-#pragma unroll 1
-                for (int m = 0; m < 3; ++m) {
-                    const int q = 128 * m + t, P = q + kPlane;
-                    const int R = P / kPlane, Cc = P - R * kPlane;
-                    float v[32];
-                    tmem_ld32(tmem + lane_off + m * 16, v);  // columns 0..15 used (+16 unused)
-                    if (q < 288 && Cc >= 1 && Cc <= 16) {
-                        const int px = (R - 1) * 16 + (Cc - 1);
-                        const float y = v[0] + sBias[96];
-                        const float d = sD[px], g = sG[px];
-                        const float lo = kStartFrac * fmaxf(d + g, 1e-3f) - g;
-                        u0[tile * 256 + px] = fmaxf(fmaf(sd, y, d), lo);
-                    }
+                // tile done: its successor's pixels were gathered during its layers
+                tile_s[sl] += stride;
+                layer_s[sl] = 0;
+                if (tile_s[sl] < src.n_tiles) {
+                    build(sl);
+                    issue(sl, 0);
+                    if (tile_s[sl] + stride < src.n_tiles)
+                        gather(tile_s[sl] + stride, dv[sl], gv[sl]);
                 }
             }
         }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            dv[h] = ndv[h];
-            gv[h] = ngv[h];
-        }
+        if (!any || !alive) break;
     }
 
     if (!alive) {
         if (t == 0 && status) atomicExch(status, 1);
-        // drain: give the outstanding MMAs a bounded time to complete
-        wait_bounded(bar_a, phase);
+        // drain: give every slot's outstanding MMAs a bounded time to complete
+#pragma unroll
+        for (int sl = 0; sl < kSlots; ++sl)
+            if (tile_s[sl] < src.n_tiles) wait_bounded(smem_u32(&bar[sl]), phase_s[sl]);
     }
     fence_before();
     __syncthreads();
@@ -470,7 +538,7 @@ int launch(const Src& src, const float* params, float* u0, int32_t* status, cuda
     int per_sm = per_sm_bytes / (kSmemBytes + 1024 + reserved);  // + static shared memory
     per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
     long long grid = (long long)sms * per_sm;
-    if (grid > src.n_tiles) grid = src.n_tiles;
+    if (grid > (src.n_tiles + kSlots - 1) / kSlots) grid = (src.n_tiles + kSlots - 1) / kSlots;
     infer_tc<<<(unsigned)grid, kThreads, kSmemBytes, s>>>(src, params, u0, status);
     return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
 }
@@ -488,7 +556,8 @@ int launch_batch(const float* params, const StackDesc* stacks, int n_stacks, lon
 }
 
 static_assert(2 * (kSmemBytes + 2048) <= 228 * 1024, "two CTAs per SM");
-static_assert(kOffAct0 % 1024 == 0 && kOffAct1 % 16 == 0, "alignment");
+static_assert(2 * kTmemCols <= 512, "two CTAs' tensor memory fits an SM");
+static_assert(kOffAct % 16 == 0 && kActBytes % 16 == 0 && kOffTile % 16 == 0, "alignment");
 static_assert(kIm2colPos + kQ <= kPos - 21, "im2col rows stay inside the rewritten range");
 
 }  // namespace nettc

@@ -68,6 +68,35 @@ def test_tiles_vs_fp64_optimum_and_reference(ncs, oracle_libs, mode):
         assert (numpy.abs(u[i] - uref) / numpy.maximum(numpy.abs(uref), 1.0)).max() <= 1e-3
 
 
+@pytest.mark.parametrize("alpha", [0.0, 1e-3, 2.0, 10.0])
+def test_alpha_range_vs_fp64_optimum(ncs, mode, alpha):
+    """alpha from 0 (pure likelihood: the optimum is u = d) to 10 (noise term
+    dominant), on bright tiles and on dark tiles with hot pixels: every tile
+    within 1e-4 relative cost of the FP64 Newton optimum (the north-star
+    tolerance), none stopped by the iteration cap."""
+    from oracle import numpy_ref as nr
+    rng = numpy.random.default_rng(21)
+    bright, gb = tiles_seed1(16)
+    dark = rng.uniform(0.2, 3.0, size=(16, 16, 16)).astype(numpy.float32)
+    dark[:, 5, 7] = 400.0  # a hot pixel per tile
+    gd = rng.uniform(0.5, 40.0, size=(16, 16, 16)).astype(numpy.float32)
+    data, gamma = numpy.concatenate([bright, dark]), numpy.concatenate([gb, gd])
+    ms = create_otf_mask_shifted()
+    s = ncs.Solver(alpha=alpha, max_iters=2000, mode=mode)
+    s.set_otf_mask_shifted(ms)
+    u, iters, status, cost = s.solve_tiles(torch.from_numpy(data).cuda(),
+                                           torch.from_numpy(gamma).cuda())
+    status = status.cpu().numpy()
+    assert (status != -2).all(), status
+    _, fstar, _ = nr.newton_solve(data, gamma, ms.astype(numpy.float64), alpha)
+    f = nr.cost(u.cpu().numpy().astype(numpy.float64), data.astype(numpy.float64),
+                gamma.astype(numpy.float64), ms.astype(numpy.float64), alpha)
+    assert nr.rel_cost_gap(f, fstar).max() <= 1e-4
+    if alpha == 0.0:
+        # no noise term: each pixel's optimum is its data value
+        assert numpy.abs(u.cpu().numpy() - data).max() <= 1e-3 * max(1.0, data.max())
+
+
 def test_matches_pycncs_on_photon_like_tiles(ncs, oracle_libs, mode):
     """GPU vs the pyCNCS C path on bright photon-like tiles (alpha 0.2).
 

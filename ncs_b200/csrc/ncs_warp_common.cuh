@@ -197,8 +197,10 @@ __device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8]
 }
 
 // Column stage of the inverse: from a spectrum in the layout warp_fft_fwd
-// leaves, fb[r][KC] = the row spectrum (horizontal frequency KC) of spatial
-// row r, for all 16 rows.
+// leaves, the even-frequency (H = 0) and twiddled odd-frequency (H = 1)
+// halves of every column's inverse: fb[r][KC] = E_r and fb[r + 8][KC] = O_r,
+// r = 0..7, so that row r of the row spectra is E_r + O_r and row r + 8 is
+// E_r - O_r.  The reader combines them, which costs no shuffles.
 __device__ __forceinline__ void warp_ifft_cols(float2 (&e)[8], WarpSmem& ws, const LaneGeo& L) {
     fft8_inv(e);
 #pragma unroll
@@ -206,16 +208,9 @@ __device__ __forceinline__ void warp_ifft_cols(float2 (&e)[8], WarpSmem& ws, con
         const float2 w = w16(r);
         e[r] = L.H ? conjmul(e[r], w) : e[r];
     }
-    float2 out[8];
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const float2 q = shfl_xor2(e[r], 1);
-        // H = 0: rows r = e + q ; H = 1: rows r + 8 = q - e
-        out[r] = make_float2(fmaf(L.sH, e[r].x, q.x), fmaf(L.sH, e[r].y, q.y));
-    }
     __syncwarp();  // every lane has read the row spectra
 #pragma unroll
-    for (int r = 0; r < 8; ++r) ws.fb[r + 8 * L.H][L.KC] = out[r];
+    for (int r = 0; r < 8; ++r) ws.fb[r + 8 * L.H][L.KC] = e[r];
     __syncwarp();
 }
 
@@ -255,7 +250,9 @@ __device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float (&y)[8], Warp
     float2 V[4], z[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const float2 a = ws.fb[L.P][L.k0 + k], b = ws.fb[L.P + 8][L.k0 + k];
+        // rows P = E + O and P + 8 = E - O, packed as one complex row
+        const float2 ev = ws.fb[L.P][L.k0 + k], od = ws.fb[L.P + 8][L.k0 + k];
+        const float2 a = ev + od, b = ev - od;
         V[k] = make_float2(a.x - b.y, a.y + b.x);
     }
     warp_ifft_row(V, z, L);

@@ -285,3 +285,26 @@ def test_host_pipeline_equals_device_solve(ncs, mode):
     assert torch.equal(s.reduce_noise_host(big, gbig, chunk_frames=1), ref)
     with pytest.raises(ValueError):
         s.reduce_noise_host(images, gamma[:10])
+
+
+def test_host_entry_with_pageable_numpy(ncs):
+    """ncsb_reduce_noise_host called through the C ABI on pageable (not
+    page-locked) numpy arrays, as a reference-side ctypes binding would: the
+    driver stages the copies, and the result equals the device solve."""
+    import ctypes
+    rng = numpy.random.default_rng(12)
+    T, H, W = 9, 33, 61
+    images = rng.uniform(1.0, 90.0, size=(T, H, W)).astype(numpy.float32)
+    for g in (rng.uniform(1.0, 20.0, size=(H, W)).astype(numpy.float32),
+              rng.uniform(1.0, 20.0, size=(T, H, W)).astype(numpy.float32)):
+        s = ncs.Solver(alpha=0.2, max_iters=30)
+        s.set_otf_mask_shifted(create_otf_mask_shifted())
+        ref = s.reduce_noise(torch.from_numpy(images).cuda(), torch.from_numpy(g).cuda()).cpu()
+        out = numpy.full_like(images, numpy.nan)
+        rc = s.lib.ncsb_reduce_noise_host(
+            s._handle, images.ctypes.data_as(ctypes.c_void_p), T, H, W,
+            g.ctypes.data_as(ctypes.c_void_p), int(g.ndim == 3),
+            out.ctypes.data_as(ctypes.c_void_p), 2, 3, ctypes.c_void_p(0))
+        assert rc == 0
+        assert numpy.array_equal(out, ref.numpy())
+        s.close()

@@ -317,27 +317,29 @@ class Solver:
         (``ncsb_reduce_noise_host``).
 
         ``images`` [T, H, W] and ``gamma`` [H, W] or [T, H, W] are float32 CPU
-        tensors or numpy arrays, page-locked here if they are not already.
-        The library cuts the stack into chunks (``chunk_frames`` frames,
-        default T / 40, at most 64 MB); chunk i is copied in, solved and
-        copied out on stream i % ``n_streams`` (default 4), so both directions
-        of the host link and the solve run at once.  Returns the pinned
-        [T, H, W] result, bit-identical to ``reduce_noise``."""
-        def pinned(x):
+        tensors or numpy arrays.  The library cuts the stack into chunks
+        (``chunk_frames`` frames, default T / 40, at most 64 MB); chunk i is
+        copied in, solved and copied out on stream i % ``n_streams`` (default
+        4), so both directions of the host link and the solve run at once.
+        Page-locked inputs and ``out`` (``tensor.pin_memory()``, allocated once
+        and reused) give that overlap; pageable memory is accepted as it is
+        (the driver stages its copies, which is slower but avoids locking a
+        copy of the stack on every call).  Returns ``out`` (by default a new
+        float32 CPU tensor), bit-identical to ``reduce_noise``."""
+        def host(x):
             t = x if isinstance(x, torch.Tensor) else torch.from_numpy(numpy.asarray(x))
             if t.device.type != "cpu":
                 raise TypeError("reduce_noise_host takes host arrays")
             if t.dtype != torch.float32:
                 t = t.float()
-            t = t.contiguous()
-            return t if t.is_pinned() else t.pin_memory()
-        h_in = pinned(images)
+            return t.contiguous()
+        h_in = host(images)
         if h_in.dim() == 2:
             h_in = h_in.unsqueeze(0)
         if h_in.dim() != 3:
             raise ValueError("images must be [T, H, W] or [H, W]")
         T, H, W = h_in.shape
-        h_g = pinned(gamma)
+        h_g = host(gamma)
         if tuple(h_g.shape) == (H, W):
             per_frame = 0
         elif tuple(h_g.shape) == (T, H, W):
@@ -345,7 +347,7 @@ class Solver:
         else:
             raise ValueError("gamma must be [H, W] or [T, H, W]")
         if out is None:
-            out = torch.empty((T, H, W), dtype=torch.float32).pin_memory()
+            out = torch.empty((T, H, W), dtype=torch.float32)
         elif (out.device.type != "cpu" or out.dtype != torch.float32
               or tuple(out.shape) != (T, H, W) or not out.is_contiguous()):
             raise ValueError("out must be a contiguous float32 host tensor [T, H, W]")

@@ -58,6 +58,13 @@ struct HostPipe {
     cudaEvent_t start = nullptr, gamma_in = nullptr, done[kMaxStreams] = {};
 };
 
+// Wait for everything queued on the pipeline's streams (before its buffers
+// are freed or resized, and when a call stops early on an error).
+void sync_pipe(HostPipe* q) {
+    for (cudaStream_t st : q->st)
+        if (st) cudaStreamSynchronize(st);
+}
+
 void free_buffers(HostPipe* q) {
     for (int b = 0; b < HostPipe::kMaxStreams; ++b) {
         cudaFree(q->d_in[b]);
@@ -72,8 +79,7 @@ void free_buffers(HostPipe* q) {
 
 void destroy_pipe(HostPipe* q) {
     if (!q) return;
-    for (cudaStream_t st : q->st)
-        if (st) cudaStreamSynchronize(st);
+    sync_pipe(q);
     free_buffers(q);
     cudaFree(q->d_gamma);
     cudaFree(q->d_queues);
@@ -330,7 +336,7 @@ cudaError_t prepare_pipe(ncsb_handle* h, int n, size_t chunk_px, size_t gamma_px
     }
     HostPipe* q = h->pipe;
     if (q->n != n || q->chunk_px < chunk_px || (per_frame && !q->per_frame)) {
-        // the previous call has finished: every call waits for all its streams
+        sync_pipe(q);  // a call that stopped on an error may have left work queued
         free_buffers(q);
         const size_t bytes = chunk_px * sizeof(float);
         for (int k = 0; k < n; ++k) {
@@ -347,6 +353,7 @@ cudaError_t prepare_pipe(ncsb_handle* h, int n, size_t chunk_px, size_t gamma_px
         q->per_frame = per_frame;
     }
     if (!per_frame && q->gamma_px < gamma_px) {
+        sync_pipe(q);
         cudaFree(q->d_gamma);
         q->d_gamma = nullptr;
         q->gamma_px = 0;
@@ -410,7 +417,10 @@ int ncsb_reduce_noise_host(ncsb_handle* h, const float* images, int n_frames, in
         if (e == cudaSuccess && gamma_per_frame)
             e = cudaMemcpyAsync(q->d_gf[k], gamma + (size_t)f0 * frame_px, (size_t)n * fb,
                                 cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline copy in");
+        if (e != cudaSuccess) {
+            sync_pipe(q);
+            return cuda_fail(h, e, "host pipeline copy in");
+        }
         ncsb::SolveArgs a{};
         a.tile_mode = 0;
         a.data = q->d_in[k];
@@ -424,10 +434,16 @@ int ncsb_reduce_noise_host(ncsb_handle* h, const float* images, int n_frames, in
         a.tiles_y = tiles_along(width);
         a.n_tiles = (long long)n * a.tiles_x * a.tiles_y;
         const int rc = launch(h, a, st, q->d_queues + k);
-        if (rc != NCSB_OK) return rc;
+        if (rc != NCSB_OK) {
+            sync_pipe(q);
+            return rc;
+        }
         e = cudaMemcpyAsync(out + (size_t)f0 * frame_px, q->d_out[k], (size_t)n * fb,
                             cudaMemcpyDeviceToHost, st);
-        if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline copy out");
+        if (e != cudaSuccess) {
+            sync_pipe(q);
+            return cuda_fail(h, e, "host pipeline copy out");
+        }
     }
     // the caller's stream, and this call's return, wait for every stream
     for (int k = 0; k < n_streams && e == cudaSuccess; ++k) {

@@ -12,10 +12,12 @@ no flush is needed between steps.
 
 Prints one JSON line.  ``value`` is Mpixel/s of the whole job (all ranks) with
 the stack resident in HBM, timed with CUDA events; ``e2e`` is the same metric
-through the public ``Solver.reduce_noise_host`` API from pinned host memory
-(every step copies the stack in, solves it and copies it out; frame chunks on
-three streams overlap the copies with the solve).  Under torchrun each rank solves its own stack
-(replicas by frame, weak scaling, no collective in the data path); the time
+through the public ``Solver.reduce_noise_host`` API (the C entry
+ncsb_reduce_noise_host) from pinned host memory: every step copies the stack
+in, solves it and copies it out, in frame chunks round-robin over four
+streams so that the copies overlap the solve.  Under torchrun each rank solves
+its own stack (replicas by frame, weak scaling, no collective in the data
+path); the time
 is the max over ranks.  ``--impl reference`` times the reference's own CPU
 path (pyCNCS ncs.c compiled by oracle/Makefile, else the oracle's C port) on
 all host cores instead.

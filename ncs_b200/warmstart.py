@@ -5,7 +5,7 @@ after the first three layers, 19,393 FP32 parameters) maps each 16x16 tile's
 photon image d and gamma map to a proposed start u0 for the L-BFGS solve; the
 solver (``Solver.reduce_noise_from``) starts each tile at the proposal unless
 the proposal's cost is higher than the photon image's, so the unchanged
-stopping rule and the plain start remain the judge and the fallback.  The
+stopping rule decides convergence and the plain start is the fallback.  The
 reference has no learned part: its solves always start at u = d
 (clib/pyCNCS/ncs.c:548-551, cuda/ncs.cu:933).
 

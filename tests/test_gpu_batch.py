@@ -137,6 +137,41 @@ def test_batch_tensor_core_proposals_equal_per_stack(ncs, stacks):
     assert torch.equal(u0, torch.cat(per))
 
 
+def test_warm_batch_replays_from_a_cuda_graph(ncs, stacks):
+    """Tensor-core proposals over the batch and the batched solve from them,
+    captured together in one CUDA graph (the mixed workload's launch), replay
+    bit for bit like the eager calls."""
+    from ncs_b200 import warmstart
+    net = warmstart.WarmStartNet.load()
+    s = ncs.Solver()
+    outs = s.batch_set(stacks)
+    u0 = torch.empty((s.batch_tiles, 16, 16), dtype=torch.float32, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stats = s.batch_stats()
+    net.propose_batch_tc(s, out=u0, status=st)
+    s.batch_reduce_noise(u0_tiles=u0, stats=stats)
+    torch.cuda.synchronize()
+    ref_u0, ref = u0.clone(), [o.clone() for o in outs]
+    ref_it, ref_start = stats["iters"].clone(), stats["start"].clone()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        net.propose_batch_tc(s, out=u0, status=st)
+        s.batch_reduce_noise(u0_tiles=u0, stats=stats)
+    for _ in range(2):
+        u0.zero_()
+        for o in outs:
+            o.zero_()
+        stats["iters"].zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        assert int(st.item()) == 0
+        assert torch.equal(u0, ref_u0)
+        for o, r in zip(outs, ref):
+            assert torch.equal(o, r)
+        assert torch.equal(stats["iters"], ref_it) and torch.equal(stats["start"], ref_start)
+    del graph
+
+
 def test_batch_launch_replays_from_a_cuda_graph(ncs, stacks):
     s = ncs.Solver()
     outs = s.batch_set(stacks)

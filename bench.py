@@ -56,6 +56,13 @@ FLOP_TRIAL = 2048
 FLOP_ITER_BASE = {"plain": 11264 + 1536 + 2304 + 2048, "plain_wg": 11264 + 1536 + 2304 + 2048,
                   "spectral": 11776 + 1536 + 2816 + 2048}
 FLOP_PER_PAIR = {"plain": 4 * 256 * 2, "plain_wg": 4 * 256 * 2, "spectral": 5 * 256 * 2}
+# Warp instructions per solver pass (one iteration or the initial gradient),
+# from the kernels' ncu captures on stack512 at 64 frames (profiles/*.md):
+# executed warp instructions / (tiles x passes).  Used for the issue-rate
+# bound, the one that limits these kernels.
+WARP_INST_PER_PASS = {"spectral": 674715776 / (87616 * 6.0483),
+                      "plain": 2546982558 / (87616 * 15.5539),
+                      "plain_wg": 7479161369 / (87616 * 15.5538)}
 # multiply-adds x 2 of the warm-start network per 16x16 tile:
 # 256 px x 9 taps x (2*32 + 32*32 + 32*32 + 32*1)
 INFER_FLOP_PER_TILE = 2 * 256 * 9 * (2 * 32 + 32 * 32 + 32 * 32 + 32 * 1)
@@ -492,6 +499,8 @@ def run_ours(args, world, rank, local):
     n_sms = torch.cuda.get_device_properties(dev).multi_processor_count
     fp32_peak = fp32_peak_tflops(pk.get("sm_max_mhz", 1965.0), n_sms)
     launch_ms = statistics.mean(per_step)
+    inst_launch = WARP_INST_PER_PASS[args.form] * (iters_n + n_tiles)
+    issue_peak = n_sms * 4 * pk.get("sm_max_mhz", 1965.0) * 1e6
     achieved = flops / (launch_ms / 1e3) / 1e12
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
@@ -519,7 +528,14 @@ def run_ours(args, world, rank, local):
                      "flops_per_launch": flops,
                      "hbm": {"algorithmic_bytes": alg_bytes,
                              "achieved_gbs": alg_bytes / (launch_ms / 1e3) / 1e9,
-                             "peak_gbs": pk.get("hbm_gbs")}},
+                             "peak_gbs": pk.get("hbm_gbs")},
+                     "issue": {"est_warp_inst_per_launch": inst_launch,
+                               "achieved_warp_inst_per_s": inst_launch / (launch_ms / 1e3),
+                               "peak_warp_inst_per_s": issue_peak,
+                               "frac": inst_launch / (launch_ms / 1e3) / issue_peak,
+                               "source": "warp instructions per pass from the kernel's ncu "
+                                         "capture (profiles/) x passes counted in this run; "
+                                         "peak = SMs x 4 schedulers x sm_max_mhz"}},
         "e2e": {"value": e2e_value, "unit": "Mpixel/s",
                 "h2d_bytes_per_step": int(h_in.numel() * 4 + h_gamma.numel() * 4),
                 "d2h_bytes_per_step": int(h_out.numel() * 4),

@@ -755,6 +755,118 @@ def run_mixed(args, world, rank, local):
     return 0
 
 
+def run_normalized(args, world, rank, local):
+    """The normalised single-pixel variant (the reference's MATLAB package,
+    ncsb_reduce_noise_normalized) on the stack512 stack with its demos'
+    settings: alpha 1, 15 iterations, the 3 x 3 genfilter mask of twice the
+    NA.  One launch per step (one thread per pixel); replicas by frame."""
+    import ncs_b200
+    from ncs_b200 import otf, sim
+    from oracle import normalized_ref as nref
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = sim.make_stack("stack512", T=args.frames, device=dev, seed=1234 + rank)
+    images, gamma = w["images"], w["gamma"]
+    T, H, W = images.shape
+    mask = otf.normalized_mask(0.1, 1.4, 0.7)
+    alpha, cap = 1.0, 15
+    out, it, st, cost = ncs_b200.reduce_noise_normalized(images, gamma, mask, alpha=alpha,
+                                                         max_iters=cap, stats=True)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        ncs_b200.reduce_noise_normalized(images, gamma, mask, alpha=alpha, max_iters=cap)
+    stream = torch.cuda.current_stream(dev)
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.begin()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ncs_b200.reduce_noise_normalized(images, gamma, mask, alpha=alpha, max_iters=cap)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks.end()
+    barrier(world)
+    clk = clocks.stop()
+    total_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    px = sum_over_ranks(float(T * H * W), world)
+    value = px * args.steps / (total_ms / 1e3) / 1e6
+
+    # end to end: pinned host stack in, solve, result out, on one stream
+    h_in = images.cpu().pin_memory()
+    h_g = gamma.cpu().pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    steps2 = max(1, min(args.steps, 5))
+    barrier(world)
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(steps2):
+        images.copy_(h_in, non_blocking=True)
+        gamma.copy_(h_g, non_blocking=True)
+        o = ncs_b200.reduce_noise_normalized(images, gamma, mask, alpha=alpha, max_iters=cap)
+        h_out.copy_(o, non_blocking=True)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
+
+    stv = st.cpu().numpy()
+    line = {
+        "metric": "Mpixel/s, normalised single-pixel NCS variant (3x3 segment per pixel)",
+        "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded WLC structure + sCMOS camera model)",
+        "config": {"workload": "normalized: stack512 (%d frames x %dx%d), alpha %.1f, BFGS cap "
+                               "%d, 3x3 genfilter mask of 2 NA (the reference demos' settings)"
+                               % (T, H, W, alpha, cap),
+                   "frames": T, "height": H, "width": W,
+                   "l2": "inputs+outputs %.0f MB > 126 MB L2, no flush" % (2 * T * H * W * 4 / 1e6),
+                   "parallelism": "replicas by frame (one stack per rank)"},
+        "mean_iters": float(it.double().mean().item()),  # per pixel
+        "status": {str(k): int((stv == k).sum()) for k in range(-5, 1) if (stv == k).any()},
+        "e2e": {"value": px * steps2 / (e2e_ms / 1e3) / 1e6, "unit": "Mpixel/s",
+                "h2d_bytes_per_step": int(h_in.numel() * 4 + h_g.numel() * 4),
+                "d2h_bytes_per_step": int(h_out.numel() * 4),
+                "api": "pinned copies + ncs_b200.reduce_noise_normalized, one stream"},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+    }
+    if rank == 0:
+        # accuracy: per-pixel final cost vs the FP64 Newton optimum of its segment
+        rng = numpy.random.default_rng(0)
+        n = T * H * W
+        idx = rng.choice(n, size=min(args.accuracy_tiles, n), replace=False)
+        im = images.cpu().numpy().astype(numpy.float64)
+        gm = gamma.cpu().numpy().astype(numpy.float64)
+        cst = cost.cpu().numpy().reshape(-1)
+        m64 = numpy.asarray(mask, dtype=numpy.float32).astype(numpy.float64)
+        gaps, t0 = [], time.time()
+        for k in idx:
+            f, rem = divmod(int(k), H * W)
+            y, x = divmod(rem, W)
+            ys = numpy.clip(numpy.arange(y - 1, y + 2), 0, H - 1)
+            xs = numpy.clip(numpy.arange(x - 1, x + 2), 0, W - 1)
+            _, fstar = nref.newton(im[f][numpy.ix_(ys, xs)], gm[numpy.ix_(ys, xs)], m64, alpha)
+            gaps.append((cst[k] - fstar) / max(abs(fstar), 1.0))
+        cpu_s = time.time() - t0
+        gaps = numpy.array(gaps)
+        line["accuracy"] = {"pixels_checked": int(idx.size),
+                            "frac_within_1e-4": float((gaps <= 1e-4).mean()),
+                            "max_rel_gap": float(gaps.max()),
+                            "median_rel_gap": float(numpy.median(gaps)),
+                            "referee": "FP64 damped Newton per segment "
+                                       "(oracle/normalized_ref.py), run to convergence"}
+        line["cpu_baseline"] = {"value": idx.size / cpu_s / 1e6, "unit": "Mpixel/s", "cores": 1,
+                                "kind": "port",
+                                "sample": "%d pixels, FP64 Newton per 3x3 segment in numpy (the "
+                                          "MATLAB fminunc reference cannot run here)" % idx.size}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -784,6 +896,8 @@ def main():
     try:
         if args.workload == "mixed":
             return run_mixed(args, world, rank, local)
+        if args.workload == "normalized":
+            return run_normalized(args, world, rank, local)
         return run_ours(args, world, rank, local)
     finally:
         if world > 1:

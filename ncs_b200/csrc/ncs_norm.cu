@@ -14,8 +14,10 @@
 // line search with the fraction-to-barrier rule of the main solver.  The
 // reference minimises with MATLAB's fminunc quasi-Newton; the stopping rule
 // here is fminunc's first-order optimality test, ||g||_inf <= tol *
-// max(1, ||g_0||_inf), with its iteration cap.  Q (9 x 9, symmetric) is built
-// on the host from the 3 x 3 centred mask and passed packed.
+// max(1, ||g_0||_inf), with its iteration cap.  Q (9 x 9, symmetric) is the
+// 3 x 3 circular convolution with the kernel qk = ifft2(M^2) / 9 (block
+// circulant with circulant blocks): Q[p][q] = qk[(p1 - q1) mod 3][(p2 - q2)
+// mod 3], so the kernel takes 9 values from the host instead of 45.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <stdint.h>
@@ -34,7 +36,7 @@ struct Args {
     long long gstride;
     float* out;
     int T, H, W;
-    double q[kPacked];
+    double qk[9];  // Q[p][q] = qk[((p/3 - q/3) mod 3) * 3 + (p%3 - q%3) mod 3]
     double alpha, tol, c1, min_step;
     int max_iters;
     int32_t* iters;
@@ -46,9 +48,6 @@ __host__ __device__ constexpr int pk(int i, int j) {  // packed index, i <= j
     return i * 9 - i * (i - 1) / 2 + (j - i);
 }
 
-__device__ __forceinline__ double qij(const Args& a, int i, int j) {
-    return i <= j ? a.q[pk(i, j)] : a.q[pk(j, i)];
-}
 
 // Per-thread constants of the segment in shared memory (c = d + gamma, gamma),
 // column t of each [9][kThreads] array.
@@ -69,7 +68,8 @@ __device__ double evaluate(const Args& a, const double (&u)[9], const Seg& sg, d
         S += u[i];
         double acc = 0.0;
 #pragma unroll
-        for (int j = 0; j < 9; ++j) acc = fma(qij(a, i, j), u[j], acc);
+        for (int j = 0; j < 9; ++j)
+            acc = fma(a.qk[((i / 3 - j / 3 + 3) % 3) * 3 + (i % 3 - j % 3 + 3) % 3], u[j], acc);
         Qu[i] = acc;
     }
     double P = 0.0;
@@ -170,14 +170,15 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
                 feas = feas && (un[i] + sg.G(i) >= 0.01 * (u[i] + sg.G(i)));
             }
             if (feas) {
-                fn = evaluate(a, un, sg, gn, false);
+                // with the gradient: nearly every first trial is accepted, and
+                // evaluating again after acceptance would repeat the logs and Q u
+                fn = evaluate(a, un, sg, gn, true);
                 if (fn <= fu + a.c1 * step * gd) { ok = true; break; }
             }
             step *= 0.5;
             if (!(step >= a.min_step)) break;
         }
         if (!ok) { status = NCSB_MINIMUM_STEP; break; }
-        fn = evaluate(a, un, sg, gn, true);
         // BFGS update of the inverse Hessian with s = un - u, y = gn - g
         double s[9], yv[9], sy = 0.0, yy = 0.0;
 #pragma unroll
@@ -260,14 +261,13 @@ int ncsb_reduce_noise_normalized(const float* images, int n_frames, int height, 
         for (int j = 0; j < 3; ++j) sym[i][j] = 0.5 * (mu[i][j] + mu[(3 - i) % 3][(3 - j) % 3]);
     Args a{};
     const double tw = 2.0 * 3.14159265358979323846 / 3.0;
-    for (int p = 0; p < 9; ++p)
-        for (int q = p; q < 9; ++q) {
-            const int p1 = p / 3, p2 = p % 3, q1 = q / 3, q2 = q % 3;
+    // qk[d1][d2] = Q[(d1, d2)][(0, 0)]; Re(e^{+i th_p} e^{-i th_q}) = cos(th_p - th_q)
+    for (int d1 = 0; d1 < 3; ++d1)
+        for (int d2 = 0; d2 < 3; ++d2) {
             double acc = 0.0;
             for (int k1 = 0; k1 < 3; ++k1)
-                for (int k2 = 0; k2 < 3; ++k2)  // Re(e^{+i th_p} e^{-i th_q}) = cos(th_p - th_q)
-                    acc += sym[k1][k2] * cos(tw * (k1 * (p1 - q1) + k2 * (p2 - q2)));
-            a.q[pk(p, q)] = acc / 9.0;
+                for (int k2 = 0; k2 < 3; ++k2) acc += sym[k1][k2] * cos(tw * (k1 * d1 + k2 * d2));
+            a.qk[d1 * 3 + d2] = acc / 9.0;
         }
     a.data = images;
     a.gamma = gamma;

@@ -175,15 +175,16 @@ int ncsb_reduce_noise_start(ncsb_handle *h, const float *images, int n_frames, i
                             int32_t *tile_status, double *tile_cost, int32_t *tile_evals,
                             int32_t *tile_start, void *stream);
 
-/* ---- raw camera frames: the preprocessing prologue fused into the solve ---
+/* ---- raw camera frames: the preprocessing prologue on the device -----------
  * The reference converts ADU to photo-electrons on the host before the solve
  * (python3-6/pyNCS/denoisetools.py:222-224, python3-6/NCSdemo_experiment.py:47-49:
  * d = (ADU - offset) / gain, d <= 0 -> 1e-6; gamma = var / gain^2,
  * denoisetools.py:266), and for cameras with several gain amplifiers picks
  * each pixel's gain and variance maps by its ADU level (matlab/genmaps.m:29-62:
  * level 0 below levels[0], level k for levels[k-1] <= ADU < levels[k], the
- * last level above the last threshold).  Here the solver's tile gather does
- * this per pixel, so neither d nor gamma is ever written to memory. */
+ * last level above the last threshold).  Here one device pass does this per
+ * pixel into a buffer the handle owns, and the solve reads it: the frames
+ * never return to the host between conversion and solve. */
 typedef struct {
     const float *offset;    /* device [height][width], ADU */
     const float *gain;      /* device [n_levels][height][width], ADU per photo-electron (> 0) */
@@ -194,7 +195,9 @@ typedef struct {
 
 /* ncsb_reduce_noise on raw ADU frames adu [n_frames][height][width] with the
  * camera calibration `cal` (host struct of device pointers).  out is in
- * photo-electrons, as ncsb_reduce_noise's.  Spectral form only. */
+ * photo-electrons, as ncsb_reduce_noise's.  Any solver form.  The handle
+ * allocates (and keeps, growing it when needed) a device buffer of
+ * n_frames x height x width floats, twice that with several map pairs. */
 int ncsb_reduce_noise_adu(ncsb_handle *h, const float *adu, int n_frames, int height, int width,
                           const ncsb_calibration *cal, float *out, int32_t *tile_iters,
                           int32_t *tile_status, double *tile_cost, int32_t *tile_evals,

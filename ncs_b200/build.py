@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libncs_b200.so")
 SOURCES = ["ncs_capi.cu", "ncs_plain.cu", "ncs_warp.cu", "ncs_spectral.cu", "ncs_noalloc.cu",
            "ncs_net.cu", "ncs_masks.cu", "ncs_sim.cu",
-           "ncs_norm.cu", "ncs_net_tc.cu"]
+           "ncs_norm.cu", "ncs_net_tc.cu", "ncs_adu.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

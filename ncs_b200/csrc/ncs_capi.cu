@@ -28,6 +28,10 @@ namespace net {
 int launch_infer_batch(const float* params, const StackDesc* stacks, int n_stacks,
                        long long n_tiles, float* u0, cudaStream_t s);
 }  // namespace net
+namespace adu {
+cudaError_t launch_convert(const float* adu, int T, int H, int W, const ncsb_calibration* cal,
+                           float* d, float* gamma, cudaStream_t s);
+}  // namespace adu
 namespace nettc {
 int launch_batch(const float* params, const StackDesc* stacks, int n_stacks, long long n_tiles,
                  float* u0, int32_t* status, cudaStream_t s);
@@ -109,6 +113,8 @@ struct ncsb_handle {
     int n_stacks = 0;
     long long batch_tiles = 0;
     HostPipe* pipe = nullptr;  // ncsb_reduce_noise_host
+    float* d_adu = nullptr;    // ncsb_reduce_noise_adu: converted frames, then gamma
+    size_t adu_px = 0;         // capacity of d_adu in floats
     std::string err;
 };
 
@@ -247,6 +253,7 @@ int ncsb_set_params(ncsb_handle* h, const ncsb_params* p) {
 int ncsb_destroy(ncsb_handle* h) {
     if (!h) return NCSB_EINVAL;
     destroy_pipe(h->pipe);
+    cudaFree(h->d_adu);
     cudaFree(h->d_msq);
     cudaFree(h->d_queue);
     cudaFree(h->d_stacks);
@@ -496,8 +503,6 @@ int ncsb_reduce_noise_adu(ncsb_handle* h, const float* adu, int n_frames, int he
                           int32_t* tile_status, double* tile_cost, int32_t* tile_evals,
                           void* stream) {
     if (!h) return NCSB_EINVAL;
-    if (h->p.mode != NCSB_MODE_SPECTRAL)
-        return fail(h, NCSB_EINVAL, "raw-ADU input needs the spectral form");
     if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
     if (!adu || !out || !cal || !cal->offset || !cal->gain || !cal->variance)
         return fail(h, NCSB_EINVAL, "null buffer");
@@ -511,10 +516,30 @@ int ncsb_reduce_noise_adu(ncsb_handle* h, const float* adu, int n_frames, int he
     if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
         return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
     if (n_frames == 0) return NCSB_OK;
+    // converted frames, then gamma (one map, or one per frame with several pairs)
+    const size_t frame_px = (size_t)height * width, stack_px = (size_t)n_frames * frame_px;
+    const bool multi = cal->n_levels > 1;
+    const size_t need = stack_px + (multi ? stack_px : frame_px);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (h->adu_px < need) {
+        // earlier calls on the handle (on any stream) may still read the old buffer
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaFree(h->d_adu);
+        h->d_adu = nullptr;
+        h->adu_px = 0;
+        if (e == cudaSuccess) e = cudaMalloc(&h->d_adu, need * sizeof(float));
+        if (e != cudaSuccess) return cuda_fail(h, e, "raw-ADU conversion buffer");
+        h->adu_px = need;
+    }
+    float* d = h->d_adu;
+    float* gam = h->d_adu + stack_px;
+    cudaError_t e = ncsb::adu::launch_convert(adu, n_frames, height, width, cal, d, gam, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "raw-ADU conversion");
     ncsb::SolveArgs a{};
     a.tile_mode = 0;
-    a.data = adu;
-    a.gamma = cal->variance;  // not read as gamma; kept non-null
+    a.data = d;
+    a.gamma = gam;
+    a.gamma_frame_stride = multi ? (long long)frame_px : 0;
     a.out = out;
     a.T = n_frames;
     a.H = height;
@@ -526,12 +551,7 @@ int ncsb_reduce_noise_adu(ncsb_handle* h, const float* adu, int n_frames, int he
     a.status = tile_status;
     a.cost = tile_cost;
     a.evals = tile_evals;
-    a.adu_offset = cal->offset;
-    a.adu_gain = cal->gain;
-    a.adu_var = cal->variance;
-    a.n_levels = cal->n_levels;
-    for (int q = 0; q < 3; ++q) a.levels[q] = cal->levels[q];
-    return launch(h, a, (cudaStream_t)stream);
+    return launch(h, a, s);
 }
 
 int ncsb_solve_tiles(ncsb_handle* h, const float* data_in, const float* gamma_in, const float* u0,

@@ -65,14 +65,6 @@ struct SolveArgs {
     const StackDesc* stacks;
     int n_stacks;
     const float* mk_lane;          // [n_stacks][256]
-    // raw-ADU input (the fused preprocessing prologue): data holds ADU counts;
-    // per pixel d = (ADU - offset) / gain (d <= 0 -> 1e-6), gamma = var / gain^2,
-    // with the gain / variance pair chosen by the pixel's ADU level
-    const float* adu_offset;       // [H][W]
-    const float* adu_gain;         // [n_levels][H][W]
-    const float* adu_var;          // [n_levels][H][W]
-    int n_levels;                  // 1..4
-    float levels[3];               // ascending ADU thresholds between the pairs
 };
 
 // ---- tile geometry (segmentation of ncs.c:66-113, shared by every kernel) ----

@@ -69,9 +69,8 @@ __device__ __forceinline__ Geo geo_of(const SolveArgs& a, const StackDesc& sd) {
 // Warm: the launch carries proposals (a.u0); the cold variant compiles
 // without the start passes.  Batch: tiles of several stacks (own alpha and
 // mask each, a.stacks) share one queue; a tile's stack is found by binary
-// search over the stacks' first tiles.  Adu: the stack holds raw ADU counts
-// and the gather applies the camera calibration (offset, gain, variance).
-template <int MinBlocks, int MaxM, bool Warm, bool Batch, bool Adu = false>
+// search over the stacks' first tiles.
+template <int MinBlocks, int MaxM, bool Warm, bool Batch>
 __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kernel(const SolveArgs a) {
     static_assert(MaxM >= 1 && MaxM <= kMaxM, "history capacity");
     extern __shared__ __align__(16) unsigned char dsm[];
@@ -155,23 +154,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int col = clampi(oy + G.Qd + 4 * j - 1, 0, sg.W - 1);
-                    if constexpr (Adu) {
-                        // denoisetools.py:222-224 and :266, genmaps.m:36-58
-                        const long long pix = row * sg.W + col;
-                        const float av = __ldg(img + pix);
-                        int lv = 0;
-#pragma unroll
-                        for (int q = 0; q < 3; ++q)
-                            lv += (q + 1 < a.n_levels && av >= a.levels[q]) ? 1 : 0;
-                        const long long at = (long long)lv * sg.H * sg.W + pix;
-                        const float gn = __ldg(a.adu_gain + at);
-                        const float dv = (av - __ldg(a.adu_offset + pix)) / gn;
-                        d[2 * j + s] = dv <= 0.0f ? 1.0e-6f : dv;
-                        gm[2 * j + s] = __ldg(a.adu_var + at) / (gn * gn);
-                    } else {
-                        d[2 * j + s] = __ldg(img + row * sg.W + col);
-                        gm[2 * j + s] = __ldg(gmap + row * sg.W + col);
-                    }
+                    d[2 * j + s] = __ldg(img + row * sg.W + col);
+                    gm[2 * j + s] = __ldg(gmap + row * sg.W + col);
                     u[2 * j + s] = d[2 * j + s];
                 }
             }
@@ -520,19 +504,18 @@ size_t spectral_smem_bytes(int m) {
 }
 
 template <int B, int MaxM>
-KernelFn spectral_special(bool warm, bool batch, bool adu) {
-    if (adu) return ncs_spectral_kernel<B, MaxM, false, false, true>;
+KernelFn spectral_special(bool warm, bool batch) {
     if (batch) return warm ? ncs_spectral_kernel<B, MaxM, true, true>
                            : ncs_spectral_kernel<B, MaxM, false, true>;
     return ncs_spectral_kernel<B, MaxM, true, false>;
 }
 
 template <int MaxM>
-KernelFn spectral_variant_m(int blocks, bool warm, bool batch, bool adu) {
-    // proposals, batches and raw-ADU input: 3 or 4 CTAs per SM
-    if (adu || batch || warm)
-        return blocks >= 4 ? spectral_special<4, MaxM>(warm, batch, adu)
-                           : spectral_special<3, MaxM>(warm, batch, adu);
+KernelFn spectral_variant_m(int blocks, bool warm, bool batch) {
+    // proposals and batches: 3 or 4 CTAs per SM
+    if (batch || warm)
+        return blocks >= 4 ? spectral_special<4, MaxM>(warm, batch)
+                           : spectral_special<3, MaxM>(warm, batch);
     switch (blocks <= 3 ? 3 : (blocks >= 5 ? 5 : blocks)) {
         case 3: return ncs_spectral_kernel<3, MaxM, false, false>;
         case 4: return ncs_spectral_kernel<4, MaxM, false, false>;
@@ -540,10 +523,10 @@ KernelFn spectral_variant_m(int blocks, bool warm, bool batch, bool adu) {
     }
 }
 
-KernelFn spectral_variant(int blocks, int m, bool warm, bool batch, bool adu = false) {
-    return m <= 1 ? spectral_variant_m<1>(blocks, warm, batch, adu)
-                  : (m <= 2 ? spectral_variant_m<2>(blocks, warm, batch, adu)
-                            : spectral_variant_m<4>(blocks, warm, batch, adu));
+KernelFn spectral_variant(int blocks, int m, bool warm, bool batch) {
+    return m <= 1 ? spectral_variant_m<1>(blocks, warm, batch)
+                  : (m <= 2 ? spectral_variant_m<2>(blocks, warm, batch)
+                            : spectral_variant_m<4>(blocks, warm, batch));
 }
 
 int spectral_default_blocks(int m) {
@@ -563,8 +546,7 @@ int spectral_default_blocks(int m) {
 cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream) {
     const size_t smem = spectral_smem_bytes(args.m);
     const KernelFn fn = spectral_variant(blocks > 0 ? blocks : spectral_default_blocks(args.m), args.m,
-                                         args.u0 != nullptr, args.stacks != nullptr,
-                                         args.adu_gain != nullptr);
+                                         args.u0 != nullptr, args.stacks != nullptr);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     fn<<<grid, kWarpCtaThreads, smem, stream>>>(args);

@@ -195,9 +195,10 @@ class Solver:
         [H, W], ``gain`` and ``variance`` [H, W] or [L, H, W] (L gain
         amplifiers, chosen per pixel by ADU level against the L - 1 ascending
         ``levels``).  The conversion to photo-electrons (d = (ADU - offset) /
-        gain, non-positive d -> 1e-6, gamma = variance / gain^2) happens inside
-        the solver's tile gather.  Returns ``out`` in photo-electrons, or with
-        ``tile_stats`` (out, iters, status, cost, evals)."""
+        gain, non-positive d -> 1e-6, gamma = variance / gain^2) is one device
+        pass into a handle-owned buffer, then the solve; any solver form.
+        Returns ``out`` in photo-electrons, or with ``tile_stats`` (out, iters,
+        status, cost, evals)."""
         adu = self._tensor(adu, "adu")
         if adu.dim() == 2:
             adu = adu.unsqueeze(0)
@@ -220,9 +221,11 @@ class Solver:
         for q, v in enumerate(levels):
             cal.levels[q] = float(v)
         out = torch.empty_like(adu) if out is None else self._tensor(out, "out", (T, H, W))
-        n = self.num_tiles(T, H, W)
-        st = [torch.empty(n, dtype=torch.int32, device=self.device) for _ in range(3)]
-        cost = torch.empty(n, dtype=torch.float64, device=self.device)
+        st, cost = [None] * 3, None
+        if tile_stats:   # the per-tile FP64 cost is computed only when asked for
+            n = self.num_tiles(T, H, W)
+            st = [torch.empty(n, dtype=torch.int32, device=self.device) for _ in range(3)]
+            cost = torch.empty(n, dtype=torch.float64, device=self.device)
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_reduce_noise_adu(

@@ -1,12 +1,13 @@
-"""GPU tests of the fused preprocessing prologue (ncsb_reduce_noise_adu).
+"""GPU tests of the preprocessing prologue (ncsb_reduce_noise_adu).
 
-The solver's gather converts raw ADU counts with the camera calibration
-(python3-6/pyNCS/denoisetools.py:222-224 and :266, matlab/genmaps.m:29-62).
-It computes d = (ADU - offset) / gain and gamma = var / gain^2 with IEEE
-float32 subtraction, division and multiplication, so it must reproduce bit
-for bit the solve of photo-electron frames preprocessed by the same float32
-operations outside the kernel; against the FP64 oracle preprocessing
-(oracle/numpy_ref.py adu_to_photons) the solves agree to rounding.
+The library converts raw ADU counts with the camera calibration
+(python3-6/pyNCS/denoisetools.py:222-224 and :266, matlab/genmaps.m:29-62)
+in one device pass before the solve.  It computes d = (ADU - offset) / gain
+and gamma = var / gain^2 with IEEE float32 subtraction, division and
+multiplication, so it must reproduce bit for bit the solve of photo-electron
+frames preprocessed by the same float32 operations elsewhere; against the
+FP64 oracle preprocessing (oracle/numpy_ref.py adu_to_photons) the solves
+agree to rounding.
 """
 import numpy
 import pytest
@@ -42,7 +43,7 @@ def camera(T, H, W, L, seed):
 
 
 def torch_prologue(adu, offset, gain, var, levels):
-    """The same float32 operations as the kernel, outside it."""
+    """The same float32 operations as the library's conversion pass, in torch."""
     lv = torch.zeros(adu.shape, dtype=torch.long, device=adu.device)
     for t in levels:
         lv += (adu >= t).long()
@@ -92,7 +93,9 @@ def test_adu_errors(ncs):
         s.reduce_noise_adu(adu, off, gain, var, ())            # 2 pairs need 1 threshold
     with pytest.raises(RuntimeError):
         s.reduce_noise_adu(adu, off, gain, var, (float("nan"),))    # non-finite threshold
+    # the prologue feeds every solver form: the plain form on raw frames equals
+    # the plain form on frames converted with the same FP32 operations
     p = ncs.Solver(alpha=0.2, mode="plain")
     p.set_otf_mask(mask)
-    with pytest.raises(RuntimeError):
-        p.reduce_noise_adu(adu, off, gain, var, levels)
+    d, g = torch_prologue(adu, off, gain, var, levels)
+    assert torch.equal(p.reduce_noise_adu(adu, off, gain, var, levels), p.reduce_noise(d, g))

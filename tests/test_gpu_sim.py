@@ -8,7 +8,7 @@ ncsb_sim_uniforms).
   within 6 standard errors and chi-square / Kolmogorov-Smirnov tests against
   the exact distributions at p > 1e-6, for fixed seeds;
 * draws are a function of (seed, frame, pixel) only;
-* the raw-ADU output solved through the fused prologue equals the
+* the raw-ADU output solved through the preprocessing prologue equals the
   photo-electron output solved directly.
 """
 import numpy

@@ -196,6 +196,46 @@ def sum_over_ranks(x, world):
     return float(t.item())
 
 
+def host_link_ceiling(h_in, h_out, d_res, stream, reps=5):
+    """The e2e roofline: plain copies of the same bytes over the host link.
+    Times (CUDA events, median of ``reps``) the copy of ``h_in`` to the device
+    alone, of the device result ``d_res`` to ``h_out`` alone, and both at once
+    on two streams -- the floor for any pipeline that must move the stack in
+    and the result out.  Overwrites ``h_out`` with ``d_res``."""
+    d_in = torch.empty(h_in.shape, dtype=h_in.dtype, device=d_res.device)
+    s_in, s_out = torch.cuda.Stream(d_res.device), torch.cuda.Stream(d_res.device)
+
+    def timed(up, down):
+        ms = []
+        for _ in range(reps + 1):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s_in.wait_stream(stream)
+            s_out.wait_stream(stream)
+            if up:
+                with torch.cuda.stream(s_in):
+                    d_in.copy_(h_in, non_blocking=True)
+            if down:
+                with torch.cuda.stream(s_out):
+                    h_out.copy_(d_res, non_blocking=True)
+            stream.wait_stream(s_in)
+            stream.wait_stream(s_out)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        ms = sorted(ms[1:])
+        return ms[len(ms) // 2]
+
+    h2d, d2h, both = timed(True, False), timed(False, True), timed(True, True)
+    nb_in, nb_out = h_in.numel() * h_in.element_size(), d_res.numel() * d_res.element_size()
+    del d_in
+    return {"bound": "host link (PCIe), measured copies of the same bytes",
+            "h2d_gbs": nb_in / h2d / 1e6, "d2h_gbs": nb_out / d2h / 1e6,
+            "h2d_ms": h2d, "d2h_ms": d2h, "both_ms": both,
+            "note": "frac = both_ms / e2e ms_per_step: the stack in and the result out "
+                    "copied at once on two streams, no compute"}
+
+
 # ----------------------------------------------------------- CPU reference --
 
 class _quiet_stdout:
@@ -410,6 +450,8 @@ def run_ours(args, world, rank, local):
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
     e2e_value = px * e2e_steps / (e2e_ms / 1e3) / 1e6
     assert torch.equal(h_out, out.cpu()), "e2e result differs from the device-resident run"
+    link = host_link_ceiling(h_in, h_out, out, stream)
+    link["frac"] = link["both_ms"] / (e2e_ms / e2e_steps)
 
     # the plain GPU forms (the reference's L-BFGS: scalar initial matrix,
     # Armijo backtracking) on the same stack, for the "vs plain GPU" part of
@@ -541,7 +583,9 @@ def run_ours(args, world, rank, local):
                 "d2h_bytes_per_step": int(h_out.numel() * 4),
                 "api": "ncs_b200.Solver.reduce_noise_host -> ncsb_reduce_noise_host: pinned "
                        "host buffers; T/40-frame chunks round-robin over 4 streams, each copying "
-                       "in, solving and copying out"},
+                       "in, solving and copying out",
+                "ms_per_step": e2e_ms / e2e_steps,
+                "roofline": link},
         "gpu_launches": args.steps,
         "clocks": clk,
     }
@@ -756,25 +800,28 @@ def run_mixed(args, world, rank, local):
 
 
 def run_adu(args, world, rank, local):
-    """Raw camera frames through the device preprocessing prologue
-    (Solver.reduce_noise_adu: one conversion kernel, ADU -> photo-electrons
-    and gamma, then the solve) against the two-step path of the reference's
-    scripts written in torch (elementwise conversion, then solve), on a
-    stack512-sized stack of simulated raw frames.  Replicas by frame."""
+    """Raw camera frames -- 16-bit counts, as an sCMOS camera writes them --
+    through the device preprocessing prologue (Solver.reduce_noise_adu: one
+    conversion kernel, ADU -> photo-electrons and gamma, then the solve)
+    against the two-step path of the reference's scripts written in torch
+    (elementwise conversion, then solve), on a stack512-sized stack of
+    simulated raw frames.  e2e: host counts in, host photo-electrons out
+    through the pipelined Solver.reduce_noise_adu_host.  Replicas by frame."""
     import ncs_b200
     from ncs_b200 import sim
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     w = sim.make_stack_gpu("stack512", T=args.frames, device=dev, seed=1234 + rank, adu=True)
-    adu, off, gain, var = w["adu"], w["offset"], w["gain"], w["var"]
+    adu = w["adu"].round().clamp(0.0, 65535.0).to(torch.uint16)
+    off, gain, var = w["offset"], w["gain"], w["var"]
     T, H, W = adu.shape
     solver = ncs_b200.Solver(alpha=w["alpha"], max_iters=w["max_iters"])
     solver.set_otf_mask(w["mask"])
-    out = torch.empty_like(adu)
+    out = torch.empty(adu.shape, dtype=torch.float32, device=dev)
     gamma = var / (gain * gain)
 
     def two_step():
-        d = (adu - off) / gain
+        d = (adu.float() - off) / gain
         d = torch.where(d <= 0, torch.full_like(d, 1e-6), d)
         return solver.reduce_noise(d, gamma)
 
@@ -806,27 +853,26 @@ def run_adu(args, world, rank, local):
     px = sum_over_ranks(float(T * H * W), world)
     value = px * args.steps / (total_ms / 1e3) / 1e6
 
-    # end to end: raw frames from pinned host memory, result back
+    # end to end: raw counts from pinned host memory, photo-electrons back,
+    # through the pipelined host entry
     h_adu = adu.cpu().pin_memory()
-    h_out = torch.empty_like(h_adu).pin_memory()
-    steps2 = max(1, min(args.steps, 10))
-
-    def e2e_step():
-        adu.copy_(h_adu, non_blocking=True)
-        solver.reduce_noise_adu(adu, off, gain, var, out=out)
-        h_out.copy_(out, non_blocking=True)
-    e2e_ms = timed(e2e_step, steps2)
+    h_out = torch.empty(adu.shape, dtype=torch.float32).pin_memory()
+    steps2 = max(1, min(2 * args.steps, 20))
+    e2e_ms = timed(lambda: solver.reduce_noise_adu_host(h_adu, off, gain, var, out=h_out), steps2)
+    assert torch.equal(h_out, out.cpu()), "e2e result differs from the device-resident run"
+    link = host_link_ceiling(h_adu, h_out, out, stream)
+    link["frac"] = link["both_ms"] / (e2e_ms / steps2)
     line = {
         "metric": "Mpixel/s, raw ADU frames through the device preprocessing prologue",
         "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (u16 counts in)",
         "data": "synthetic raw frames (GPU simulator: WLC structure, sCMOS offset/gain/"
-                "variance maps, Poisson + read noise)",
-        "config": {"workload": "adu: stack512 raw frames (%d x %dx%d ADU), one gain/variance "
-                               "map pair, spectral form" % (T, H, W),
+                "variance maps, Poisson + read noise, rounded to 16-bit counts)",
+        "config": {"workload": "adu: stack512 raw frames (%d x %dx%d uint16 ADU), one "
+                               "gain/variance map pair, spectral form" % (T, H, W),
                    "frames": T, "height": H, "width": W,
-                   "l2": "inputs+outputs %.0f MB > 126 MB L2, no flush" % (2 * T * H * W * 4 / 1e6),
+                   "l2": "inputs+outputs %.0f MB > 126 MB L2, no flush" % (6 * T * H * W / 1e6),
                    "parallelism": "replicas by frame (one stack per rank)"},
         "two_step": {"ms_per_step": two_ms / args.steps,
                      "api": "torch elementwise ADU -> photo-electrons, then Solver.reduce_noise",
@@ -834,9 +880,13 @@ def run_adu(args, world, rank, local):
         "speedup_vs_two_step": two_ms / total_ms,
         "launches_per_step": "conversion kernel + solver kernel",
         "e2e": {"value": px * steps2 / (e2e_ms / 1e3) / 1e6, "unit": "Mpixel/s",
-                "h2d_bytes_per_step": int(h_adu.numel() * 4),
+                "h2d_bytes_per_step": int(h_adu.numel() * h_adu.element_size()),
                 "d2h_bytes_per_step": int(h_out.numel() * 4),
-                "api": "pinned raw frames in, Solver.reduce_noise_adu, result out; one stream"},
+                "ms_per_step": e2e_ms / steps2,
+                "api": "Solver.reduce_noise_adu_host -> ncsb_reduce_noise_adu_host: pinned "
+                       "16-bit counts in, T/40-frame chunks over 4 streams, each copying "
+                       "counts in, converting, solving and copying photo-electrons out",
+                "roofline": link},
         "gpu_launches": 2 * args.steps,
         "clocks": clk,
     }

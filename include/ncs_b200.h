@@ -203,6 +203,34 @@ int ncsb_reduce_noise_adu(ncsb_handle *h, const float *adu, int n_frames, int he
                           int32_t *tile_status, double *tile_cost, int32_t *tile_evals,
                           void *stream);
 
+/* Element types of raw frames: FP32 counts, or the unsigned integers cameras
+ * store (the reference's experimental stack, python3-6/EB300004.mat 'ims',
+ * is 8-bit; its script converts the counts in float64,
+ * python3-6/NCSdemo_experiment.py:47-49).  Integer counts convert to FP32
+ * exactly, so an integer stack gives the same result, bit for bit, as the
+ * same counts passed as FP32. */
+#define NCSB_ADU_F32 0
+#define NCSB_ADU_U16 1
+#define NCSB_ADU_U8 2
+
+/* ncsb_reduce_noise_adu on device frames of element type adu_type
+ * (NCSB_ADU_*); NCSB_EINVAL for another type. */
+int ncsb_reduce_noise_adu_typed(ncsb_handle *h, const void *adu, int adu_type, int n_frames,
+                                int height, int width, const ncsb_calibration *cal, float *out,
+                                int32_t *tile_iters, int32_t *tile_status, double *tile_cost,
+                                int32_t *tile_evals, void *stream);
+
+/* Raw frames in HOST memory (element type adu_type) to photo-electron
+ * results in host memory, pipelined like ncsb_reduce_noise_host: chunk i of
+ * chunk_frames frames (<= 0: T / 40, at most 64 MB of FP32) is copied in as
+ * raw counts, converted, solved and copied out on stream i % n_streams
+ * (<= 0: 4).  The calibration maps of `cal` are device pointers; adu and out
+ * should be page-locked for the copies to overlap.  Returns after the last
+ * copy out; out equals ncsb_reduce_noise_adu_typed's result bit for bit. */
+int ncsb_reduce_noise_adu_host(ncsb_handle *h, const void *adu, int adu_type, int n_frames,
+                               int height, int width, const ncsb_calibration *cal, float *out,
+                               int chunk_frames, int n_streams, void *stream);
+
 /* ---- OTF masks from optics parameters, built on the device ---------------
  * genfilter of the reference (python3-6/pyNCS/denoisetools.py:227-261 with
  * genkspace :96-101): a raised-cosine high-pass of the radial frequency

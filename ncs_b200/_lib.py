@@ -20,6 +20,11 @@ MODE_PLAIN = 0
 MODE_PLAIN_WG = 1
 MODE_SPECTRAL = 2
 
+# raw-frame element types (NCSB_ADU_*)
+ADU_F32 = 0
+ADU_U16 = 1
+ADU_U8 = 2
+
 # Per-tile status codes (cuda/ncs.cu:61-67).
 SUCCESS = 0
 UNSTARTED = -1
@@ -114,6 +119,7 @@ EXPORTS = [
     "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms", "ncsb_reduce_noise_normalized",
     "ncsb_net_infer_stack_tc", "ncsb_net_infer_tiles_tc", "ncsb_genpsfparam",
     "ncsb_net_infer_batch_tc", "ncsb_reduce_noise_host",
+    "ncsb_reduce_noise_adu_typed", "ncsb_reduce_noise_adu_host",
 ]
 
 _lib = None
@@ -169,6 +175,12 @@ def load():
     lib.ncsb_reduce_noise_adu.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           P(NcsbCalibration), vp, vp, vp, vp, vp, vp]
     lib.ncsb_reduce_noise_adu.restype = ctypes.c_int
+    lib.ncsb_reduce_noise_adu_typed.argtypes = [vp, vp, ci, ci, ci, ci, P(NcsbCalibration), vp,
+                                                vp, vp, vp, vp, vp]
+    lib.ncsb_reduce_noise_adu_typed.restype = ctypes.c_int
+    lib.ncsb_reduce_noise_adu_host.argtypes = [vp, vp, ci, ci, ci, ci, P(NcsbCalibration), vp,
+                                               ci, ci, vp]
+    lib.ncsb_reduce_noise_adu_host.restype = ctypes.c_int
     lib.ncsb_sim_render.argtypes = [vp, vp, ci, ci, ctypes.c_double, ci, f32, vp, vp]
     lib.ncsb_sim_render.restype = ctypes.c_int
     lib.ncsb_sim_camera.argtypes = [vp, ci, ci, ci, vp, vp, vp, ctypes.c_uint64, vp, vp, vp]

@@ -20,87 +20,132 @@
 namespace ncsb {
 namespace adu {
 
-// d (and gamma) of pixel p in frame t, scalar (several map pairs, or the
-// remainder of a frame whose size is not a multiple of 4)
-__device__ __forceinline__ void convert_one(const float* __restrict__ adu, long long i,
-                                            long long p, long long hw,
-                                            const float* __restrict__ offset,
-                                            const float* __restrict__ gain,
-                                            const float* __restrict__ var, int n_levels,
-                                            const float (&lev)[3], float* __restrict__ d,
-                                            float* __restrict__ gamma_frames) {
-    const float av = __ldg(adu + i);
-    int lv = 0;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) lv += (q + 1 < n_levels && av >= lev[q]) ? 1 : 0;
-    const long long at = (long long)lv * hw + p;
-    const float gn = __ldg(gain + at);
-    const float dv = (av - __ldg(offset + p)) / gn;
-    d[i] = dv <= 0.0f ? 1.0e-6f : dv;
-    if (gamma_frames) gamma_frames[i] = __ldg(var + at) / (gn * gn);
+// Raw counts as the camera stores them (FP32, or unsigned 16- or 8-bit
+// integers; every integer below 2^24 converts to FP32 exactly, so an integer
+// stack gives the same bits as the same counts in FP32).
+__device__ __forceinline__ float load1(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float load1(const uint16_t* p) {
+    return (float)__ldg(reinterpret_cast<const unsigned short*>(p));
+}
+__device__ __forceinline__ float load1(const uint8_t* p) {
+    return (float)__ldg(reinterpret_cast<const unsigned char*>(p));
+}
+__device__ __forceinline__ float4 load4(const float* p) {
+    return __ldg(reinterpret_cast<const float4*>(p));
+}
+__device__ __forceinline__ float4 load4(const uint16_t* p) {
+    const ushort4 v = __ldg(reinterpret_cast<const ushort4*>(p));
+    return make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+}
+__device__ __forceinline__ float4 load4(const uint8_t* p) {
+    const uchar4 v = __ldg(reinterpret_cast<const uchar4*>(p));
+    return make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
 }
 
+__device__ __forceinline__ float clamp_d(float dv) { return dv <= 0.0f ? 1.0e-6f : dv; }
+
 // Grid: x over groups of 4 pixels of a frame, y over frames (y-stride for
-// more than 65535 frames).  With one map pair and a frame size divisible by
-// 4, 16-byte loads and stores; frame 0's threads also write the gamma map.
-// gamma_frames: [T][H][W] with several pairs (gamma depends on the level),
-// else null.
-__global__ void __launch_bounds__(256) convert(const float* __restrict__ adu, int T, long long hw,
+// more than 65535 frames).  vec (set by the host: one map pair, a frame size
+// divisible by 4 and every pointer aligned for it): 4-wide loads and 16-byte
+// stores.  gamma_frames: [T][H][W] with several pairs (gamma depends on the
+// level), else null; gamma_map: [H][W], written by frame 0's threads, or null.
+template <typename In>
+__global__ void __launch_bounds__(256) convert(const In* __restrict__ adu, int T, long long hw,
                                                const float* __restrict__ offset,
                                                const float* __restrict__ gain,
                                                const float* __restrict__ var, int n_levels,
-                                               float l0, float l1, float l2,
+                                               float l0, float l1, float l2, int vec,
                                                float* __restrict__ d,
                                                float* __restrict__ gamma_frames,
                                                float* __restrict__ gamma_map) {
-    const float lev[3] = {l0, l1, l2};
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // pixel group
     const long long p0 = 4 * q;
     if (p0 >= hw) return;
-    const bool vec = n_levels == 1 && (hw & 3) == 0;
     for (int t = blockIdx.y; t < T; t += gridDim.y) {
         const long long i0 = (long long)t * hw + p0;
         if (vec) {
-            const float4 av = __ldg(reinterpret_cast<const float4*>(adu + i0));
+            const float4 av = load4(adu + i0);
             const float4 off = __ldg(reinterpret_cast<const float4*>(offset + p0));
             const float4 gn = __ldg(reinterpret_cast<const float4*>(gain + p0));
-            float4 dv = make_float4((av.x - off.x) / gn.x, (av.y - off.y) / gn.y,
-                                    (av.z - off.z) / gn.z, (av.w - off.w) / gn.w);
-            dv.x = dv.x <= 0.0f ? 1.0e-6f : dv.x;
-            dv.y = dv.y <= 0.0f ? 1.0e-6f : dv.y;
-            dv.z = dv.z <= 0.0f ? 1.0e-6f : dv.z;
-            dv.w = dv.w <= 0.0f ? 1.0e-6f : dv.w;
-            *reinterpret_cast<float4*>(d + i0) = dv;
-            if (t == 0) {
+            *reinterpret_cast<float4*>(d + i0) =
+                make_float4(clamp_d((av.x - off.x) / gn.x), clamp_d((av.y - off.y) / gn.y),
+                            clamp_d((av.z - off.z) / gn.z), clamp_d((av.w - off.w) / gn.w));
+            if (t == 0 && gamma_map) {
                 const float4 vv = __ldg(reinterpret_cast<const float4*>(var + p0));
                 *reinterpret_cast<float4*>(gamma_map + p0) =
                     make_float4(vv.x / (gn.x * gn.x), vv.y / (gn.y * gn.y), vv.z / (gn.z * gn.z),
                                 vv.w / (gn.w * gn.w));
             }
-        } else {
-            for (long long p = p0; p < p0 + 4 && p < hw; ++p) {
-                convert_one(adu, (long long)t * hw + p, p, hw, offset, gain, var, n_levels, lev,
-                            d, gamma_frames);
-                if (t == 0 && n_levels == 1) {
-                    const float gn = __ldg(gain + p);
-                    gamma_map[p] = __ldg(var + p) / (gn * gn);
-                }
-            }
+            continue;
+        }
+        for (long long p = p0; p < p0 + 4 && p < hw; ++p) {
+            const long long i = (long long)t * hw + p;
+            const float av = load1(adu + i);
+            // the pair of the pixel's ADU level: level k for levels[k-1] <= ADU
+            int lv = 0;
+            lv += (1 < n_levels && av >= l0) ? 1 : 0;
+            lv += (2 < n_levels && av >= l1) ? 1 : 0;
+            lv += (3 < n_levels && av >= l2) ? 1 : 0;
+            const long long at = (long long)lv * hw + p;
+            const float gn = __ldg(gain + at);
+            d[i] = clamp_d((av - __ldg(offset + p)) / gn);
+            if (gamma_frames) gamma_frames[i] = __ldg(var + at) / (gn * gn);
+            if (t == 0 && gamma_map) gamma_map[p] = __ldg(var + p) / (gn * gn);
         }
     }
 }
 
-cudaError_t launch_convert(const float* adu, int T, int H, int W, const ncsb_calibration* cal,
-                           float* d, float* gamma, cudaStream_t s) {
-    const long long hw = (long long)H * W;
+// gamma = var / gain^2 of a single map pair, for callers that convert the
+// stack in several launches
+__global__ void __launch_bounds__(256) gamma_of(long long hw, const float* __restrict__ gain,
+                                                const float* __restrict__ var,
+                                                float* __restrict__ gamma) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < hw;
+         p += (long long)gridDim.x * blockDim.x) {
+        const float gn = __ldg(gain + p);
+        gamma[p] = __ldg(var + p) / (gn * gn);
+    }
+}
+
+inline bool aligned(const void* p, size_t a) { return p == nullptr || (uintptr_t)p % a == 0; }
+
+template <typename In>
+cudaError_t launch_typed(const In* adu, int T, long long hw, const ncsb_calibration* cal,
+                         float* d, float* gamma_frames, float* gamma_map, cudaStream_t s) {
+    const bool vec = cal->n_levels == 1 && hw % 4 == 0 && aligned(adu, 4 * sizeof(In)) &&
+                     aligned(cal->offset, 16) && aligned(cal->gain, 16) &&
+                     aligned(cal->variance, 16) && aligned(d, 16) && aligned(gamma_map, 16);
     const long long groups = (hw + 3) / 4;
     const dim3 grid((unsigned)((groups + 255) / 256), (unsigned)(T < 65535 ? T : 65535));
-    const bool multi = cal->n_levels > 1;
-    // 16-byte accesses need 16-byte aligned frames: the buffers are cudaMalloc'd
-    // and a frame is a multiple of 4 floats whenever the vector path runs
-    convert<<<grid, 256, 0, s>>>(adu, T, hw, cal->offset, cal->gain, cal->variance,
-                                 cal->n_levels, cal->levels[0], cal->levels[1], cal->levels[2],
-                                 d, multi ? gamma : nullptr, multi ? nullptr : gamma);
+    convert<In><<<grid, 256, 0, s>>>(adu, T, hw, cal->offset, cal->gain, cal->variance,
+                                     cal->n_levels, cal->levels[0], cal->levels[1],
+                                     cal->levels[2], vec ? 1 : 0, d, gamma_frames, gamma_map);
+    return cudaGetLastError();
+}
+
+// T >= 1 frames of type adu_type (NCSB_ADU_*) to d [T][H][W]; gamma_frames
+// [T][H][W] (several pairs) and gamma_map [H][W] (one pair) may each be null.
+cudaError_t launch_convert(const void* adu, int adu_type, int T, int H, int W,
+                           const ncsb_calibration* cal, float* d, float* gamma_frames,
+                           float* gamma_map, cudaStream_t s) {
+    const long long hw = (long long)H * W;
+    switch (adu_type) {
+        case NCSB_ADU_F32:
+            return launch_typed((const float*)adu, T, hw, cal, d, gamma_frames, gamma_map, s);
+        case NCSB_ADU_U16:
+            return launch_typed((const uint16_t*)adu, T, hw, cal, d, gamma_frames, gamma_map, s);
+        case NCSB_ADU_U8:
+            return launch_typed((const uint8_t*)adu, T, hw, cal, d, gamma_frames, gamma_map, s);
+        default:
+            return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_gamma_map(const ncsb_calibration* cal, long long hw, float* gamma,
+                             cudaStream_t s, int num_sms) {
+    long long blocks = (hw + 255) / 256;
+    if (blocks > 8LL * num_sms) blocks = 8LL * num_sms;
+    gamma_of<<<(unsigned)blocks, 256, 0, s>>>(hw, cal->gain, cal->variance, gamma);
     return cudaGetLastError();
 }
 

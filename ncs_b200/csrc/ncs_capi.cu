@@ -29,8 +29,11 @@ int launch_infer_batch(const float* params, const StackDesc* stacks, int n_stack
                        long long n_tiles, float* u0, cudaStream_t s);
 }  // namespace net
 namespace adu {
-cudaError_t launch_convert(const float* adu, int T, int H, int W, const ncsb_calibration* cal,
-                           float* d, float* gamma, cudaStream_t s);
+cudaError_t launch_convert(const void* adu, int adu_type, int T, int H, int W,
+                           const ncsb_calibration* cal, float* d, float* gamma_frames,
+                           float* gamma_map, cudaStream_t s);
+cudaError_t launch_gamma_map(const ncsb_calibration* cal, long long hw, float* gamma,
+                             cudaStream_t s, int num_sms);
 }  // namespace adu
 namespace nettc {
 int launch_batch(const float* params, const StackDesc* stacks, int n_stacks, long long n_tiles,
@@ -127,6 +130,28 @@ int fail(ncsb_handle* h, int code, const std::string& msg) {
 
 int cuda_fail(ncsb_handle* h, cudaError_t e, const char* what) {
     return fail(h, NCSB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Arguments of the raw-ADU entries; NCSB_OK when the call may go ahead (with
+// n_frames == 0 it then does nothing).
+int check_adu_call(ncsb_handle* h, const void* adu, int adu_type, int n_frames, int height,
+                   int width, const ncsb_calibration* cal, const float* out) {
+    if (!h) return NCSB_EINVAL;
+    if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
+    if (!adu || !out || !cal || !cal->offset || !cal->gain || !cal->variance)
+        return fail(h, NCSB_EINVAL, "null buffer");
+    if (adu_type != NCSB_ADU_F32 && adu_type != NCSB_ADU_U16 && adu_type != NCSB_ADU_U8)
+        return fail(h, NCSB_EINVAL, "adu_type must be NCSB_ADU_F32, NCSB_ADU_U16 or NCSB_ADU_U8");
+    if (cal->n_levels < 1 || cal->n_levels > 4)
+        return fail(h, NCSB_EINVAL, "n_levels must be 1..4");
+    for (int q = 0; q + 1 < cal->n_levels; ++q) {
+        if (!std::isfinite(cal->levels[q]) || (q > 0 && !(cal->levels[q] > cal->levels[q - 1])))
+            return fail(h, NCSB_EINVAL, "levels must be finite and ascending");
+    }
+    if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
+    if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
+        return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
+    return NCSB_OK;
 }
 
 int check_params(const ncsb_params* p, std::string* why) {
@@ -371,21 +396,17 @@ cudaError_t prepare_pipe(ncsb_handle* h, int n, size_t chunk_px, size_t gamma_px
     return cudaSuccess;
 }
 
-}  // namespace
-
-extern "C" {
-
-int ncsb_reduce_noise_host(ncsb_handle* h, const float* images, int n_frames, int height,
-                           int width, const float* gamma, int gamma_per_frame, float* out,
-                           int chunk_frames, int n_streams, void* stream) {
-    if (!h) return NCSB_EINVAL;
-    if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
-    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
-    if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
-    if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
-        return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
-    if (n_frames == 0) return NCSB_OK;
-    const size_t frame_px = (size_t)height * width;
+// The chunk loop of the host entries.  init(q, st0) queues work on stream 0
+// that every chunk needs (a shared gamma map); stage(q, k, f0, n, st, a)
+// queues chunk k's copy in (and conversion) on st and points a.data /
+// a.gamma at the result.  Then each chunk is solved into d_out[k] and copied
+// out on the same stream.  Returns after the last copy out; an error waits
+// for the queued work before returning.
+template <typename Init, typename Stage>
+int run_host_pipe(ncsb_handle* h, int n_frames, int height, int width, bool per_frame,
+                  float* out, int chunk_frames, int n_streams, cudaStream_t caller, Init init,
+                  Stage stage) {
+    const size_t frame_px = (size_t)height * width, fb = frame_px * sizeof(float);
     if (chunk_frames <= 0) {
         // about 40 chunks per stack (fastest on B200 for 200 x 512^2 and
         // close to it for 100 x 2048^2: short fill and drain, few per-chunk
@@ -399,40 +420,33 @@ int ncsb_reduce_noise_host(ncsb_handle* h, const float* images, int n_frames, in
     if (n_streams <= 0) n_streams = 4;
     if (n_streams > HostPipe::kMaxStreams) n_streams = HostPipe::kMaxStreams;
     cudaError_t e = prepare_pipe(h, n_streams, (size_t)chunk_frames * frame_px, frame_px,
-                                 gamma_per_frame != 0);
+                                 per_frame);
     if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline set-up");
     HostPipe* q = h->pipe;
-    cudaStream_t caller = (cudaStream_t)stream;
-    const size_t fb = frame_px * sizeof(float);
-    // every stream starts after the caller's earlier work and, for a shared
-    // gamma map, after its copy in
+    // every stream starts after the caller's earlier work and after stream
+    // 0's shared set-up
     e = cudaEventRecord(q->start, caller);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(q->st[0], q->start, 0);
-    if (e == cudaSuccess && !gamma_per_frame) {
-        e = cudaMemcpyAsync(q->d_gamma, gamma, fb, cudaMemcpyHostToDevice, q->st[0]);
-        if (e == cudaSuccess) e = cudaEventRecord(q->gamma_in, q->st[0]);
-    }
+    if (e == cudaSuccess) e = init(q, q->st[0]);
+    if (e == cudaSuccess) e = cudaEventRecord(q->gamma_in, q->st[0]);
     for (int k = 1; k < n_streams && e == cudaSuccess; ++k)
-        e = cudaStreamWaitEvent(q->st[k], gamma_per_frame ? q->start : q->gamma_in, 0);
-    if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline start");
+        e = cudaStreamWaitEvent(q->st[k], q->gamma_in, 0);
+    if (e != cudaSuccess) {
+        sync_pipe(q);
+        return cuda_fail(h, e, "host pipeline start");
+    }
     for (int i = 0, f0 = 0; f0 < n_frames; ++i, f0 += chunk_frames) {
         const int n = n_frames - f0 < chunk_frames ? n_frames - f0 : chunk_frames;
         const int k = i % n_streams;
         cudaStream_t st = q->st[k];
-        e = cudaMemcpyAsync(q->d_in[k], images + (size_t)f0 * frame_px, (size_t)n * fb,
-                            cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess && gamma_per_frame)
-            e = cudaMemcpyAsync(q->d_gf[k], gamma + (size_t)f0 * frame_px, (size_t)n * fb,
-                                cudaMemcpyHostToDevice, st);
+        ncsb::SolveArgs a{};
+        e = stage(q, k, f0, n, st, a);
         if (e != cudaSuccess) {
             sync_pipe(q);
             return cuda_fail(h, e, "host pipeline copy in");
         }
-        ncsb::SolveArgs a{};
         a.tile_mode = 0;
-        a.data = q->d_in[k];
-        a.gamma = gamma_per_frame ? q->d_gf[k] : q->d_gamma;
-        a.gamma_frame_stride = gamma_per_frame ? (long long)frame_px : 0;
+        a.gamma_frame_stride = per_frame ? (long long)frame_px : 0;
         a.out = q->d_out[k];
         a.T = n;
         a.H = height;
@@ -458,8 +472,47 @@ int ncsb_reduce_noise_host(ncsb_handle* h, const float* images, int n_frames, in
         if (e == cudaSuccess) e = cudaStreamWaitEvent(caller, q->done[k], 0);
     }
     for (int k = 0; k < n_streams && e == cudaSuccess; ++k) e = cudaEventSynchronize(q->done[k]);
-    if (e != cudaSuccess) return cuda_fail(h, e, "host pipeline finish");
+    if (e != cudaSuccess) {
+        sync_pipe(q);
+        return cuda_fail(h, e, "host pipeline finish");
+    }
     return NCSB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ncsb_reduce_noise_host(ncsb_handle* h, const float* images, int n_frames, int height,
+                           int width, const float* gamma, int gamma_per_frame, float* out,
+                           int chunk_frames, int n_streams, void* stream) {
+    if (!h) return NCSB_EINVAL;
+    if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
+    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
+    if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
+    if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
+        return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
+    if (n_frames == 0) return NCSB_OK;
+    const size_t frame_px = (size_t)height * width, fb = frame_px * sizeof(float);
+    const bool per_frame = gamma_per_frame != 0;
+    // stream 0 copies a shared gamma map in before any chunk
+    auto init = [&](HostPipe* q, cudaStream_t st0) {
+        return per_frame ? cudaSuccess
+                         : cudaMemcpyAsync(q->d_gamma, gamma, fb, cudaMemcpyHostToDevice, st0);
+    };
+    // chunk k: the photon frames (and per-frame gamma) straight into the solve's inputs
+    auto stage = [&](HostPipe* q, int k, int f0, int n, cudaStream_t st, ncsb::SolveArgs& a) {
+        cudaError_t e = cudaMemcpyAsync(q->d_in[k], images + (size_t)f0 * frame_px,
+                                        (size_t)n * fb, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && per_frame)
+            e = cudaMemcpyAsync(q->d_gf[k], gamma + (size_t)f0 * frame_px, (size_t)n * fb,
+                                cudaMemcpyHostToDevice, st);
+        a.data = q->d_in[k];
+        a.gamma = per_frame ? q->d_gf[k] : q->d_gamma;
+        return e;
+    };
+    return run_host_pipe(h, n_frames, height, width, per_frame, out, chunk_frames, n_streams,
+                         (cudaStream_t)stream, init, stage);
 }
 
 int ncsb_reduce_noise_start(ncsb_handle* h, const float* images, int n_frames, int height,
@@ -502,20 +555,16 @@ int ncsb_reduce_noise_adu(ncsb_handle* h, const float* adu, int n_frames, int he
                           const ncsb_calibration* cal, float* out, int32_t* tile_iters,
                           int32_t* tile_status, double* tile_cost, int32_t* tile_evals,
                           void* stream) {
-    if (!h) return NCSB_EINVAL;
-    if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
-    if (!adu || !out || !cal || !cal->offset || !cal->gain || !cal->variance)
-        return fail(h, NCSB_EINVAL, "null buffer");
-    if (cal->n_levels < 1 || cal->n_levels > 4)
-        return fail(h, NCSB_EINVAL, "n_levels must be 1..4");
-    for (int q = 0; q + 1 < cal->n_levels; ++q) {
-        if (!std::isfinite(cal->levels[q]) || (q > 0 && !(cal->levels[q] > cal->levels[q - 1])))
-            return fail(h, NCSB_EINVAL, "levels must be finite and ascending");
-    }
-    if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
-    if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
-        return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
-    if (n_frames == 0) return NCSB_OK;
+    return ncsb_reduce_noise_adu_typed(h, adu, NCSB_ADU_F32, n_frames, height, width, cal, out,
+                                       tile_iters, tile_status, tile_cost, tile_evals, stream);
+}
+
+int ncsb_reduce_noise_adu_typed(ncsb_handle* h, const void* adu, int adu_type, int n_frames,
+                                int height, int width, const ncsb_calibration* cal, float* out,
+                                int32_t* tile_iters, int32_t* tile_status, double* tile_cost,
+                                int32_t* tile_evals, void* stream) {
+    const int rc = check_adu_call(h, adu, adu_type, n_frames, height, width, cal, out);
+    if (rc != NCSB_OK || n_frames == 0) return rc;
     // converted frames, then gamma (one map, or one per frame with several pairs)
     const size_t frame_px = (size_t)height * width, stack_px = (size_t)n_frames * frame_px;
     const bool multi = cal->n_levels > 1;
@@ -533,7 +582,8 @@ int ncsb_reduce_noise_adu(ncsb_handle* h, const float* adu, int n_frames, int he
     }
     float* d = h->d_adu;
     float* gam = h->d_adu + stack_px;
-    cudaError_t e = ncsb::adu::launch_convert(adu, n_frames, height, width, cal, d, gam, s);
+    cudaError_t e = ncsb::adu::launch_convert(adu, adu_type, n_frames, height, width, cal, d,
+                                              multi ? gam : nullptr, multi ? nullptr : gam, s);
     if (e != cudaSuccess) return cuda_fail(h, e, "raw-ADU conversion");
     ncsb::SolveArgs a{};
     a.tile_mode = 0;
@@ -552,6 +602,38 @@ int ncsb_reduce_noise_adu(ncsb_handle* h, const float* adu, int n_frames, int he
     a.cost = tile_cost;
     a.evals = tile_evals;
     return launch(h, a, s);
+}
+
+int ncsb_reduce_noise_adu_host(ncsb_handle* h, const void* adu, int adu_type, int n_frames,
+                               int height, int width, const ncsb_calibration* cal, float* out,
+                               int chunk_frames, int n_streams, void* stream) {
+    const int rc = check_adu_call(h, adu, adu_type, n_frames, height, width, cal, out);
+    if (rc != NCSB_OK || n_frames == 0) return rc;
+    const size_t frame_px = (size_t)height * width;
+    const size_t esize = adu_type == NCSB_ADU_F32 ? 4 : adu_type == NCSB_ADU_U16 ? 2 : 1;
+    const bool multi = cal->n_levels > 1;
+    const char* src = static_cast<const char*>(adu);
+    // one pair: stream 0 computes the shared gamma map before any chunk
+    auto init = [&](HostPipe* q, cudaStream_t st0) {
+        return multi ? cudaSuccess
+                     : ncsb::adu::launch_gamma_map(cal, (long long)frame_px, q->d_gamma, st0,
+                                                   h->num_sms);
+    };
+    // chunk k: raw counts into d_out[k] (at most 4 bytes a pixel, so they fit;
+    // the solve overwrites them only after the conversion, in stream order),
+    // converted into d_in[k] (and per-frame gamma into d_gf[k])
+    auto stage = [&](HostPipe* q, int k, int f0, int n, cudaStream_t st, ncsb::SolveArgs& a) {
+        cudaError_t e = cudaMemcpyAsync(q->d_out[k], src + (size_t)f0 * frame_px * esize,
+                                        (size_t)n * frame_px * esize, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = ncsb::adu::launch_convert(q->d_out[k], adu_type, n, height, width, cal, q->d_in[k],
+                                          multi ? q->d_gf[k] : nullptr, nullptr, st);
+        a.data = q->d_in[k];
+        a.gamma = multi ? q->d_gf[k] : q->d_gamma;
+        return e;
+    };
+    return run_host_pipe(h, n_frames, height, width, multi, out, chunk_frames, n_streams,
+                         (cudaStream_t)stream, init, stage);
 }
 
 int ncsb_solve_tiles(ncsb_handle* h, const float* data_in, const float* gamma_in, const float* u0,

@@ -40,6 +40,8 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
 
 
+_ADU_TYPES = {torch.float32: _lib.ADU_F32, torch.uint16: _lib.ADU_U16, torch.uint8: _lib.ADU_U8}
+
 _MODES = {"plain": _lib.MODE_PLAIN, "plain_wg": _lib.MODE_PLAIN_WG,
           "spectral": _lib.MODE_SPECTRAL}
 
@@ -189,20 +191,9 @@ class Solver:
                 ctypes.c_void_p(s.cuda_stream)))
         return out, iters, status, cost, evals, start
 
-    def reduce_noise_adu(self, adu, offset, gain, variance, levels=(), out=None,
-                         tile_stats=False, stream=None):
-        """Denoise raw camera frames: ``adu`` [T, H, W] counts, ``offset``
-        [H, W], ``gain`` and ``variance`` [H, W] or [L, H, W] (L gain
-        amplifiers, chosen per pixel by ADU level against the L - 1 ascending
-        ``levels``).  The conversion to photo-electrons (d = (ADU - offset) /
-        gain, non-positive d -> 1e-6, gamma = variance / gain^2) is one device
-        pass into a handle-owned buffer, then the solve; any solver form.
-        Returns ``out`` in photo-electrons, or with ``tile_stats`` (out, iters,
-        status, cost, evals)."""
-        adu = self._tensor(adu, "adu")
-        if adu.dim() == 2:
-            adu = adu.unsqueeze(0)
-        T, H, W = adu.shape
+    def _calibration(self, offset, gain, variance, levels, H, W):
+        """ncsb_calibration of device maps: offset [H, W], gain and variance
+        [H, W] or [L, H, W], L - 1 ascending thresholds."""
         offset = self._tensor(offset, "offset", (H, W))
         gain = self._tensor(gain, "gain")
         variance = self._tensor(variance, "variance")
@@ -220,7 +211,33 @@ class Solver:
         cal.n_levels = L
         for q, v in enumerate(levels):
             cal.levels[q] = float(v)
-        out = torch.empty_like(adu) if out is None else self._tensor(out, "out", (T, H, W))
+        return cal, (offset, gain, variance)
+
+    def reduce_noise_adu(self, adu, offset, gain, variance, levels=(), out=None,
+                         tile_stats=False, stream=None):
+        """Denoise raw camera frames: ``adu`` [T, H, W] counts (a float32,
+        uint16 or uint8 CUDA tensor), ``offset`` [H, W], ``gain`` and
+        ``variance`` [H, W] or [L, H, W] (L gain amplifiers, chosen per pixel
+        by ADU level against the L - 1 ascending ``levels``).  The conversion
+        to photo-electrons (d = (ADU - offset) / gain, non-positive d -> 1e-6,
+        gamma = variance / gain^2) is one device pass into a handle-owned
+        buffer, then the solve; any solver form.  Integer counts give the same
+        result as the same counts in float32.  Returns ``out`` in
+        photo-electrons, or with ``tile_stats`` (out, iters, status, cost,
+        evals)."""
+        if not isinstance(adu, torch.Tensor) or not adu.is_cuda:
+            raise TypeError("adu must be a CUDA tensor")
+        if adu.dtype not in _ADU_TYPES:
+            raise TypeError("adu must be float32, uint16 or uint8")
+        if adu.device != self.device:
+            raise ValueError("adu is on %s, solver on %s" % (adu.device, self.device))
+        adu = adu.contiguous()
+        if adu.dim() == 2:
+            adu = adu.unsqueeze(0)
+        T, H, W = adu.shape
+        cal, keep = self._calibration(offset, gain, variance, levels, H, W)
+        out = (torch.empty((T, H, W), dtype=torch.float32, device=self.device) if out is None
+               else self._tensor(out, "out", (T, H, W)))
         st, cost = [None] * 3, None
         if tile_stats:   # the per-tile FP64 cost is computed only when asked for
             n = self.num_tiles(T, H, W)
@@ -228,11 +245,47 @@ class Solver:
             cost = torch.empty(n, dtype=torch.float64, device=self.device)
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         with torch.cuda.device(self.device):
-            self._check(self.lib.ncsb_reduce_noise_adu(
-                self._handle, _ptr(adu), T, H, W, ctypes.byref(cal), _ptr(out), _ptr(st[0]),
-                _ptr(st[1]), _ptr(cost), _ptr(st[2]), ctypes.c_void_p(s.cuda_stream)))
+            self._check(self.lib.ncsb_reduce_noise_adu_typed(
+                self._handle, _ptr(adu), _ADU_TYPES[adu.dtype], T, H, W, ctypes.byref(cal),
+                _ptr(out), _ptr(st[0]), _ptr(st[1]), _ptr(cost), _ptr(st[2]),
+                ctypes.c_void_p(s.cuda_stream)))
         if tile_stats:
             return out, st[0], st[1], cost, st[2]
+        return out
+
+    def reduce_noise_adu_host(self, adu, offset, gain, variance, levels=(), out=None,
+                              chunk_frames=None, n_streams=None, stream=None):
+        """Raw frames in host memory to photo-electron results in host memory
+        (``ncsb_reduce_noise_adu_host``): ``adu`` [T, H, W] float32, uint16 or
+        uint8 (a CPU tensor or numpy array), the calibration maps CUDA
+        tensors as in ``reduce_noise_adu``.  Chunks of raw counts are copied
+        in, converted, solved and copied out on ``n_streams`` streams, so only
+        the camera's own bytes cross the host link inwards.  Page-locked
+        ``adu`` and ``out`` give the overlap.  Returns ``out`` (by default a
+        new float32 CPU tensor), bit-identical to ``reduce_noise_adu``."""
+        h_in = adu if isinstance(adu, torch.Tensor) else torch.from_numpy(numpy.asarray(adu))
+        if h_in.device.type != "cpu":
+            raise TypeError("reduce_noise_adu_host takes host frames")
+        if h_in.dtype not in _ADU_TYPES:
+            raise TypeError("adu must be float32, uint16 or uint8")
+        h_in = h_in.contiguous()
+        if h_in.dim() == 2:
+            h_in = h_in.unsqueeze(0)
+        if h_in.dim() != 3:
+            raise ValueError("adu must be [T, H, W] or [H, W]")
+        T, H, W = h_in.shape
+        cal, keep = self._calibration(offset, gain, variance, levels, H, W)
+        if out is None:
+            out = torch.empty((T, H, W), dtype=torch.float32)
+        elif (out.device.type != "cpu" or out.dtype != torch.float32
+              or tuple(out.shape) != (T, H, W) or not out.is_contiguous()):
+            raise ValueError("out must be a contiguous float32 host tensor [T, H, W]")
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.ncsb_reduce_noise_adu_host(
+                self._handle, _ptr(h_in), _ADU_TYPES[h_in.dtype], T, H, W, ctypes.byref(cal),
+                _ptr(out), int(chunk_frames or 0), int(n_streams or 0),
+                ctypes.c_void_p(s.cuda_stream)))
         return out
 
     # ---- batched launch: many stacks, each with its own alpha and mask ------

@@ -99,3 +99,76 @@ def test_adu_errors(ncs):
     p.set_otf_mask(mask)
     d, g = torch_prologue(adu, off, gain, var, levels)
     assert torch.equal(p.reduce_noise_adu(adu, off, gain, var, levels), p.reduce_noise(d, g))
+
+
+def integer_counts(adu, dtype):
+    """The camera's counts as stored: rounded and clipped to the type's range."""
+    hi = 255.0 if dtype == torch.uint8 else 65535.0
+    return adu.round().clamp(0.0, hi).to(dtype)
+
+
+@pytest.mark.parametrize("dtype", [torch.uint16, torch.uint8])
+@pytest.mark.parametrize("W,L", [(64, 1), (61, 1), (64, 2)])
+def test_integer_counts_equal_the_same_counts_in_float32(ncs, dtype, W, L):
+    # W = 64 takes the 4-wide path (one pair), W = 61 and two pairs the scalar one
+    adu, off, gain, var, levels, mask = camera(3, 40, W, L, seed=50 + W + L)
+    raw = integer_counts(adu, dtype)
+    s = ncs.Solver(alpha=0.2)
+    s.set_otf_mask(mask)
+    out = s.reduce_noise_adu(raw, off, gain, var, levels)
+    ref = s.reduce_noise_adu(raw.float(), off, gain, var, levels)
+    assert torch.equal(out, ref)
+    d, g = torch_prologue(raw.float(), off, gain, var, levels)
+    assert torch.equal(out, s.reduce_noise(d, g))
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.uint16, torch.uint8])
+@pytest.mark.parametrize("L", [1, 3])
+def test_host_raw_pipeline_equals_the_device_entry(ncs, dtype, L):
+    adu, off, gain, var, levels, mask = camera(7, 48, 52, L, seed=70 + L)
+    raw = adu if dtype == torch.float32 else integer_counts(adu, dtype)
+    s = ncs.Solver(alpha=0.2)
+    s.set_otf_mask(mask)
+    ref = s.reduce_noise_adu(raw, off, gain, var, levels).cpu()
+    h_raw = raw.cpu()
+    # pageable input, default chunks; page-locked input and output, 1-frame
+    # chunks over 3 streams (the last chunk is reused by stream 0 twice)
+    assert torch.equal(s.reduce_noise_adu_host(h_raw, off, gain, var, levels), ref)
+    pinned_out = torch.empty(ref.shape, dtype=torch.float32).pin_memory()
+    got = s.reduce_noise_adu_host(h_raw.pin_memory(), off, gain, var, levels, out=pinned_out,
+                                  chunk_frames=1, n_streams=3)
+    assert got is pinned_out and torch.equal(got, ref)
+    # numpy input
+    assert torch.equal(s.reduce_noise_adu_host(h_raw.numpy(), off, gain, var, levels), ref)
+
+
+def test_unaligned_maps_and_frames_take_the_scalar_path(ncs):
+    # views 4 (maps) and 2 (uint16 frames) bytes past an allocation's start
+    # cannot be read 16 bytes at a time; the host sees it and the kernel reads
+    # them one element at a time, with the same result
+    adu, off, gain, var, levels, mask = camera(2, 32, 64, 1, seed=90)
+    raw = integer_counts(adu, torch.uint16)
+    s = ncs.Solver(alpha=0.2)
+    s.set_otf_mask(mask)
+    ref = s.reduce_noise_adu(raw, off, gain, var, levels)
+
+    def shifted(x):
+        buf = torch.empty(x.numel() + 1, dtype=x.dtype, device=x.device)
+        buf[1:] = x.reshape(-1)
+        return buf[1:].view(x.shape)
+    u_off, u_gain, u_var, u_raw = shifted(off), shifted(gain), shifted(var), shifted(raw)
+    assert u_off.data_ptr() % 16 and u_raw.data_ptr() % 8
+    assert torch.equal(s.reduce_noise_adu(u_raw, u_off, u_gain, u_var, levels), ref)
+    assert torch.equal(s.reduce_noise_adu(raw, u_off, gain, var, levels), ref)
+
+
+def test_adu_type_errors(ncs):
+    adu, off, gain, var, levels, mask = camera(1, 32, 32, 1, seed=6)
+    s = ncs.Solver(alpha=0.2)
+    s.set_otf_mask(mask)
+    with pytest.raises(TypeError):
+        s.reduce_noise_adu(adu.to(torch.int32), off, gain, var, levels)
+    with pytest.raises(TypeError):
+        s.reduce_noise_adu_host(adu, off, gain, var, levels)          # device frames
+    with pytest.raises(TypeError):
+        s.reduce_noise_adu_host(adu.cpu().double(), off, gain, var, levels)

@@ -292,9 +292,11 @@ def cpu_sample_frames(images_cpu, threads, budget_s=20.0):
     return min(images_cpu.shape[0], max(1, threads))
 
 
-def accuracy_gate(w, tile_cost, n_sample, seed=0):
+def accuracy_gate(w, tile_cost, n_sample, seed=0, tile_u=None):
     """Per-tile final cost vs the FP64 Newton optimum (oracle) on a random
-    sample of tiles: fraction within 1e-4 relative, max and median gap."""
+    sample of tiles: fraction within 1e-4 relative, max and median gap.
+    tile_cost: the solver's own per-tile FP64 costs; or tile_u, the final
+    tiles [N, 16, 16], whose costs are then computed here in FP64."""
     from oracle import numpy_ref as nr
     images = w["images"]
     T, H, W = images.shape
@@ -315,6 +317,10 @@ def accuracy_gate(w, tile_cost, n_sample, seed=0):
         gms.append(gam[ox[i]:ox[i] + 16, oy[j]:oy[j] + 16])
     ms = numpy.fft.fftshift(w["mask"]).astype(numpy.float32).astype(numpy.float64)
     _, fstar, _ = nr.newton_solve(numpy.array(data), numpy.array(gms), ms, w["alpha"])
+    if tile_cost is None:
+        tile_cost = numpy.zeros(T * per)
+        tile_cost[idx] = nr.cost(tile_u[idx].astype(numpy.float64), numpy.array(data),
+                                 numpy.array(gms), ms, w["alpha"])
     gap = nr.rel_cost_gap(tile_cost[idx], fstar)
     return {"tiles_checked": int(idx.size), "frac_within_1e-4": float((gap <= 1e-4).mean()),
             "max_rel_gap": float(gap.max()), "median_rel_gap": float(numpy.median(gap)),
@@ -357,8 +363,55 @@ def run_reference(args, world, rank):
         "e2e": {"value": value, "unit": "Mpixel/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    ref_gpu = reference_gpu(w, args)
+    if ref_gpu is not None:
+        line["reference_gpu"] = ref_gpu
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_gpu(w, args):
+    """The reference's own GPU path on the arm's workload: ncsReduceNoise of
+    cuda/ncs.cu compiled unmodified for sm_100a (oracle/_ref), launched as
+    cuda/pyCUDANCS/ncs.py launches it, one 16-thread block per tile.  The
+    tiles are cut and stitched on the device outside the timed region
+    (pyCUDANCS does both on the host); the kernel alone is timed with CUDA
+    events.  It runs to its own stopping rule (||g|| <= 1e-4 max(||u||, 1),
+    200 iterations at most): the kernel has no cap parameter.  None when the
+    kernel was not built or there is no GPU."""
+    from oracle import refgpu
+    if args.no_compare_plain or not torch.cuda.is_available() or not refgpu.available():
+        return None
+    dev = torch.device("cuda", 0)
+    images, gamma = w["images"].to(dev), w["gamma"].to(dev)
+    T, H, W = images.shape
+    dt, gt = refgpu.segment(images, gamma)
+    ms = numpy.fft.fftshift(w["mask"]).astype(numpy.float32)
+    u, it, st = refgpu.reduce_noise_tiles(dt, gt, ms, w["alpha"])   # warm-up
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    reps = max(1, min(args.steps, 2))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        u, it, st = refgpu.reduce_noise_tiles(dt, gt, ms, w["alpha"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_step = e0.elapsed_time(e1) / reps
+    status = {str(k): int(v) for k, v in zip(*numpy.unique(st.cpu().numpy(), return_counts=True))}
+    rec = {"kernel": "ncsReduceNoise (cuda/ncs.cu, unmodified, nvcc sm_100a; block 16, grid = "
+                     "tiles, as cuda/pyCUDANCS/ncs.py:116-125)",
+           "ms_per_step": ms_step, "value": T * H * W / (ms_step / 1e3) / 1e6,
+           "unit": "Mpixel/s", "tiles": int(dt.shape[0]),
+           "mean_iters": it.double().mean().item(), "status": status,
+           "stopping_rule": "||g|| <= 1e-4 max(||u||, 1) or 200 iterations (ncs.cu:55-57)",
+           "timed": "kernel only, CUDA events, mean of %d launches after one warm-up" % reps}
+    from oracle import numpy_ref as nr
+    if dt.shape[0] == T * len(nr.tile_origins(H)) * len(nr.tile_origins(W)):
+        rec["accuracy"] = accuracy_gate(w, None, args.accuracy_tiles,
+                                        tile_u=u.cpu().numpy())
+    del dt, gt, u
+    return rec
 
 
 METRIC = "Mpixel/s at <=1e-4 rel cost vs FP64: warm-start+TC vs plain GPU (pyCNCS ref)"

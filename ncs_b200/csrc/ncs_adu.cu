@@ -11,7 +11,7 @@
 // built and measured (stack512 with the per-tile cost report on: 3.72 ms
 // against 3.07 ms for this pass plus the solve) -- its extra code in the
 // persistent solver's tile loop cost the hot loop more than the HBM round
-// trip of d that this pass adds (about 0.08 ms on stack512).
+// trip of d that this pass adds (about 0.06 ms on stack512).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -44,11 +44,17 @@ __device__ __forceinline__ float4 load4(const uint8_t* p) {
 
 __device__ __forceinline__ float clamp_d(float dv) { return dv <= 0.0f ? 1.0e-6f : dv; }
 
-// Grid: x over groups of 4 pixels of a frame, y over frames (y-stride for
-// more than 65535 frames).  vec (set by the host: one map pair, a frame size
-// divisible by 4 and every pointer aligned for it): 4-wide loads and 16-byte
-// stores.  gamma_frames: [T][H][W] with several pairs (gamma depends on the
-// level), else null; gamma_map: [H][W], written by frame 0's threads, or null.
+// Frames one thread converts: its maps are loaded once per chunk and stay in
+// registers, so L2 serves each map once per kFramesPerThread frames instead
+// of once per frame.
+constexpr int kFramesPerThread = 8;
+
+// Grid: x over groups of 4 pixels of a frame, y over chunks of
+// kFramesPerThread frames (y-stride past 65535 chunks).  vec (set by the
+// host: one map pair, a frame size divisible by 4 and every pointer aligned
+// for it): 4-wide loads and 16-byte stores.  gamma_frames: [T][H][W] with
+// several pairs (gamma depends on the level), else null; gamma_map: [H][W],
+// written by the threads of frame 0, or null.
 template <typename In>
 __global__ void __launch_bounds__(256) convert(const In* __restrict__ adu, int T, long long hw,
                                                const float* __restrict__ offset,
@@ -61,36 +67,47 @@ __global__ void __launch_bounds__(256) convert(const In* __restrict__ adu, int T
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // pixel group
     const long long p0 = 4 * q;
     if (p0 >= hw) return;
-    for (int t = blockIdx.y; t < T; t += gridDim.y) {
-        const long long i0 = (long long)t * hw + p0;
-        if (vec) {
-            const float4 av = load4(adu + i0);
-            const float4 off = __ldg(reinterpret_cast<const float4*>(offset + p0));
-            const float4 gn = __ldg(reinterpret_cast<const float4*>(gain + p0));
-            *reinterpret_cast<float4*>(d + i0) =
-                make_float4(clamp_d((av.x - off.x) / gn.x), clamp_d((av.y - off.y) / gn.y),
-                            clamp_d((av.z - off.z) / gn.z), clamp_d((av.w - off.w) / gn.w));
-            if (t == 0 && gamma_map) {
-                const float4 vv = __ldg(reinterpret_cast<const float4*>(var + p0));
-                *reinterpret_cast<float4*>(gamma_map + p0) =
-                    make_float4(vv.x / (gn.x * gn.x), vv.y / (gn.y * gn.y), vv.z / (gn.z * gn.z),
-                                vv.w / (gn.w * gn.w));
-            }
-            continue;
+    if (vec) {
+        const float4 off = __ldg(reinterpret_cast<const float4*>(offset + p0));
+        const float4 gn = __ldg(reinterpret_cast<const float4*>(gain + p0));
+        if (blockIdx.y == 0 && gamma_map) {
+            const float4 vv = __ldg(reinterpret_cast<const float4*>(var + p0));
+            *reinterpret_cast<float4*>(gamma_map + p0) =
+                make_float4(vv.x / (gn.x * gn.x), vv.y / (gn.y * gn.y), vv.z / (gn.z * gn.z),
+                            vv.w / (gn.w * gn.w));
         }
-        for (long long p = p0; p < p0 + 4 && p < hw; ++p) {
-            const long long i = (long long)t * hw + p;
-            const float av = load1(adu + i);
-            // the pair of the pixel's ADU level: level k for levels[k-1] <= ADU
-            int lv = 0;
-            lv += (1 < n_levels && av >= l0) ? 1 : 0;
-            lv += (2 < n_levels && av >= l1) ? 1 : 0;
-            lv += (3 < n_levels && av >= l2) ? 1 : 0;
-            const long long at = (long long)lv * hw + p;
-            const float gn = __ldg(gain + at);
-            d[i] = clamp_d((av - __ldg(offset + p)) / gn);
-            if (gamma_frames) gamma_frames[i] = __ldg(var + at) / (gn * gn);
-            if (t == 0 && gamma_map) gamma_map[p] = __ldg(var + p) / (gn * gn);
+        for (long long t0 = (long long)blockIdx.y * kFramesPerThread; t0 < T;
+             t0 += (long long)gridDim.y * kFramesPerThread) {
+            const int n = T - t0 < kFramesPerThread ? (int)(T - t0) : kFramesPerThread;
+#pragma unroll 4
+            for (int k = 0; k < n; ++k) {
+                const long long i0 = (t0 + k) * hw + p0;
+                const float4 av = load4(adu + i0);
+                *reinterpret_cast<float4*>(d + i0) = make_float4(
+                    clamp_d((av.x - off.x) / gn.x), clamp_d((av.y - off.y) / gn.y),
+                    clamp_d((av.z - off.z) / gn.z), clamp_d((av.w - off.w) / gn.w));
+            }
+        }
+        return;
+    }
+    for (long long t0 = (long long)blockIdx.y * kFramesPerThread; t0 < T;
+         t0 += (long long)gridDim.y * kFramesPerThread) {
+        const long long t1 = T - t0 < kFramesPerThread ? T : t0 + kFramesPerThread;
+        for (long long t = t0; t < t1; ++t) {
+            for (long long p = p0; p < p0 + 4 && p < hw; ++p) {
+                const long long i = t * hw + p;
+                const float av = load1(adu + i);
+                // the pair of the pixel's ADU level: level k for levels[k-1] <= ADU
+                int lv = 0;
+                lv += (1 < n_levels && av >= l0) ? 1 : 0;
+                lv += (2 < n_levels && av >= l1) ? 1 : 0;
+                lv += (3 < n_levels && av >= l2) ? 1 : 0;
+                const long long at = (long long)lv * hw + p;
+                const float gn = __ldg(gain + at);
+                d[i] = clamp_d((av - __ldg(offset + p)) / gn);
+                if (gamma_frames) gamma_frames[i] = __ldg(var + at) / (gn * gn);
+                if (t == 0 && gamma_map) gamma_map[p] = __ldg(var + p) / (gn * gn);
+            }
         }
     }
 }
@@ -116,7 +133,8 @@ cudaError_t launch_typed(const In* adu, int T, long long hw, const ncsb_calibrat
                      aligned(cal->offset, 16) && aligned(cal->gain, 16) &&
                      aligned(cal->variance, 16) && aligned(d, 16) && aligned(gamma_map, 16);
     const long long groups = (hw + 3) / 4;
-    const dim3 grid((unsigned)((groups + 255) / 256), (unsigned)(T < 65535 ? T : 65535));
+    const long long chunks = (T + kFramesPerThread - 1) / kFramesPerThread;
+    const dim3 grid((unsigned)((groups + 255) / 256), (unsigned)(chunks < 65535 ? chunks : 65535));
     convert<In><<<grid, 256, 0, s>>>(adu, T, hw, cal->offset, cal->gain, cal->variance,
                                      cal->n_levels, cal->levels[0], cal->levels[1],
                                      cal->levels[2], vec ? 1 : 0, d, gamma_frames, gamma_map);

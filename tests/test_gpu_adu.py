@@ -172,3 +172,24 @@ def test_adu_type_errors(ncs):
         s.reduce_noise_adu_host(adu, off, gain, var, levels)          # device frames
     with pytest.raises(TypeError):
         s.reduce_noise_adu_host(adu.cpu().double(), off, gain, var, levels)
+
+
+def test_more_frames_than_one_grid_dimension(ncs):
+    # 530,000 frames: the conversion grid's frame dimension (chunks of 8
+    # frames) stops at 65,535 and strides over the rest; the solve covers
+    # every frame
+    T, H, W = 530000, 16, 16
+    g = torch.Generator(device="cuda").manual_seed(3)
+    off = torch.full((H, W), 100.0, device="cuda")
+    gain = 2.0 + 0.1 * torch.rand((H, W), device="cuda", generator=g)
+    var = 50.0 + torch.rand((H, W), device="cuda", generator=g)
+    phot = 20.0 + 10.0 * torch.rand((T, H, W), device="cuda", generator=g)
+    raw = (phot * gain + off).round().to(torch.uint16)
+    s = ncs.Solver(alpha=0.2, max_iters=5)
+    from conftest import create_otf_mask_shifted
+    s.set_otf_mask_shifted(create_otf_mask_shifted())
+    out = s.reduce_noise_adu(raw, off, gain, var)
+    d = (raw.float() - off) / gain
+    d = torch.where(d <= 0, torch.full_like(d, 1e-6), d)
+    ref = s.reduce_noise(d, var / (gain * gain))
+    assert torch.equal(out, ref)

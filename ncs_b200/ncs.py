@@ -40,6 +40,23 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
 
 
+def launch_stream(stream, device, *tensors):
+    """The stream a call's kernels run on: ``stream``, else the current one.
+    On a caller's stream other than the current one, that stream first waits
+    for the current stream (where the wrappers make their contiguous copies
+    and allocate their outputs), and every device tensor of the launch is
+    recorded on it, so that the caching allocator does not hand their memory
+    to other work while the launch may still use it."""
+    cur = torch.cuda.current_stream(device)
+    if stream is None or stream == cur:
+        return cur
+    stream.wait_stream(cur)
+    for t in tensors:
+        if isinstance(t, torch.Tensor) and t.is_cuda:
+            t.record_stream(stream)
+    return stream
+
+
 _ADU_TYPES = {torch.float32: _lib.ADU_F32, torch.uint16: _lib.ADU_U16, torch.uint8: _lib.ADU_U8}
 
 _MODES = {"plain": _lib.MODE_PLAIN, "plain_wg": _lib.MODE_PLAIN_WG,
@@ -146,7 +163,7 @@ class Solver:
             status = torch.empty(n, dtype=torch.int32, device=self.device)
             cost = torch.empty(n, dtype=torch.float64, device=self.device)
             evals = torch.empty(n, dtype=torch.int32, device=self.device)
-        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        s = launch_stream(stream, self.device, images, gamma, out, iters, status, cost, evals)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_reduce_noise(
                 self._handle, _ptr(images), T, H, W, _ptr(gamma), per_frame, _ptr(out),
@@ -183,7 +200,8 @@ class Solver:
         cost = torch.empty(n, dtype=torch.float64, device=self.device)
         evals = torch.empty(n, dtype=torch.int32, device=self.device)
         start = torch.empty(n, dtype=torch.int32, device=self.device)
-        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        s = launch_stream(stream, self.device, images, gamma, u0_tiles, out, iters, status, cost,
+                          evals, start)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_reduce_noise_start(
                 self._handle, _ptr(images), T, H, W, _ptr(gamma), per_frame, _ptr(u0_tiles),
@@ -243,7 +261,7 @@ class Solver:
             n = self.num_tiles(T, H, W)
             st = [torch.empty(n, dtype=torch.int32, device=self.device) for _ in range(3)]
             cost = torch.empty(n, dtype=torch.float64, device=self.device)
-        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        s = launch_stream(stream, self.device, adu, out, cost, *st, *keep)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_reduce_noise_adu_typed(
                 self._handle, _ptr(adu), _ADU_TYPES[adu.dtype], T, H, W, ctypes.byref(cal),
@@ -280,7 +298,7 @@ class Solver:
         elif (out.device.type != "cpu" or out.dtype != torch.float32
               or tuple(out.shape) != (T, H, W) or not out.is_contiguous()):
             raise ValueError("out must be a contiguous float32 host tensor [T, H, W]")
-        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        s = launch_stream(stream, self.device, *keep)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_reduce_noise_adu_host(
                 self._handle, _ptr(h_in), _ADU_TYPES[h_in.dtype], T, H, W, ctypes.byref(cal),
@@ -352,7 +370,8 @@ class Solver:
         if u0_tiles is not None:
             u0_tiles = self._tensor(u0_tiles, "u0_tiles", (self.batch_tiles, 16, 16))
         st = stats or {}
-        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        s = launch_stream(stream, self.device, u0_tiles, *st.values(),
+                          *[t for stack in self._batch for t in stack])
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_batch_reduce_noise(
                 self._handle, _ptr(u0_tiles), _ptr(st.get("iters")), _ptr(st.get("status")),
@@ -407,7 +426,7 @@ class Solver:
         elif (out.device.type != "cpu" or out.dtype != torch.float32
               or tuple(out.shape) != (T, H, W) or not out.is_contiguous()):
             raise ValueError("out must be a contiguous float32 host tensor [T, H, W]")
-        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        s = launch_stream(stream, self.device)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_reduce_noise_host(
                 self._handle, _ptr(h_in), T, H, W, _ptr(h_g), per_frame, _ptr(out),
@@ -429,7 +448,7 @@ class Solver:
         status = torch.empty(n, dtype=torch.int32, device=self.device)
         cost = torch.empty(n, dtype=torch.float64, device=self.device)
         evals = torch.empty(n, dtype=torch.int32, device=self.device)
-        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        s = launch_stream(stream, self.device, data, gamma, u0, u, iters, status, cost, evals)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_solve_tiles(
                 self._handle, _ptr(data), _ptr(gamma), _ptr(u0), n, _ptr(u), _ptr(iters),
@@ -604,7 +623,7 @@ def reduce_noise_normalized(images, gamma, mask3_centred, alpha=1.0, max_iters=1
         it = torch.empty(n, dtype=torch.int32, device=images.device)
         st = torch.empty(n, dtype=torch.int32, device=images.device)
         cost = torch.empty(n, dtype=torch.float64, device=images.device)
-    s = stream if stream is not None else torch.cuda.current_stream(images.device)
+    s = launch_stream(stream, images.device, images, gamma, out, it, st, cost)
     with torch.cuda.device(images.device):
         rc = lib.ncsb_reduce_noise_normalized(
             _ptr(images), T, H, W, _ptr(gamma), per_frame,

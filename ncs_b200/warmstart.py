@@ -32,7 +32,7 @@ import numpy
 import torch
 
 from . import _lib
-from .ncs import Solver, _ptr
+from .ncs import Solver, _ptr, launch_stream
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, "warmstart_params.npy")
@@ -66,9 +66,10 @@ def init_params(seed=0):
     return p
 
 
-def _stream_ptr(stream, device):
-    s = stream if stream is not None else torch.cuda.current_stream(device)
-    return ctypes.c_void_p(s.cuda_stream)
+def _stream_ptr(stream, device, *tensors):
+    """The launch stream as a C pointer (ncs.launch_stream: a caller's stream
+    waits for the current one, and ``tensors`` are recorded on it)."""
+    return ctypes.c_void_p(launch_stream(stream, device, *tensors).cuda_stream)
 
 
 class WarmStartNet:
@@ -115,10 +116,12 @@ class WarmStartNet:
         n = _lib.num_tiles(T, H, W)
         if out is None:
             out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
+        images, gamma = images.contiguous(), gamma.contiguous()
+        sp = _stream_ptr(stream, self.device, self.params, images, gamma, out)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_net_infer_stack(
-                _ptr(self.params), _ptr(images.contiguous()), T, H, W, _ptr(gamma.contiguous()),
-                per_frame, _ptr(out), _stream_ptr(stream, self.device)), "ncsb_net_infer_stack")
+                _ptr(self.params), _ptr(images), T, H, W, _ptr(gamma), per_frame, _ptr(out), sp),
+                "ncsb_net_infer_stack")
         return out
 
     def propose_batch(self, solver, out=None, stream=None):
@@ -129,8 +132,8 @@ class WarmStartNet:
             out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_net_infer_batch(
-                _ptr(self.params), solver._handle, _ptr(out), _stream_ptr(stream, self.device)),
-                "ncsb_net_infer_batch")
+                _ptr(self.params), solver._handle, _ptr(out),
+                _stream_ptr(stream, self.device, self.params, out)), "ncsb_net_infer_batch")
         return out
 
     def propose_stack_tc(self, images, gamma, out=None, stream=None):
@@ -143,11 +146,12 @@ class WarmStartNet:
         if out is None:
             out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
         status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        images, gamma = images.contiguous(), gamma.contiguous()
+        sp = _stream_ptr(stream, self.device, self.params, images, gamma, out, status)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_net_infer_stack_tc(
-                _ptr(self.params), _ptr(images.contiguous()), T, H, W, _ptr(gamma.contiguous()),
-                per_frame, _ptr(out), _ptr(status), _stream_ptr(stream, self.device)),
-                "ncsb_net_infer_stack_tc")
+                _ptr(self.params), _ptr(images), T, H, W, _ptr(gamma), per_frame, _ptr(out),
+                _ptr(status), sp), "ncsb_net_infer_stack_tc")
         return out, status
 
     def propose_batch_tc(self, solver, out=None, status=None, stream=None):
@@ -163,26 +167,31 @@ class WarmStartNet:
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_net_infer_batch_tc(
                 _ptr(self.params), solver._handle, _ptr(out), _ptr(status),
-                _stream_ptr(stream, self.device)), "ncsb_net_infer_batch_tc")
+                _stream_ptr(stream, self.device, self.params, out, status)),
+                "ncsb_net_infer_batch_tc")
         return out, status
 
     def propose_tiles_tc(self, d, gamma, stream=None):
         n = d.shape[0]
         out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
         status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        d, gamma = d.contiguous(), gamma.contiguous()
+        sp = _stream_ptr(stream, self.device, self.params, d, gamma, out, status)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_net_infer_tiles_tc(
-                _ptr(self.params), _ptr(d.contiguous()), _ptr(gamma.contiguous()), n, _ptr(out),
-                _ptr(status), _stream_ptr(stream, self.device)), "ncsb_net_infer_tiles_tc")
+                _ptr(self.params), _ptr(d), _ptr(gamma), n, _ptr(out), _ptr(status), sp),
+                "ncsb_net_infer_tiles_tc")
         return out, status
 
     def propose_tiles(self, d, gamma, stream=None):
         n = d.shape[0]
         out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
+        d, gamma = d.contiguous(), gamma.contiguous()
+        sp = _stream_ptr(stream, self.device, self.params, d, gamma, out)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_net_infer_tiles(
-                _ptr(self.params), _ptr(d.contiguous()), _ptr(gamma.contiguous()), n, _ptr(out),
-                _stream_ptr(stream, self.device)), "ncsb_net_infer_tiles")
+                _ptr(self.params), _ptr(d), _ptr(gamma), n, _ptr(out), sp),
+                "ncsb_net_infer_tiles")
         return out
 
     # ---- training -----------------------------------------------------------

@@ -10,7 +10,7 @@
 // One thread per pixel: 9 unknowns, FP64 iterate, gradient and costs (the
 // cost is a sum of terms of order 100 whose differences near convergence are
 // of order 1e-5), BFGS with a dense 9 x 9 inverse-Hessian approximation kept
-// in shared memory (45 packed FP32 entries per thread), backtracking Armijo
+// in shared memory (45 packed FP64 entries per thread), backtracking Armijo
 // line search with the fraction-to-barrier rule of the main solver.  The
 // reference minimises with MATLAB's fminunc quasi-Newton; the stopping rule
 // here is fminunc's first-order optimality test, ||g||_inf <= tol *
@@ -27,7 +27,10 @@
 namespace ncsb {
 namespace norm {
 
-constexpr int kThreads = 128;
+// 64 threads: the FP64 inverse Hessians (45 x 8 B a thread) and segment
+// constants fit the 48 KB of static shared memory, and at 255 registers a
+// thread the SM holds 4 such blocks either way
+constexpr int kThreads = 64;
 constexpr int kPacked = 45;  // upper triangle of a symmetric 9 x 9
 
 struct Args {
@@ -94,7 +97,7 @@ __device__ double evaluate(const Args& a, const double (&u)[9], const Seg& sg, d
 }
 
 __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
-    __shared__ float Hm[kPacked][kThreads];  // inverse-Hessian approximation, per thread
+    __shared__ double Hm[kPacked][kThreads];  // inverse-Hessian approximation, per thread
     __shared__ double Cs[9][kThreads], Gs[9][kThreads];
     const long long HW = (long long)a.H * a.W;
     const long long idx = (long long)blockIdx.x * kThreads + threadIdx.x;
@@ -123,7 +126,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
 #pragma unroll
     for (int i = 0; i < 9; ++i)
 #pragma unroll
-        for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0f : 0.0f;
+        for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0 : 0.0;
 
     double fu = evaluate(a, u, sg, g, true);
     double g0 = 0.0;
@@ -143,7 +146,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
             double acc = 0.0;
 #pragma unroll
             for (int j = 0; j < 9; ++j)
-                acc = fma((double)Hm[i <= j ? pk(i, j) : pk(j, i)][t], g[j], acc);
+                acc = fma(Hm[i <= j ? pk(i, j) : pk(j, i)][t], g[j], acc);
             d[i] = -acc;
             gd = fma(g[i], d[i], gd);
         }
@@ -151,7 +154,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
 #pragma unroll
             for (int i = 0; i < 9; ++i)
 #pragma unroll
-                for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0f : 0.0f;
+                for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0 : 0.0;
             gd = 0.0;
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
         }
         if (sy > 1e-300) {
             if (it == 0) {  // scale the identity before the first update
-                const float sc = (float)(sy / yy);
+                const double sc = sy / yy;
 #pragma unroll
                 for (int i = 0; i < 9; ++i) Hm[pk(i, i)][t] = sc;
             }
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
                 double acc = 0.0;
 #pragma unroll
                 for (int j = 0; j < 9; ++j)
-                    acc = fma((double)Hm[i <= j ? pk(i, j) : pk(j, i)][t], yv[j], acc);
+                    acc = fma(Hm[i <= j ? pk(i, j) : pk(j, i)][t], yv[j], acc);
                 v[i] = acc;
                 yHy = fma(yv[i], acc, yHy);
             }
@@ -210,8 +213,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
 #pragma unroll
                 for (int j = i; j < 9; ++j) {
                     const double h = Hm[pk(i, j)][t];
-                    Hm[pk(i, j)][t] =
-                        (float)(h - rho * (v[i] * s[j] + s[i] * v[j]) + k2 * s[i] * s[j]);
+                    Hm[pk(i, j)][t] = h - rho * (v[i] * s[j] + s[i] * v[j]) + k2 * s[i] * s[j];
                 }
         }
         bool moved = false;

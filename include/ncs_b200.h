@@ -7,9 +7,11 @@
  * caller owns them.  `stream` is a cudaStream_t passed as void* (NULL = the
  * legacy default stream).  Every call returns NCSB_OK (0) or a negative
  * NCSB_E* code and never aborts; ncsb_last_error() describes the last failure
- * on a handle.  One handle must not be used by two host threads at once, and
- * two launches on one handle must not overlap on the GPU (they share the
- * handle's work-queue counter).
+ * on a handle.  A call for 0 frames (or 0 tiles) checks its shape and
+ * parameters and does nothing; its data buffers may then be null (an empty
+ * tensor's data_ptr() is 0).  One handle must not be used by two host
+ * threads at once, and two launches on one handle must not overlap on the
+ * GPU (they share the handle's work-queue counter).
  *
  * Reference interfaces replaced (paths in the HuanglabPurdue/NCS tree):
  *   ncsb_reduce_noise  <- C   ncsReduceNoise(double*, double*, double*, double*,

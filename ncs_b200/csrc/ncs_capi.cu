@@ -133,13 +133,13 @@ int cuda_fail(ncsb_handle* h, cudaError_t e, const char* what) {
 }
 
 // Arguments of the raw-ADU entries; NCSB_OK when the call may go ahead (with
-// n_frames == 0 it then does nothing).
+// n_frames == 0 it then does nothing, and adu and out may be null).
 int check_adu_call(ncsb_handle* h, const void* adu, int adu_type, int n_frames, int height,
                    int width, const ncsb_calibration* cal, const float* out) {
     if (!h) return NCSB_EINVAL;
     if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
-    if (!adu || !out || !cal || !cal->offset || !cal->gain || !cal->variance)
-        return fail(h, NCSB_EINVAL, "null buffer");
+    if (!cal || !cal->offset || !cal->gain || !cal->variance)
+        return fail(h, NCSB_EINVAL, "null calibration map");
     if (adu_type != NCSB_ADU_F32 && adu_type != NCSB_ADU_U16 && adu_type != NCSB_ADU_U8)
         return fail(h, NCSB_EINVAL, "adu_type must be NCSB_ADU_F32, NCSB_ADU_U16 or NCSB_ADU_U8");
     if (cal->n_levels < 1 || cal->n_levels > 4)
@@ -151,6 +151,7 @@ int check_adu_call(ncsb_handle* h, const void* adu, int adu_type, int n_frames, 
     if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
     if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
         return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
+    if (n_frames > 0 && (!adu || !out)) return fail(h, NCSB_EINVAL, "null buffer");
     return NCSB_OK;
 }
 
@@ -317,11 +318,11 @@ int ncsb_reduce_noise(ncsb_handle* h, const float* images, int n_frames, int hei
                       void* stream) {
     if (!h) return NCSB_EINVAL;
     if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
-    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
     if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
     if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
         return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
-    if (n_frames == 0) return NCSB_OK;
+    if (n_frames == 0) return NCSB_OK;  // nothing read or written: buffers may be null
+    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
     ncsb::SolveArgs a{};
     a.tile_mode = 0;
     a.data = images;
@@ -488,11 +489,11 @@ int ncsb_reduce_noise_host(ncsb_handle* h, const float* images, int n_frames, in
                            int chunk_frames, int n_streams, void* stream) {
     if (!h) return NCSB_EINVAL;
     if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
-    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
     if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
     if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
         return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
-    if (n_frames == 0) return NCSB_OK;
+    if (n_frames == 0) return NCSB_OK;  // nothing read or written: buffers may be null
+    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
     const size_t frame_px = (size_t)height * width, fb = frame_px * sizeof(float);
     const bool per_frame = gamma_per_frame != 0;
     // stream 0 copies a shared gamma map in before any chunk
@@ -523,13 +524,13 @@ int ncsb_reduce_noise_start(ncsb_handle* h, const float* images, int n_frames, i
     if (!h) return NCSB_EINVAL;
     if (h->p.mode != NCSB_MODE_SPECTRAL)
         return fail(h, NCSB_EINVAL, "a proposed start needs the spectral form");
-    if (!u0_tiles) return fail(h, NCSB_EINVAL, "null proposal");
     if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
-    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
     if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
     if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)
         return fail(h, NCSB_ESIZE, "frames must be at least 14 x 14");
-    if (n_frames == 0) return NCSB_OK;
+    if (n_frames == 0) return NCSB_OK;  // nothing read or written: buffers may be null
+    if (!images || !gamma || !out) return fail(h, NCSB_EINVAL, "null buffer");
+    if (!u0_tiles) return fail(h, NCSB_EINVAL, "null proposal");
     ncsb::SolveArgs a{};
     a.tile_mode = 0;
     a.data = images;
@@ -641,9 +642,9 @@ int ncsb_solve_tiles(ncsb_handle* h, const float* data_in, const float* gamma_in
                      double* cost, int32_t* evals, void* stream) {
     if (!h) return NCSB_EINVAL;
     if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
-    if (!data_in || !gamma_in || !data_out) return fail(h, NCSB_EINVAL, "null buffer");
     if (n_tiles < 0) return fail(h, NCSB_EINVAL, "negative tile count");
-    if (n_tiles == 0) return NCSB_OK;
+    if (n_tiles == 0) return NCSB_OK;  // nothing read or written: buffers may be null
+    if (!data_in || !gamma_in || !data_out) return fail(h, NCSB_EINVAL, "null buffer");
     ncsb::SolveArgs a{};
     a.tile_mode = 1;
     a.data = data_in;

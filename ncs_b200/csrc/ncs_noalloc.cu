@@ -96,12 +96,13 @@ extern "C" int ncsb_reduce_noise_noalloc(const ncsb_params* p, const float* mask
                                          int width, const float* gamma, int gamma_per_frame,
                                          float* out, int32_t* tile_iters, int32_t* tile_status,
                                          double* tile_cost, int32_t* tile_evals, void* stream) {
-    if (!params_ok(p) || !mask_shifted_host || !images || !gamma || !out) return NCSB_EINVAL;
+    if (!params_ok(p) || !mask_shifted_host) return NCSB_EINVAL;
     if (n_frames < 0 || height <= 0 || width <= 0) return NCSB_EINVAL;
     if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2) return NCSB_ESIZE;
     // Everything this call keeps on the device must fit the static array.
     if (kTableOffset + kTableBytes > (size_t)NCSB_NOALLOC_SCRATCH_BYTES) return NCSB_ESCRATCH;
-    if (n_frames == 0) return NCSB_OK;
+    if (n_frames == 0) return NCSB_OK;  // nothing read or written: buffers may be null
+    if (!images || !gamma || !out) return NCSB_EINVAL;
 
     DeviceSetup* dev = nullptr;
     int rc = setup_current_device(&dev);

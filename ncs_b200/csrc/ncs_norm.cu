@@ -245,10 +245,11 @@ int ncsb_reduce_noise_normalized(const float* images, int n_frames, int height, 
                                  const float* mask3_centred, double alpha, int max_iters,
                                  double tolerance, float* out, int32_t* px_iters,
                                  int32_t* px_status, double* px_cost, void* stream) {
-    if (!images || !gamma || !out || !mask3_centred) return NCSB_EINVAL;
+    if (!mask3_centred) return NCSB_EINVAL;
     if (n_frames < 0 || height <= 0 || width <= 0 || max_iters < 0) return NCSB_EINVAL;
     if (!(alpha >= 0.0) || !(tolerance >= 0.0)) return NCSB_EINVAL;
-    if (n_frames == 0) return NCSB_OK;
+    if (n_frames == 0) return NCSB_OK;  // nothing read or written: buffers may be null
+    if (!images || !gamma || !out) return NCSB_EINVAL;
     // Q[a][b] = (1/9) sum_k Mu_k^2 Re(conj(F_a[k]) F_b[k]), Mu = ifftshift(mask) (the mask
     // multiplies fftshift(fft2(u))), symmetrised over k -> -k; F_a = fft2 of unit vector a
     double mu[3][3];

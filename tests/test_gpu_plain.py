@@ -308,3 +308,26 @@ def test_host_entry_with_pageable_numpy(ncs):
         assert rc == 0
         assert numpy.array_equal(out, ref.numpy())
         s.close()
+
+
+def test_empty_inputs(ncs, mode):
+    # zero frames or tiles: an empty result, whatever the entry (empty tensors
+    # have null data pointers, which the C entries accept when there is no work)
+    s = ncs.Solver(alpha=0.1, mode=mode)
+    s.set_otf_mask_shifted(create_otf_mask_shifted())
+    g = torch.ones(20, 24, device="cuda")
+    out = s.reduce_noise(torch.empty(0, 20, 24, device="cuda"), g)
+    assert out.shape == (0, 20, 24)
+    u, it, st, cost = s.solve_tiles(torch.empty(0, 16, 16, device="cuda"),
+                                    torch.empty(0, 16, 16, device="cuda"))
+    assert u.shape == (0, 16, 16) and it.numel() == 0
+    host = s.reduce_noise_host(numpy.zeros((0, 20, 24), dtype=numpy.float32),
+                               numpy.ones((20, 24), dtype=numpy.float32))
+    assert tuple(host.shape) == (0, 20, 24)
+    off, gain = torch.zeros(20, 24, device="cuda"), torch.ones(20, 24, device="cuda")
+    raw = torch.empty(0, 20, 24, dtype=torch.uint16, device="cuda")
+    assert s.reduce_noise_adu(raw, off, gain, g).shape == (0, 20, 24)
+    assert tuple(s.reduce_noise_adu_host(raw.cpu(), off, gain, g).shape) == (0, 20, 24)
+    # the size check still applies to an empty stack
+    with pytest.raises((ValueError, RuntimeError)):
+        s.reduce_noise(torch.empty(0, 10, 10, device="cuda"), torch.ones(10, 10, device="cuda"))

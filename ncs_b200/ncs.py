@@ -140,7 +140,11 @@ class Solver:
     def reduce_noise(self, images, gamma, out=None, tile_stats=False, stream=None):
         """Denoise a [T, H, W] float32 CUDA stack; gamma is [H, W] (shared) or
         [T, H, W].  Returns ``out`` or, with ``tile_stats``, (out, iters,
-        status, cost) where the per-tile arrays follow (frame, row, col) order."""
+        status, cost) where the per-tile arrays follow (frame, row, col) order;
+        ``tile_stats="all"`` adds the evaluation counts, and
+        ``tile_stats="status"`` returns (out, iters, status) only, without the
+        per-tile FP64 cost, whose 256 double-precision logs per tile the
+        kernel then skips."""
         images = self._tensor(images, "images")
         if images.dim() == 2:
             images = images.unsqueeze(0)
@@ -161,8 +165,9 @@ class Solver:
             n = self.num_tiles(T, H, W)
             iters = torch.empty(n, dtype=torch.int32, device=self.device)
             status = torch.empty(n, dtype=torch.int32, device=self.device)
-            cost = torch.empty(n, dtype=torch.float64, device=self.device)
-            evals = torch.empty(n, dtype=torch.int32, device=self.device)
+            if tile_stats != "status":
+                cost = torch.empty(n, dtype=torch.float64, device=self.device)
+                evals = torch.empty(n, dtype=torch.int32, device=self.device)
         s = launch_stream(stream, self.device, images, gamma, out, iters, status, cost, evals)
         with torch.cuda.device(self.device):
             self._check(self.lib.ncsb_reduce_noise(
@@ -171,6 +176,8 @@ class Solver:
                 ctypes.c_void_p(s.cuda_stream)))
         if tile_stats == "all":
             return out, iters, status, cost, evals
+        if tile_stats == "status":
+            return out, iters, status
         if tile_stats:
             return out, iters, status, cost
         return out
@@ -551,7 +558,7 @@ class NCSCUDA:
         dev = solver.device
         x = host.to(dev, non_blocking=True)
         g = ghost.to(dev, non_blocking=True)
-        out, iters, status, _ = solver.reduce_noise(x, g, tile_stats=True)
+        out, iters, status = solver.reduce_noise(x, g, tile_stats="status")
         result = out.cpu().numpy()
         if verbose:
             print("Processed {0:d} sub-regions.".format(iters.numel()))

@@ -331,3 +331,17 @@ def test_empty_inputs(ncs, mode):
     # the size check still applies to an empty stack
     with pytest.raises((ValueError, RuntimeError)):
         s.reduce_noise(torch.empty(0, 10, 10, device="cuda"), torch.ones(10, 10, device="cuda"))
+
+
+def test_status_only_tile_stats(ncs, mode):
+    # tile_stats="status" (the drop-in's warnings) skips the FP64 cost report;
+    # iterations, statuses and the result are those of the full report
+    rng = numpy.random.default_rng(21)
+    x = torch.from_numpy(rng.uniform(5.0, 80.0, size=(2, 40, 33)).astype(numpy.float32)).cuda()
+    g = torch.from_numpy(rng.uniform(2.0, 4.0, size=(40, 33)).astype(numpy.float32)).cuda()
+    s = ncs.Solver(alpha=0.2, mode=mode)
+    s.set_otf_mask_shifted(create_otf_mask_shifted())
+    out1, it1, st1, cost1 = s.reduce_noise(x, g, tile_stats=True)
+    out2, it2, st2 = s.reduce_noise(x, g, tile_stats="status")
+    assert torch.equal(out1, out2) and torch.equal(it1, it2) and torch.equal(st1, st2)
+    assert cost1.dtype == torch.float64 and cost1.numel() == it1.numel()

@@ -671,7 +671,7 @@ def run_ours(args, world, rank, local):
 
 def mixed_accuracy(stacks, cost, n_sample, seed=0):
     """accuracy_gate over a batch: a random sample of tiles across all stacks,
-    each judged against the FP64 optimum with its own stack's alpha and mask."""
+    each checked against the FP64 optimum with its own stack's alpha and mask."""
     from oracle import numpy_ref as nr
     per, offs = [], [0]
     for st in stacks:

@@ -62,7 +62,8 @@ def test_tiles_vs_fp64_optimum_and_reference(ncs, oracle_libs, mode):
         uref, ret, fref = oracle_libs.solve_tile(data[i].astype(numpy.float64),
                                                  gamma[i].astype(numpy.float64),
                                                  ms.astype(numpy.float64), alpha)
-        # reference criterion (test_solver.py:116-118) and the north-star one
+        # reference criterion (test_solver.py:116-118), then 1e-4 relative cost and
+        # 1e-3 relative per pixel against the C solver
         assert numpy.abs(u[i] - uref).max() / numpy.abs(uref).max() < 1e-2
         assert nr.rel_cost_gap(f_gpu[i], fref) <= 1e-4
         assert (numpy.abs(u[i] - uref) / numpy.maximum(numpy.abs(uref), 1.0)).max() <= 1e-3
@@ -72,8 +73,8 @@ def test_tiles_vs_fp64_optimum_and_reference(ncs, oracle_libs, mode):
 def test_alpha_range_vs_fp64_optimum(ncs, mode, alpha):
     """alpha from 0 (pure likelihood: the optimum is u = d) to 10 (noise term
     dominant), on bright tiles and on dark tiles with hot pixels: every tile
-    within 1e-4 relative cost of the FP64 Newton optimum (the north-star
-    tolerance), none stopped by the iteration cap."""
+    within 1e-4 relative cost of the FP64 Newton optimum (the accuracy bar of
+    the throughput metric), none stopped by the iteration cap."""
     from oracle import numpy_ref as nr
     rng = numpy.random.default_rng(21)
     bright, gb = tiles_seed1(16)

@@ -20,7 +20,10 @@ its own stack (replicas by frame, weak scaling, no collective in the data
 path); the time
 is the max over ranks.  ``--impl reference`` times the reference's own CPU
 path (pyCNCS ncs.c compiled by oracle/Makefile, else the oracle's C port) on
-all host cores instead.
+all host cores instead, and beside it, where a GPU and the build are present,
+the reference's own CUDA kernel (cuda/ncs.cu compiled unmodified) on the same
+workload as ``reference_gpu``.  ``e2e.roofline`` is the host link's measured
+ceiling: plain copies of the same bytes in and out at once.
 """
 import argparse
 import ctypes

@@ -87,3 +87,41 @@ def test_mixed_workload_parameters():
         assert s["wavelength"] in (0.52, 0.6, 0.7) and s["kind"] in ("chains", "beads")
         assert s["mask"].shape == (16, 16) and (s["images"] > 0).all()
     assert len({(s["NA"], s["wavelength"]) for s in st}) > 1
+
+
+def test_host_side_rejections_and_empty_calls(lib):
+    """Checks the entries make before any device work: a null handle, bad
+    shapes and parameters are rejected, and a call for 0 frames succeeds with
+    null data buffers (an empty tensor's data_ptr() is 0) without touching a
+    device."""
+    from ncs_b200 import _lib
+    EINVAL, OK, ESIZE = _lib.NCSB_EINVAL, _lib.NCSB_OK, _lib.NCSB_ESIZE
+    cal = _lib.NcsbCalibration()
+    assert lib.ncsb_reduce_noise_adu_typed(None, None, 1, 1, 16, 16, ctypes.byref(cal), None,
+                                           None, None, None, None, None) == EINVAL
+    assert lib.ncsb_reduce_noise_adu_host(None, None, 1, 1, 16, 16, ctypes.byref(cal), None,
+                                          0, 0, None) == EINVAL
+    # the handle-free entries: no-alloc solve and the normalised variant
+    p = _lib.default_params()
+    mask = (ctypes.c_float * 256)(*([1.0] * 256))
+    m3 = (ctypes.c_float * 9)(*([1.0] * 9))
+    noalloc, norm = lib.ncsb_reduce_noise_noalloc, lib.ncsb_reduce_noise_normalized
+    assert noalloc(ctypes.byref(p), mask, None, 0, 20, 24, None, 0, None,
+                   None, None, None, None, None) == OK
+    assert noalloc(ctypes.byref(p), mask, None, 1, 20, 24, None, 0, None,
+                   None, None, None, None, None) == EINVAL          # data needed for 1 frame
+    assert noalloc(ctypes.byref(p), mask, None, 0, 10, 24, None, 0, None,
+                   None, None, None, None, None) == ESIZE           # shape still checked
+    assert noalloc(None, mask, None, 0, 20, 24, None, 0, None, None, None, None, None,
+                   None) == EINVAL
+    bad = _lib.default_params()
+    bad.m = 0
+    assert noalloc(ctypes.byref(bad), mask, None, 0, 20, 24, None, 0, None, None, None, None,
+                   None, None) == EINVAL
+    assert norm(None, 0, 8, 8, None, 0, m3, 1.0, 15, 1e-6, None, None, None, None, None) == OK
+    assert norm(None, 1, 8, 8, None, 0, m3, 1.0, 15, 1e-6, None, None, None, None,
+                None) == EINVAL
+    assert norm(None, 0, 8, 8, None, 0, m3, -1.0, 15, 1e-6, None, None, None, None,
+                None) == EINVAL                                      # negative alpha
+    assert norm(None, 0, 8, 8, None, 0, None, 1.0, 15, 1e-6, None, None, None, None,
+                None) == EINVAL                                      # no mask

@@ -181,11 +181,16 @@ def barrier(world):
         dist.barrier()
 
 
+def _reduce_device():
+    # NCCL reduces device tensors; gloo (CPU-only runs) host tensors
+    return "cuda" if torch.cuda.is_available() else "cpu"
+
+
 def max_over_ranks(x, world):
     if world == 1:
         return x
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -194,7 +199,7 @@ def sum_over_ranks(x, world):
     if world == 1:
         return x
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 

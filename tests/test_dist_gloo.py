@@ -71,3 +71,39 @@ def test_frame_range():
                 assert b == c and b >= a
             sizes = [b - a for a, b in spans]
             assert max(sizes) - min(sizes) <= 1
+
+
+def _bench_worker(rank, world, port, q):
+    import datetime
+    import sys
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        bench.barrier(world)
+        # per-rank times and pixel counts: the job's time is the slowest
+        # rank's, its pixels the sum over ranks
+        q.put((rank, bench.max_over_ranks(10.0 + rank, world),
+               bench.sum_over_ranks(100.0 * (rank + 1), world)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_rank_reductions_gloo():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bench_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(mx == 11.0 and sm == 300.0 for _, mx, sm in res)

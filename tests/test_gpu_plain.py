@@ -346,3 +346,27 @@ def test_status_only_tile_stats(ncs, mode):
     out2, it2, st2 = s.reduce_noise(x, g, tile_stats="status")
     assert torch.equal(out1, out2) and torch.equal(it1, it2) and torch.equal(st1, st2)
     assert cost1.dtype == torch.float64 and cost1.numel() == it1.numel()
+
+
+@pytest.mark.parametrize("case,converged", [(1, False), (2, True), (3, True)])
+@pytest.mark.parametrize("pmode", ["plain", "plain_wg"])
+def test_stopping_rule_edge_cases(ncs, case, converged, pmode):
+    """The converged() cases of opencl/pyOpenCLNCS/test/test_solver_fns.py:63-110:
+    ||g|| / max(||x||, 1) against epsilon 1e-4 for x = 0.9 and g = 1e-4 in every
+    pixel (ratio 1.11e-4: not converged), x = 1.1 (9.1e-5: converged) and
+    x = 0.1/16, g = 0.9e-4/16 (||x|| = 0.1, so the floor 1 applies: 0.9e-4,
+    converged).  With alpha 0 the gradient at a proposed start x is
+    1 - (d + gamma)/(x + gamma), so d is chosen to give that g; with no
+    iterations allowed, the status is the stopping test's verdict at x (the
+    plain forms start at the proposal as given)."""
+    x_val, g_val = {1: (0.9, 1e-4), 2: (1.1, 1e-4), 3: (0.1 / 16, 0.9e-4 / 16)}[case]
+    gamma = 1.0
+    d_val = (1.0 - g_val) * (x_val + gamma) - gamma
+    d = torch.full((2, 16, 16), d_val, device="cuda")
+    g = torch.full((2, 16, 16), gamma, device="cuda")
+    x = torch.full((2, 16, 16), x_val, device="cuda")
+    s = ncs.Solver(alpha=0.0, epsilon=1e-4, max_iters=0, mode=pmode)
+    s.set_otf_mask_shifted(create_otf_mask_shifted())
+    _, it, st, _ = s.solve_tiles(d, g, u0=x)
+    st = st.cpu().numpy()
+    assert (st == (0 if converged else -2)).all(), st

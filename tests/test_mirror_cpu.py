@@ -43,3 +43,22 @@ def test_mirror_barrier_rule_on_dark_pixel():
     assert st[0] == 0
     assert nr.rel_cost_gap(nr.cost(u.astype(numpy.float64), d, g, ms, 0.2), fs)[0] <= 1e-7
     assert (u + g).min() > 0
+
+
+def test_mirror_stopping_rule_edge_cases():
+    """The converged() cases of opencl/pyOpenCLNCS/test/test_solver_fns.py:63-110
+    (||g|| / max(||x||, 1) against 1e-4): x = 0.9 with g = 1e-4 is not
+    converged, x = 1.1 is, and x = 0.1/16 with g = 0.9e-4/16 is through the
+    floor of 1 on ||x||.  With alpha 0 the gradient at a start x is
+    1 - (d + gamma)/(x + gamma), so d is chosen to give that g; with no
+    iterations allowed the status is the stopping test's verdict."""
+    from conftest import create_otf_mask_shifted
+    from oracle import gpu_mirror as gm
+    for (x_val, g_val), expect in [((0.9, 1e-4), gm.MAXITERS), ((1.1, 1e-4), gm.SUCCESS),
+                                   ((0.1 / 16, 0.9e-4 / 16), gm.SUCCESS)]:
+        d = numpy.full((1, 16, 16), (1.0 - g_val) * (x_val + 1.0) - 1.0, numpy.float32)
+        g = numpy.ones((1, 16, 16), numpy.float32)
+        x = numpy.full((1, 16, 16), x_val, numpy.float32)
+        _, it, st, _ = gm.solve(d, g, create_otf_mask_shifted(), 0.0, max_iters=0, eps=1e-4,
+                                u0=x)
+        assert st[0] == expect and it[0] == 0

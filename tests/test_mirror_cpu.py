@@ -62,3 +62,5 @@ def test_mirror_stopping_rule_edge_cases():
         _, it, st, _ = gm.solve(d, g, create_otf_mask_shifted(), 0.0, max_iters=0, eps=1e-4,
                                 u0=x)
         assert st[0] == expect and it[0] == 0
+
+

@@ -59,16 +59,18 @@ FLOP_TRIAL = 2048
 FLOP_ITER_BASE = {"plain": 11264 + 1536 + 2304 + 2048, "plain_wg": 11264 + 1536 + 2304 + 2048,
                   "spectral": 11776 + 1536 + 2816 + 2048}
 FLOP_PER_PAIR = {"plain": 4 * 256 * 2, "plain_wg": 4 * 256 * 2, "spectral": 5 * 256 * 2}
-# Warp instructions per solver pass (one iteration or the initial gradient),
-# from the kernels' ncu captures on stack512 at 64 frames (profiles/*.md):
-# executed warp instructions / (tiles x passes).  Used for the issue-rate
-# bound, the one that limits these kernels.
+# Warp instructions per solver pass (one iteration or the initial gradient):
+# executed warp instructions / (tiles x passes) from one ncu capture of each
+# kernel on stack512 at 64 frames, at the commit named in WARP_INST_MEASURED.
+# Used for the issue-rate bound, the one that limits these kernels; a kernel
+# changed since that commit needs a new capture.
 WARP_INST_PER_PASS = {"spectral": 674715776 / (87616 * 6.0483),
                       "plain": 2546982558 / (87616 * 15.5539),
                       "plain_wg": 7479161369 / (87616 * 15.5538)}
 # multiply-adds x 2 of the warm-start network per 16x16 tile:
 # 256 px x 9 taps x (2*32 + 32*32 + 32*32 + 32*1)
 INFER_FLOP_PER_TILE = 2 * 256 * 9 * (2 * 32 + 32 * 32 + 32 * 32 + 32 * 1)
+WARP_INST_MEASURED = {"spectral": "3563395", "plain": "cf1c4d5", "plain_wg": "cf1c4d5"}
 KERNEL = {"plain": "ncs_warp_kernel", "plain_wg": "ncs_plain_kernel",
           "spectral": "ncs_spectral_kernel"}
 
@@ -300,11 +302,14 @@ def cpu_sample_frames(images_cpu, threads, budget_s=20.0):
     return min(images_cpu.shape[0], max(1, threads))
 
 
-def accuracy_gate(w, tile_cost, n_sample, seed=0, tile_u=None):
+def accuracy_gate(w, tile_cost, n_sample, seed=0, tile_u=None, out=None):
     """Per-tile final cost vs the FP64 Newton optimum (oracle) on a random
     sample of tiles: fraction within 1e-4 relative, max and median gap.
     tile_cost: the solver's own per-tile FP64 costs; or tile_u, the final
-    tiles [N, 16, 16], whose costs are then computed here in FP64."""
+    tiles [N, 16, 16], whose costs are then computed here in FP64.  With
+    ``out`` (the stitched result [T, H, W]) the sampled tiles' owned pixels
+    of it -- the interior pixels each tile writes last -- are also compared
+    with the optimum, relative to max(|u*|, 1)."""
     from oracle import numpy_ref as nr
     images = w["images"]
     T, H, W = images.shape
@@ -324,42 +329,91 @@ def accuracy_gate(w, tile_cost, n_sample, seed=0, tile_u=None):
         data.append(p[ox[i]:ox[i] + 16, oy[j]:oy[j] + 16])
         gms.append(gam[ox[i]:ox[i] + 16, oy[j]:oy[j] + 16])
     ms = numpy.fft.fftshift(w["mask"]).astype(numpy.float32).astype(numpy.float64)
-    _, fstar, _ = nr.newton_solve(numpy.array(data), numpy.array(gms), ms, w["alpha"])
+    ustar, fstar, _ = nr.newton_solve(numpy.array(data), numpy.array(gms), ms, w["alpha"])
     if tile_cost is None:
         tile_cost = numpy.zeros(T * per)
         tile_cost[idx] = nr.cost(tile_u[idx].astype(numpy.float64), numpy.array(data),
                                  numpy.array(gms), ms, w["alpha"])
     gap = nr.rel_cost_gap(tile_cost[idx], fstar)
-    return {"tiles_checked": int(idx.size), "frac_within_1e-4": float((gap <= 1e-4).mean()),
-            "max_rel_gap": float(gap.max()), "median_rel_gap": float(numpy.median(gap)),
-            "referee": "FP64 damped Newton (oracle/numpy_ref.py)"}
+    rec = {"tiles_checked": int(idx.size), "frac_within_1e-4": float((gap <= 1e-4).mean()),
+           "max_rel_gap": float(gap.max()), "median_rel_gap": float(numpy.median(gap)),
+           "referee": "FP64 damped Newton (oracle/numpy_ref.py)"}
+    if out is not None:
+        own_x = numpy.array([nr.owner_origin(y, ox) for y in range(H)])
+        own_y = numpy.array([nr.owner_origin(y, oy) for y in range(W)])
+        rel = []
+        frames = {}
+        for k, t in enumerate(idx):
+            f, rem = divmod(int(t), per)
+            i, j = divmod(rem, len(oy))
+            rows = numpy.nonzero(own_x == ox[i])[0]
+            cols = numpy.nonzero(own_y == oy[j])[0]
+            if f not in frames:
+                frames = {f: out[f].cpu().numpy().astype(numpy.float64)}
+            got = frames[f][numpy.ix_(rows, cols)]
+            ref = ustar[k][numpy.ix_(rows - ox[i] + 1, cols - oy[j] + 1)]
+            rel.append((numpy.abs(got - ref) / numpy.maximum(numpy.abs(ref), 1.0)).ravel())
+        rel = numpy.concatenate(rel)
+        rec["pixels"] = {"checked": int(rel.size), "max_rel": float(rel.max()),
+                         "median_rel": float(numpy.median(rel)),
+                         "frac_within_1e-3": float((rel <= 1e-3).mean()),
+                         "what": "owned pixels of the sampled tiles in the stitched result "
+                                 "vs the FP64 optimum, |u - u*| / max(|u*|, 1)"}
+    return rec
+
+
+def cpu_readings(images_cpu, gamma, mask_shifted, alpha, cap, threads):
+    """The reference C path (pyCNCS cReduceNoise) on bounded samples of the
+    workload, three ways: at the workload's iteration cap on all host
+    threads (one frame per thread), to convergence (max_iterations 0, the
+    reference's default) on the same frames, and capped on one core (one
+    frame).  Returns {reading: {value Mpx/s, cores, sample, seconds}}."""
+    T, H, W = images_cpu.shape
+    n = cpu_sample_frames(images_cpu, threads)
+    frames = [images_cpu[i].astype(numpy.float64) for i in range(n)]
+    out = {}
+    for name, fr, th, it in (("capped_all_cores", frames, threads, cap),
+                             ("unlimited_all_cores", frames, threads, 0),
+                             ("capped_one_core", frames[:1], 1, cap)):
+        wall, kind = cpu_reduce_frames(fr, gamma, mask_shifted, alpha, it, th)
+        out[name] = {"value": len(fr) * H * W / wall / 1e6, "unit": "Mpixel/s", "cores": th,
+                     "kind": kind, "seconds": wall,
+                     "sample": "%d of %d frames (%dx%d), one per thread, max_iterations=%s"
+                               % (len(fr), T, H, W, it if it else "0 (until convergence)")}
+    return out
 
 
 # --------------------------------------------------------------- arms -------
 
 def run_reference(args, world, rank):
+    """The reference arm: pyCNCS cReduceNoise (the reference's C path) on the
+    host cores, on bounded samples of the workload.  The workload is drawn
+    with torch alone (on the GPU when there is one), so this process never
+    loads this library's CUDA code."""
     if rank != 0:
         return 0
     from ncs_b200 import sim
-    w = sim.make_stack(args.workload, T=args.frames, device="cpu", seed=1234)
-    imgs = w["images"].numpy()
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    w = sim.make_stack(args.workload, T=args.frames, device=dev, seed=1234)
     threads = cpu_threads()
-    n = cpu_sample_frames(imgs, threads)
+    n = cpu_sample_frames(w["images"], threads)
+    imgs = w["images"][:n].cpu().numpy()
+    T = w["images"].shape[0]
+    gamma = w["gamma"].cpu().numpy()
     frames = [imgs[i].astype(numpy.float64) for i in range(n)]
     ms = numpy.fft.fftshift(w["mask"])
     for _ in range(args.warmup):
-        cpu_reduce_frames(frames, w["gamma"].numpy(), ms, w["alpha"], w["max_iters"], threads)
+        cpu_reduce_frames(frames, gamma, ms, w["alpha"], w["max_iters"], threads)
     walls = []
     kind = None
     for _ in range(args.steps):
-        wall, kind = cpu_reduce_frames(frames, w["gamma"].numpy(), ms, w["alpha"],
-                                       w["max_iters"], threads)
+        wall, kind = cpu_reduce_frames(frames, gamma, ms, w["alpha"], w["max_iters"], threads)
         walls.append(wall)
     H, W = imgs.shape[1:]
     value = n * H * W / (sum(walls) / len(walls)) / 1e6
     sample = ("%d of %d frames (%dx%d) per step, one frame per thread, pyCNCS cReduceNoise "
-              "FP64 with libLBFGS-API max_iterations=%d" % (n, imgs.shape[0], H, W,
-                                                            w["max_iters"]))
+              "FP64 with libLBFGS-API max_iterations=%d" % (n, T, H, W, w["max_iters"]))
+    readings = cpu_readings(imgs, gamma, ms, w["alpha"], w["max_iters"], threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpixel/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -367,7 +421,7 @@ def run_reference(args, world, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(w, args),
         "cpu_baseline": {"value": value, "unit": "Mpixel/s", "cores": threads, "kind": kind,
-                         "sample": sample},
+                         "sample": sample, "readings": readings},
         "e2e": {"value": value, "unit": "Mpixel/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -454,6 +508,9 @@ def run_ours(args, world, rank, local):
     # untimed statistics run: per-tile iterations / evaluations / final cost
     _, iters, status, cost, evals = solver.reduce_noise(images, gamma, out=out, tile_stats="all")
     torch.cuda.synchronize()
+    # the timed launches must reproduce this launch's result bit for bit, so
+    # that its per-tile costs are the costs of the timed output
+    stats_out = out.clone()
     iters_n = iters.double().sum().item()
     evals_n = evals.double().sum().item()
     n_tiles = iters.numel()
@@ -484,6 +541,9 @@ def run_ours(args, world, rank, local):
     clocks.end()
     barrier(world)
     clk = clocks.stop()
+    timed_equal = bool(torch.equal(out, stats_out))
+    assert timed_equal, "the timed launches differ from the statistics launch"
+    del stats_out
     per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[-1])
     total_ms = max_over_ranks(total_ms, world)
@@ -636,9 +696,11 @@ def run_ours(args, world, rank, local):
                                "achieved_warp_inst_per_s": inst_launch / (launch_ms / 1e3),
                                "peak_warp_inst_per_s": issue_peak,
                                "frac": inst_launch / (launch_ms / 1e3) / issue_peak,
-                               "source": "warp instructions per pass from the kernel's ncu "
-                                         "capture (profiles/) x passes counted in this run; "
-                                         "peak = SMs x 4 schedulers x sm_max_mhz"}},
+                               "source": "warp instructions per pass from one ncu capture "
+                                         "of the kernel on stack512 at 64 frames (commit %s) "
+                                         "x passes counted in this run; peak = SMs x 4 "
+                                         "schedulers x sm_max_mhz"
+                                         % WARP_INST_MEASURED[args.form]}},
         "e2e": {"value": e2e_value, "unit": "Mpixel/s",
                 "h2d_bytes_per_step": int(h_in.numel() * 4 + h_gamma.numel() * 4),
                 "d2h_bytes_per_step": int(h_out.numel() * 4),
@@ -655,18 +717,30 @@ def run_ours(args, world, rank, local):
             k: v for k, v in rec.items() if not k.startswith("_")}
     if warm is not None:
         line["warm_start"] = {k: v for k, v in warm.items() if not k.startswith("_")}
+    if warm is not None and "plain_wg" in plain:
+        # the metric's named comparison: the warm-start + tensor-core form
+        # against the plain GPU kernel (one warp group per tile), and the same
+        # ratio for the other forms on this stack
+        line["metric_form"] = {
+            "warm_tc_over_plain_gpu": warm["value"] / plain["plain_wg"]["value"],
+            "warm_tc_over_plain_gpu_warp": warm["value"] / plain["plain"]["value"],
+            "spectral_over_plain_gpu": value / plain["plain_wg"]["value"],
+            "target": ">= 3x the plain GPU kernel at equal accuracy"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
-        imgs = images.cpu().numpy()
-        n = cpu_sample_frames(imgs, threads)
-        frames = [imgs[i].astype(numpy.float64) for i in range(n)]
-        wall, kind = cpu_reduce_frames(frames, gamma.cpu().numpy(), numpy.fft.fftshift(w["mask"]),
-                                       w["alpha"], w["max_iters"], threads)
+        n = cpu_sample_frames(images, threads)
+        readings = cpu_readings(images[:n].cpu().numpy(), gamma.cpu().numpy(),
+                                numpy.fft.fftshift(w["mask"]), w["alpha"], w["max_iters"],
+                                threads)
+        cap = readings["capped_all_cores"]
         line["cpu_baseline"] = {
-            "value": n * H * W / wall / 1e6, "unit": "Mpixel/s", "cores": threads, "kind": kind,
+            "value": cap["value"], "unit": "Mpixel/s", "cores": threads, "kind": cap["kind"],
             "sample": "%d of %d frames, one per thread, pyCNCS cReduceNoise FP64, "
-                      "max_iterations=%d" % (n, T, w["max_iters"])}
-        line["accuracy"] = accuracy_gate(w, cost.cpu().numpy(), args.accuracy_tiles)
+                      "max_iterations=%d" % (n, T, w["max_iters"]),
+            "readings": readings}
+        line["accuracy"] = accuracy_gate(w, cost.cpu().numpy(), args.accuracy_tiles, out=out)
+        line["accuracy"]["timed_output"] = ("bit-identical to the statistics launch whose "
+                                            "per-tile costs are gated: %s" % timed_equal)
         for pform, rec in plain.items():
             key = "plain_gpu" if pform == "plain_wg" else "plain_gpu_warp"
             line[key]["accuracy"] = accuracy_gate(w, rec["_cost"], args.accuracy_tiles)
@@ -849,6 +923,15 @@ def run_mixed(args, world, rank, local):
     }
     if warm is not None:
         line["warm_start"] = {k: v for k, v in warm.items() if not k.startswith("_")}
+    if warm is not None and "plain_wg" in plain:
+        # the metric's named comparison: the warm-start + tensor-core form
+        # against the plain GPU kernel (one warp group per tile), and the same
+        # ratio for the other forms on this stack
+        line["metric_form"] = {
+            "warm_tc_over_plain_gpu": warm["value"] / plain["plain_wg"]["value"],
+            "warm_tc_over_plain_gpu_warp": warm["value"] / plain["plain"]["value"],
+            "spectral_over_plain_gpu": value / plain["plain_wg"]["value"],
+            "target": ">= 3x the plain GPU kernel at equal accuracy"}
     if rank == 0:
         line["accuracy"] = mixed_accuracy(stacks, stats["cost"].cpu().numpy(),
                                           args.accuracy_tiles)
@@ -1075,7 +1158,9 @@ def main():
                     help="timed steps (40 x ~2.3 ms gives the clock sampler a few samples)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="stack512")
+    ap.add_argument("--workload", default="sensor2048",
+                    help="sensor2048 (default: 100 x 2048^2, 60 chains, 0.5%% hot pixels), "
+                         "stack512, frame256, mixed, adu or normalized")
     ap.add_argument("--frames", type=int, default=None, help="override the frame count")
     ap.add_argument("--form", default="spectral", choices=sorted(KERNEL))
     ap.add_argument("--no-compare-plain", action="store_true",

@@ -1,7 +1,10 @@
 """ctypes binding of libncs_b200.so (C ABI in include/ncs_b200.h).
 
-The library is the only compute path: if it is missing or fails to load the
-import raises -- there is no CPU fallback.
+The library is the only compute path: importing the package raises if it is
+not built (require), and the first call that needs it loads it (load), which
+raises if it fails to load -- there is no CPU fallback.  Loading on first use
+keeps processes that only use the package's host-side helpers (the seeded
+workload generators) from mapping the library.
 """
 import ctypes
 import os
@@ -19,6 +22,8 @@ NCSB_ESCRATCH = -5
 MODE_PLAIN = 0
 MODE_PLAIN_WG = 1
 MODE_SPECTRAL = 2
+MODE_TC_TF32 = 3
+MODE_TC_BF16X3 = 4
 
 # raw-frame element types (NCSB_ADU_*)
 ADU_F32 = 0
@@ -123,6 +128,12 @@ EXPORTS = [
 ]
 
 _lib = None
+
+
+def require():
+    """Raise OSError unless the library has been built."""
+    if not os.path.exists(LIB_PATH):
+        raise OSError("libncs_b200.so is not built; run `python ncs_b200/build.py`")
 
 
 def load():

@@ -27,9 +27,13 @@ class NCSCException(Exception):
     pass
 
 
-def build():
-    """Compile the oracle libraries (the reference one only if its source exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+def build(ref_root=None):
+    """Compile the oracle libraries: the C port always, the reference's own
+    ncs.c and CUDA kernel only when ``ref_root`` names a reference tree."""
+    cmd = ["make", "-s", "-C", HERE]
+    if ref_root:
+        cmd.append("REF=" + ref_root)
+    subprocess.run(cmd, check=True)
 
 
 def _common(lib):

@@ -1,9 +1,9 @@
 """Generate the golden vectors in tests/golden/ from the reference itself.
 
-Run in a container that has the reference tree (default /root/reference) and
-the built oracle (``make -C oracle``):
+Run in a container that has the reference tree and the built oracle
+(``make -C oracle REF=REFERENCE_ROOT``):
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 
 Nothing at test time reads the reference tree; tests only read the .npz files
 written here.  Sources used (paths in the HuanglabPurdue/NCS tree):
@@ -161,7 +161,9 @@ def psf_vectors(ref):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    ref_root = args[0] if args else "/root/reference"
+    if not args:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT [--psf-only]")
+    ref_root = args[0]
     if "--psf-only" not in sys.argv:
         main(ref_root)
     psf_vectors(ref_root)

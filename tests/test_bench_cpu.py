@@ -32,3 +32,26 @@ def test_reference_arm_prints_one_contract_line():
     import torch
     from oracle import refgpu
     assert ("reference_gpu" in d) == (torch.cuda.is_available() and refgpu.available())
+    readings = cb["readings"]
+    assert set(readings) == {"capped_all_cores", "unlimited_all_cores", "capped_one_core"}
+    assert readings["capped_one_core"]["cores"] == 1
+    assert all(r["value"] > 0 for r in readings.values())
+
+
+def test_reference_arm_never_maps_this_library():
+    """The reference arm times only the reference's code: it draws its
+    workload with torch and must not load libncs_b200.so into its process."""
+    code = (
+        "import sys, os, io, contextlib\n"
+        "sys.path.insert(0, %r)\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'frame256',\n"
+        "            '--steps', '1', '--warmup', '0', '--no-compare-plain']\n"
+        "import bench\n"
+        "with contextlib.redirect_stdout(io.StringIO()):\n"
+        "    rc = bench.main()\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('MAPPED' if 'libncs_b200.so' in maps else 'CLEAN', rc)\n" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().splitlines()[-1] == "CLEAN 0", r.stdout

@@ -8,6 +8,8 @@ matrix form u'Qu / sum(u) the kernel uses, its gradient and Hessian against
 central finite differences, and the product's odd-size genfilter against the
 oracle's.
 """
+import math
+
 import numpy
 import pytest
 
@@ -105,3 +107,35 @@ def test_product_mask_functions_match_the_oracle():
     assert numpy.allclose(otf.normalized_mask(0.1, 1.4, 0.7), nr.default_mask(0.1, 1.4, 0.7))
     m = otf.normalized_mask(0.1, 1.4, 0.7)
     assert m[1, 1] == 0.0 and numpy.allclose(m, m.T) and numpy.allclose(m, m[::-1, ::-1])
+
+
+# A known answer derived by hand from calcost.m:36-53 for one 3 x 3 segment.
+# u = d = [[2, 3, 1], [1, 1, 1], [1, 1, 1]], gamma = var / gain^2 = 2 / 1,
+# alpha = 1/2, centred mask M = [[1, 2, 1], [1, 1/2, 1], [1, 2, 1]].
+#   likelihood = sum(u - (d + gamma) log(u + gamma))
+#              = (2 - 4 ln 4) + (3 - 5 ln 5) + 7 (1 - 3 ln 3)
+#   fft2(u): u - 1 has 1 at (0, 0) and 2 at (0, 1), so
+#   F(k1, k2) = 9 [k = 0] + 1 + 2 exp(-2 pi i k2 / 3):  |F(0, 0)| = 12,
+#   |F(k1, 0)| = 3 for k1 = 1, 2, and |F(k1, k2)| = sqrt(3) for k2 = 1, 2.
+#   fftshift moves frequency k to centred index (k + 1) mod 3 on each axis,
+#   so |F| / 3 is 4 at M[1][1] = 1/2, 1 at M[0][1] = M[2][1] = 2, and
+#   1 / sqrt(3) at the six entries of columns 0 and 2 (all 1):
+#   sum((|F| / 3 M)^2) = 16 / 4 + 2 * 4 + 6 / 3 = 14, sum(u) = 12,
+#   noisepart = 14 / 12 = 7 / 6;
+#   fcost = 2 likelihood / 9 + alpha 7 / 6.
+KNOWN_U = [[2.0, 3.0, 1.0], [1.0, 1.0, 1.0], [1.0, 1.0, 1.0]]
+KNOWN_MASK = [[1.0, 2.0, 1.0], [1.0, 0.5, 1.0], [1.0, 2.0, 1.0]]
+KNOWN_COST = (2.0 / 9.0) * (12.0 - 4.0 * math.log(4.0) - 5.0 * math.log(5.0)
+                            - 21.0 * math.log(3.0)) + 0.5 * 7.0 / 6.0
+
+
+def test_cost_known_answer_from_calcost():
+    """The oracle's cost equals the value derived by hand above, line by line
+    from calcost.m; a transposed mask (the wrong fftshift orientation) gives
+    a different value, so the orientation is pinned too."""
+    from oracle import normalized_ref as nr
+    u = numpy.array(KNOWN_U)
+    mask = numpy.array(KNOWN_MASK)
+    assert abs(nr.noise(u, mask) - 7.0 / 6.0) <= 1e-14
+    assert abs(nr.cost(u, u, 2.0, mask, 0.5) - KNOWN_COST) <= 1e-13 * abs(KNOWN_COST)
+    assert abs(nr.noise(u, mask.T) - 7.0 / 6.0) > 0.1

@@ -52,3 +52,21 @@ def test_camera_map_distributions():
     # hot pixels: a fraction of the variance map scaled by 50
     _, _, vh = sim.camera_maps(512, 512, numpy.random.default_rng(1), hot=0.005)
     assert 0.003 < numpy.mean(vh > 1000.0) < 0.008
+
+
+def test_ideal_image_restatement_matches_the_reference_simulator():
+    """oracle/sim_ref.py's genidealimage restatement against the reference's
+    own genidealimage outputs (tests/golden/sim_vectors.npz, written by
+    make_sim_golden.py from denoisetools.py and randwlcposition.mat): grids
+    of 32-128 pixels, zoom 1-8, three numerical apertures."""
+    import os
+    from oracle import sim_ref
+    d = numpy.load(os.path.join(os.path.dirname(__file__), "golden", "sim_vectors.npz"))
+    cases = [k[:-len("_params")] for k in d.files if k.endswith("_params")]
+    assert len(cases) == 4
+    for key in cases:
+        R, zoom, px, na, lam = d[key + "_params"]
+        img, k = sim_ref.ideal_image(d["xcor"], d["ycor"], int(R), px, int(zoom), na, lam)
+        assert numpy.abs(k - d[key + "_kernel"]).max() <= 1e-15
+        ref = d[key + "_img"]
+        assert numpy.abs(img - ref).max() <= 1e-12 * numpy.abs(ref).max(), key

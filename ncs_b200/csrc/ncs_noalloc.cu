@@ -12,8 +12,12 @@
 //
 // The scratch array is shared by every call on a device and keeps the last
 // call's contents; each call re-initialises the work counter and the mask
-// table on its own stream before the launch.  Calls that overlap on the GPU
-// (two streams, or two host threads) race on it.
+// table on its own stream before the launch, with a one-block kernel that
+// receives the table by value (no host-to-device copy, so the host never
+// waits for the stream).  Calls that overlap on the GPU (two streams, or two
+// host threads) race on it.  The device address of the array is looked up
+// once per device and kept for the life of the process, so the entry must
+// not be used across cudaDeviceReset on that device.
 #include <cmath>
 #include <mutex>
 
@@ -23,8 +27,8 @@
 namespace ncsb {
 cudaError_t launch_plain(const SolveArgs& args, int grid, cudaStream_t stream);
 int plain_max_ctas_per_sm();
-cudaError_t launch_warp(const SolveArgs& args, int grid, cudaStream_t stream);
-int warp_max_ctas_per_sm(int m);
+cudaError_t launch_warp_blocks(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
+int warp_max_ctas_per_sm(int m, int blocks);
 cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
 int spectral_max_ctas_per_sm(int m, int blocks, bool warm, bool batch);
 }  // namespace ncsb
@@ -34,7 +38,8 @@ using ncsb::tiles_along;
 namespace {
 
 // Layout of the static scratch: [0, 8) work counter, [256, 1280) the
-// 256-entry M^2/256 table in the kernel's spectral layout.  Capacity is
+// 256-entry M^2/256 table in natural [kr][kc] order (the table
+// ncsb_set_otf_mask builds; each kernel remaps it to its own layout).  Capacity is
 // NCSB_NOALLOC_SCRATCH_BYTES (4 KiB); every GPU that loads the library holds
 // it until the process exits.
 constexpr size_t kQueueOffset = 0;
@@ -50,6 +55,18 @@ struct DeviceSetup {
     int num_sms = 0;
     int ctas_per_sm = 0;
 };
+
+// The M^2/256 table travels as a kernel argument (1 KiB, by value).
+struct TableArg {
+    float v[ncsb::kPix];
+};
+
+// Writes the mask table into the scratch array and resets the work counter.
+__global__ void noalloc_init_kernel(TableArg table, unsigned char* scratch) {
+    float* dst = reinterpret_cast<float*>(scratch + kTableOffset);
+    for (int i = threadIdx.x; i < ncsb::kPix; i += blockDim.x) dst[i] = table.v[i];
+    if (threadIdx.x == 0) *reinterpret_cast<unsigned long long*>(scratch + kQueueOffset) = 0ull;
+}
 
 constexpr int kMaxDevices = 64;
 DeviceSetup g_setup[kMaxDevices];
@@ -110,22 +127,19 @@ extern "C" int ncsb_reduce_noise_noalloc(const ncsb_params* p, const float* mask
 
     // M^2 symmetrised over k -> -k and scaled by 1/256, natural order (the
     // table ncsb_set_otf_mask builds).
-    float table[ncsb::kPix];
+    TableArg table;
     for (int kr = 0; kr < 16; ++kr) {
         for (int kc = 0; kc < 16; ++kc) {
             const double a = mask_shifted_host[kr * 16 + kc];
             const double b = mask_shifted_host[((16 - kr) & 15) * 16 + ((16 - kc) & 15)];
             if (!std::isfinite(a) || !std::isfinite(b)) return NCSB_EINVAL;
-            table[kr * 16 + kc] = (float)(0.5 * (a * a + b * b) / 256.0);
+            table.v[kr * 16 + kc] = (float)(0.5 * (a * a + b * b) / 256.0);
         }
     }
     cudaStream_t s = (cudaStream_t)stream;
     unsigned char* scratch = dev->scratch;
-    if (cudaMemcpyAsync(scratch + kTableOffset, table, kTableBytes, cudaMemcpyHostToDevice, s) !=
-        cudaSuccess)
-        return NCSB_ECUDA;
-    if (cudaMemsetAsync(scratch + kQueueOffset, 0, sizeof(unsigned long long), s) != cudaSuccess)
-        return NCSB_ECUDA;
+    noalloc_init_kernel<<<1, 256, 0, s>>>(table, scratch);
+    if (cudaGetLastError() != cudaSuccess) return NCSB_ECUDA;
 
     ncsb::SolveArgs a{};
     a.tile_mode = 0;
@@ -158,7 +172,7 @@ extern "C" int ncsb_reduce_noise_noalloc(const ncsb_params* p, const float* mask
                            ? p->ctas_per_sm
                            : (wg ? dev->ctas_per_sm
                                  : (spec ? ncsb::spectral_max_ctas_per_sm(a.m, 0, false, false)
-                                         : ncsb::warp_max_ctas_per_sm(a.m)));
+                                         : ncsb::warp_max_ctas_per_sm(a.m, 0)));
     const long long tiles_per_cta = wg ? 1 : 4;
     long long grid = (long long)per_sm * dev->num_sms;
     if (grid > (a.n_tiles + tiles_per_cta - 1) / tiles_per_cta)
@@ -166,6 +180,6 @@ extern "C" int ncsb_reduce_noise_noalloc(const ncsb_params* p, const float* mask
     if (grid < 1) grid = 1;
     const cudaError_t e = wg     ? ncsb::launch_plain(a, (int)grid, s)
                           : spec ? ncsb::launch_spectral(a, (int)grid, p->ctas_per_sm, s)
-                                 : ncsb::launch_warp(a, (int)grid, s);
+                                 : ncsb::launch_warp_blocks(a, (int)grid, p->ctas_per_sm, s);
     return e == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
 }

@@ -7,9 +7,11 @@ that bans cudaMalloc after start-up because it can synchronise the device);
 they cannot create a handle, so the work counter and the mask table live in
 a static device array instead.  Here it is called through the C ABI twice in
 a row, with different stacks and masks so the second call cannot lean on the
-first call's leftovers, and each result must equal what the handle-based
-ncsb_reduce_noise returns for the same inputs: the same kernel runs, so
-pixels, iteration counts, statuses and costs must agree exactly.
+first call's leftovers, in every solver mode and with a fixed CTA count, and
+each result must equal what the handle-based ncsb_reduce_noise returns for
+the same inputs: the same kernel runs, so pixels, iteration counts, statuses
+and costs must agree exactly.  A last case records the call in a CUDA graph
+and replays it.
 
 The no-alloc call comes first in each case, so in a fresh process it also
 exercises the one-time per-device set-up.  This file is named to be
@@ -38,9 +40,25 @@ def _case(seed, T, H, W):
     return images, gamma, numpy.ascontiguousarray(mask)
 
 
-def test_noalloc_matches_handle_entry_point_twice(cuda_ok):
+def _noalloc(lib, params, mask, x, g, out, it, st, cost, stream):
+    from ncs_b200 import _lib
+    T, H, W = x.shape
+    return lib.ncsb_reduce_noise_noalloc(
+        ctypes.byref(params), mask.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _ptr(x),
+        T, H, W, _ptr(g), 0, _ptr(out), _ptr(it), _ptr(st), _ptr(cost), None,
+        ctypes.c_void_p(stream.cuda_stream))
+
+
+# (mode, history size m, resident CTAs per SM; 0 = the library's choice)
+MODES = [("spectral", 1, 0), ("plain", 4, 0), ("plain_wg", 4, 0), ("spectral", 2, 3),
+         ("plain", 2, 2)]
+
+
+@pytest.mark.parametrize("mode,m,ctas", MODES)
+def test_noalloc_matches_handle_entry_point_twice(cuda_ok, mode, m, ctas):
     import ncs_b200
     from ncs_b200 import _lib
+    from ncs_b200.ncs import _MODES
     lib = _lib.load()
     cases = [(_case(1, 3, 45, 61), 0.2, 25), (_case(2, 2, 70, 33), 0.35, 40)]
     for (images, gamma, mask), alpha, cap in cases:
@@ -51,19 +69,18 @@ def test_noalloc_matches_handle_entry_point_twice(cuda_ok):
         params = _lib.default_params()
         params.alpha = alpha
         params.max_iters = cap
+        params.mode = _MODES[mode]
+        params.m = m
+        params.ctas_per_sm = ctas
         out = torch.full_like(x, -1.0)
         it = torch.full((n,), -9, dtype=torch.int32, device="cuda")
         st = torch.full((n,), -9, dtype=torch.int32, device="cuda")
         cost = torch.zeros(n, dtype=torch.float64, device="cuda")
         stream = torch.cuda.current_stream()
-        rc = lib.ncsb_reduce_noise_noalloc(
-            ctypes.byref(params), mask.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _ptr(x),
-            T, H, W, _ptr(g), 0, _ptr(out), _ptr(it), _ptr(st), _ptr(cost), None,
-            ctypes.c_void_p(stream.cuda_stream))
-        assert rc == _lib.NCSB_OK
+        assert _noalloc(lib, params, mask, x, g, out, it, st, cost, stream) == _lib.NCSB_OK
         torch.cuda.synchronize()
 
-        s = ncs_b200.Solver(alpha=alpha, max_iters=cap)
+        s = ncs_b200.Solver(alpha=alpha, max_iters=cap, mode=mode, m=m, ctas_per_sm=ctas)
         s.set_otf_mask_shifted(mask)
         ref, rit, rst, rcost = s.reduce_noise(x, g, tile_stats=True)
         torch.cuda.synchronize()
@@ -73,6 +90,51 @@ def test_noalloc_matches_handle_entry_point_twice(cuda_ok):
         assert torch.equal(cost, rcost)
         assert set(st.cpu().numpy().tolist()) <= {0, -2}
         s.close()
+
+
+def test_noalloc_captured_in_a_graph_and_replayed(cuda_ok):
+    """The call enqueues only kernels (the mask table goes to the device as a
+    kernel argument), so it can be recorded in a CUDA graph after its first,
+    set-up call; each replay re-initialises the scratch and gives the handle
+    entry's result."""
+    import ncs_b200
+    from ncs_b200 import _lib
+    lib = _lib.load()
+    images, gamma, mask = _case(3, 2, 40, 52)
+    T, H, W = images.shape
+    n = _lib.num_tiles(T, H, W)
+    x = torch.from_numpy(images).cuda()
+    g = torch.from_numpy(gamma).cuda()
+    params = _lib.default_params()
+    params.max_iters = 30
+    out = torch.zeros_like(x)
+    it = torch.zeros(n, dtype=torch.int32, device="cuda")
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    cost = torch.zeros(n, dtype=torch.float64, device="cuda")
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):  # set-up call, outside the capture
+        assert _noalloc(lib, params, mask, x, g, out, it, st, cost, side) == _lib.NCSB_OK
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        rc = _noalloc(lib, params, mask, x, g, out, it, st, cost,
+                      torch.cuda.current_stream())
+    assert rc == _lib.NCSB_OK
+    s = ncs_b200.Solver(max_iters=30)
+    s.set_otf_mask_shifted(mask)
+    ref, rit, rst, rcost = s.reduce_noise(x, g, tile_stats=True)
+    for _ in range(2):
+        out.fill_(-1.0)
+        it.fill_(-9)
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(out, ref)
+        assert torch.equal(it, rit)
+        assert torch.equal(st, rst)
+        assert torch.equal(cost, rcost)
+    del graph
+    s.close()
 
 
 def test_noalloc_rejects_bad_arguments(cuda_ok):

@@ -59,6 +59,9 @@ FLOP_TRIAL = 2048
 FLOP_ITER_BASE = {"plain": 11264 + 1536 + 2304 + 2048, "plain_wg": 11264 + 1536 + 2304 + 2048,
                   "spectral": 11776 + 1536 + 2816 + 2048}
 FLOP_PER_PAIR = {"plain": 4 * 256 * 2, "plain_wg": 4 * 256 * 2, "spectral": 5 * 256 * 2}
+# the tensor-core forms run the spectral algorithm (transforms on the tensor cores)
+for _f in ("tc_tf32", "tc_bf16x3"):
+    FLOP_ITER_BASE[_f], FLOP_PER_PAIR[_f] = FLOP_ITER_BASE["spectral"], FLOP_PER_PAIR["spectral"]
 # Warp instructions per solver pass (one iteration or the initial gradient):
 # executed warp instructions / (tiles x passes) from one ncu capture of each
 # kernel on stack512 at 64 frames, at the commit named in WARP_INST_MEASURED.
@@ -72,7 +75,17 @@ WARP_INST_PER_PASS = {"spectral": 674715776 / (87616 * 6.0483),
 INFER_FLOP_PER_TILE = 2 * 256 * 9 * (2 * 32 + 32 * 32 + 32 * 32 + 32 * 1)
 WARP_INST_MEASURED = {"spectral": "3563395", "plain": "cf1c4d5", "plain_wg": "cf1c4d5"}
 KERNEL = {"plain": "ncs_warp_kernel", "plain_wg": "ncs_plain_kernel",
-          "spectral": "ncs_spectral_kernel"}
+          "spectral": "ncs_spectral_kernel", "tc_tf32": "ncs_tc_kernel<TF32>",
+          "tc_bf16x3": "ncs_tc_kernel<BF16x3>"}
+# Tensor-core forms: MMA FLOPs executed per tile and pass (one transform pair),
+# from the four GEMM stages over 8 tiles (M = 128): stage 1 N 16 x K 16,
+# stages 2 and 3 N 32 x K 32, stage 4 N 16 x K 24 (TF32) or K 32 (BF16); the
+# three-way BF16 split runs every product three times.  The algorithmic
+# figure of a dense 256 x 256 Q-apply is 2 x 256 x 256 = 131,072 per pass.
+TC_EXEC_FLOP_PER_PASS = {
+    "tc_tf32": 2 * 128 * (16 * 16 + 2 * 32 * 32 + 16 * 24) // 8,
+    "tc_bf16x3": 3 * 2 * 128 * (16 * 16 + 2 * 32 * 32 + 16 * 32) // 8}
+DENSE_Q_FLOP_PER_PASS = 2 * 256 * 256
 
 
 def peaks():
@@ -362,6 +375,44 @@ def accuracy_gate(w, tile_cost, n_sample, seed=0, tile_u=None, out=None):
     return rec
 
 
+def tile_solver_gate(w, solver, n_sample, seed=0, u0_all=None):
+    """accuracy_gate for a form whose reported cost is its running value (the
+    tensor-core forms): the sampled tiles are solved again through the tile
+    entry (which gives the stack path's results exactly) and their exact
+    FP64 costs at the returned u are gated."""
+    from oracle import numpy_ref as nr
+    images = w["images"]
+    T, H, W = images.shape
+    ox, oy = nr.tile_origins(H), nr.tile_origins(W)
+    per = len(ox) * len(oy)
+    rng = numpy.random.default_rng(seed)
+    idx = numpy.sort(rng.choice(T * per, size=min(n_sample, T * per), replace=False))
+    gam = numpy.pad(w["gamma"].cpu().numpy(), 1, "edge")
+    data, gms = [], []
+    for t in idx:
+        f, rem = divmod(int(t), per)
+        i, j = divmod(rem, len(oy))
+        p = numpy.pad(images[f].cpu().numpy(), 1, "edge")
+        data.append(p[ox[i]:ox[i] + 16, oy[j]:oy[j] + 16])
+        gms.append(gam[ox[i]:ox[i] + 16, oy[j]:oy[j] + 16])
+    data = numpy.ascontiguousarray(numpy.array(data, dtype=numpy.float32))
+    gms = numpy.ascontiguousarray(numpy.array(gms, dtype=numpy.float32))
+    u0 = None
+    if u0_all is not None:
+        u0 = u0_all[torch.from_numpy(idx).to(u0_all.device)].contiguous()
+    u, _, _, _ = solver.solve_tiles(torch.from_numpy(data).to(images.device),
+                                    torch.from_numpy(gms).to(images.device), u0=u0)
+    ms = numpy.fft.fftshift(w["mask"]).astype(numpy.float32).astype(numpy.float64)
+    d64, g64 = data.astype(numpy.float64), gms.astype(numpy.float64)
+    _, fstar, _ = nr.newton_solve(d64, g64, ms, w["alpha"])
+    f = nr.cost(u.cpu().numpy().astype(numpy.float64), d64, g64, ms, w["alpha"])
+    gap = nr.rel_cost_gap(f, fstar)
+    return {"tiles_checked": int(idx.size), "frac_within_1e-4": float((gap <= 1e-4).mean()),
+            "max_rel_gap": float(gap.max()), "median_rel_gap": float(numpy.median(gap)),
+            "referee": "FP64 damped Newton (oracle/numpy_ref.py), exact cost at the "
+                       "returned tiles"}
+
+
 def cpu_readings(images_cpu, gamma, mask_shifted, alpha, cap, threads):
     """The reference C path (pyCNCS cReduceNoise) on bounded samples of the
     workload, three ways: at the workload's iteration cap on all host
@@ -604,6 +655,50 @@ def run_ours(args, world, rank, local):
                             "_cost": p_cost.cpu().numpy()}
             ps.close()
 
+    # the tensor-core forms on the same stack: the spectral algorithm with the
+    # noise term's transforms as tcgen05 GEMMs (TF32; three-way BF16 split)
+    tcforms = {}
+    pk0 = peaks()[0]
+    bf16_peak = pk0.get("bf16_tflops", 1590.0)
+    if not args.no_compare_plain and args.form == "spectral":
+        for tform in ("tc_tf32", "tc_bf16x3"):
+            ts_ = ncs_b200.Solver(alpha=w["alpha"], max_iters=w["max_iters"], mode=tform)
+            ts_.set_otf_mask(w["mask"])
+            _, t_it, t_st = ts_.reduce_noise(images, gamma, out=out, tile_stats="status")
+            ts_.reduce_noise(images, gamma, out=out)
+            barrier(world)
+            torch.cuda.synchronize()
+            te0, te1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ntc = max(1, min(args.steps, 5))
+            te0.record(stream)
+            for _ in range(ntc):
+                ts_.reduce_noise(images, gamma, out=out)
+            te1.record(stream)
+            torch.cuda.synchronize()
+            t_ms = max_over_ranks(te0.elapsed_time(te1), world) / ntc
+            passes = t_it.double().sum().item() + n_tiles
+            exec_tflops = passes * TC_EXEC_FLOP_PER_PASS[tform] / (t_ms / 1e3) / 1e12
+            peak_t = bf16_peak if tform == "tc_bf16x3" else 0.5 * bf16_peak
+            st_t = t_st.cpu().numpy()
+            tcforms[tform] = {
+                "form": "%s (spectral algorithm, m=1)" % tform, "kernel": KERNEL[tform],
+                "ms_per_step": t_ms, "value": px / (t_ms / 1e3) / 1e6,
+                "mean_iters": t_it.double().mean().item(),
+                "status": {str(k): int((st_t == k).sum()) for k in range(-5, 1)
+                           if (st_t == k).any()},
+                "vs_spectral_fft": (total_ms / args.steps) / t_ms,
+                "tensor": {"executed_flop_per_pass": TC_EXEC_FLOP_PER_PASS[tform],
+                           "dense_q_flop_per_pass": DENSE_Q_FLOP_PER_PASS,
+                           "executed_tflops": exec_tflops,
+                           "dense_q_equiv_tflops": passes * DENSE_Q_FLOP_PER_PASS
+                           / (t_ms / 1e3) / 1e12,
+                           "peak_tflops": peak_t,
+                           "frac": exec_tflops / peak_t,
+                           "peak_source": "dense BF16 measured burst%s"
+                                          % ("" if tform == "tc_bf16x3"
+                                             else " x 1/2 (TF32 runs at half the BF16 rate)")},
+                "_solver": ts_}
+
     # learned warm start: network inference on the stack, then the spectral
     # solve from its proposals (fallback to the photon image per tile)
     warm = None
@@ -656,13 +751,41 @@ def run_ours(args, world, rank, local):
                 "infer_flop_per_tile": INFER_FLOP_PER_TILE,
                 "speedup_vs_photon_start": (total_ms / args.steps) / tot_ms,
                 "_cost": w_cost.cpu().numpy()}
+        # the warm start with a tensor-core solve: tensor-core inference, then
+        # the TF32 tensor-core form from its proposals
+        if "tc_tf32" in tcforms:
+            tsv = tcforms["tc_tf32"]["_solver"]
+            _, wt_it, wt_st, _, _, wt_fb = tsv.reduce_noise_from(images, gamma, u0, out=out)
+            barrier(world)
+            torch.cuda.synchronize()
+            wt = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nws + 1)]
+            wt[0].record(stream)
+            for k in range(nws):
+                net.propose_stack_tc(images, gamma, out=u0)
+                wt[2 * k + 1].record(stream)
+                tsv.reduce_noise_from(images, gamma, u0, out=out)
+                wt[2 * k + 2].record(stream)
+            torch.cuda.synchronize()
+            wt_tot = max_over_ranks(wt[0].elapsed_time(wt[-1]), world) / nws
+            wt_sol = sum(wt[2 * k + 1].elapsed_time(wt[2 * k + 2]) for k in range(nws)) / nws
+            st_w = wt_st.cpu().numpy()
+            warm["tc_form"] = {
+                "kernels": "ncsb::nettc::infer_tc, ncs_tc_kernel<TF32, Warm>",
+                "ms_per_step": wt_tot, "ms_solve": wt_sol,
+                "value": px / (wt_tot / 1e3) / 1e6,
+                "mean_iters": wt_it.double().mean().item(),
+                "fallback_frac": wt_fb.double().mean().item(),
+                "status": {str(k): int((st_w == k).sum()) for k in range(-5, 1)
+                           if (st_w == k).any()},
+                "_u0": u0.clone()}
         del u0
 
     pk, pk_src = peaks()
     n_sms = torch.cuda.get_device_properties(dev).multi_processor_count
     fp32_peak = fp32_peak_tflops(pk.get("sm_max_mhz", 1965.0), n_sms)
     launch_ms = statistics.mean(per_step)
-    inst_launch = WARP_INST_PER_PASS[args.form] * (iters_n + n_tiles)
+    wipp = WARP_INST_PER_PASS.get(args.form)
+    inst_launch = wipp * (iters_n + n_tiles) if wipp else None
     issue_peak = n_sms * 4 * pk.get("sm_max_mhz", 1965.0) * 1e6
     achieved = flops / (launch_ms / 1e3) / 1e12
     traffic = None
@@ -692,7 +815,7 @@ def run_ours(args, world, rank, local):
                      "hbm": {"algorithmic_bytes": alg_bytes,
                              "achieved_gbs": alg_bytes / (launch_ms / 1e3) / 1e9,
                              "peak_gbs": pk.get("hbm_gbs")},
-                     "issue": {"est_warp_inst_per_launch": inst_launch,
+                     "issue": None if not wipp else {"est_warp_inst_per_launch": inst_launch,
                                "achieved_warp_inst_per_s": inst_launch / (launch_ms / 1e3),
                                "peak_warp_inst_per_s": issue_peak,
                                "frac": inst_launch / (launch_ms / 1e3) / issue_peak,
@@ -700,7 +823,7 @@ def run_ours(args, world, rank, local):
                                          "of the kernel on stack512 at 64 frames (commit %s) "
                                          "x passes counted in this run; peak = SMs x 4 "
                                          "schedulers x sm_max_mhz"
-                                         % WARP_INST_MEASURED[args.form]}},
+                                         % WARP_INST_MEASURED.get(args.form)}},
         "e2e": {"value": e2e_value, "unit": "Mpixel/s",
                 "h2d_bytes_per_step": int(h_in.numel() * 4 + h_gamma.numel() * 4),
                 "d2h_bytes_per_step": int(h_out.numel() * 4),
@@ -715,8 +838,14 @@ def run_ours(args, world, rank, local):
     for pform, rec in plain.items():
         line["plain_gpu" if pform == "plain_wg" else "plain_gpu_warp"] = {
             k: v for k, v in rec.items() if not k.startswith("_")}
+    if tcforms:
+        line["tensor_core_forms"] = {f_: {k: v for k, v in rec.items() if not k.startswith("_")}
+                                     for f_, rec in tcforms.items()}
     if warm is not None:
         line["warm_start"] = {k: v for k, v in warm.items() if not k.startswith("_")}
+        if "tc_form" in warm:
+            line["warm_start"]["tc_form"] = {k: v for k, v in warm["tc_form"].items()
+                                             if not k.startswith("_")}
     if warm is not None and "plain_wg" in plain:
         # the metric's named comparison: the warm-start + tensor-core form
         # against the plain GPU kernel (one warp group per tile), and the same
@@ -726,6 +855,12 @@ def run_ours(args, world, rank, local):
             "warm_tc_over_plain_gpu_warp": warm["value"] / plain["plain"]["value"],
             "spectral_over_plain_gpu": value / plain["plain_wg"]["value"],
             "target": ">= 3x the plain GPU kernel at equal accuracy"}
+        if "tc_form" in warm:
+            line["metric_form"]["warm_tc_form_over_plain_gpu"] = (
+                warm["tc_form"]["value"] / plain["plain_wg"]["value"])
+        for f_, rec in tcforms.items():
+            line["metric_form"]["%s_over_plain_gpu" % f_] = (
+                rec["value"] / plain["plain_wg"]["value"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         n = cpu_sample_frames(images, threads)
@@ -746,6 +881,15 @@ def run_ours(args, world, rank, local):
             line[key]["accuracy"] = accuracy_gate(w, rec["_cost"], args.accuracy_tiles)
         if warm is not None:
             line["warm_start"]["accuracy"] = accuracy_gate(w, warm["_cost"], args.accuracy_tiles)
+        for f_, rec in tcforms.items():
+            line["tensor_core_forms"][f_]["accuracy"] = tile_solver_gate(
+                w, rec["_solver"], args.accuracy_tiles)
+        if warm is not None and "tc_form" in warm:
+            line["warm_start"]["tc_form"]["accuracy"] = tile_solver_gate(
+                w, tcforms["tc_tf32"]["_solver"], args.accuracy_tiles,
+                u0_all=warm["tc_form"]["_u0"])
+    for rec in tcforms.values():
+        rec["_solver"].close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -923,15 +1067,6 @@ def run_mixed(args, world, rank, local):
     }
     if warm is not None:
         line["warm_start"] = {k: v for k, v in warm.items() if not k.startswith("_")}
-    if warm is not None and "plain_wg" in plain:
-        # the metric's named comparison: the warm-start + tensor-core form
-        # against the plain GPU kernel (one warp group per tile), and the same
-        # ratio for the other forms on this stack
-        line["metric_form"] = {
-            "warm_tc_over_plain_gpu": warm["value"] / plain["plain_wg"]["value"],
-            "warm_tc_over_plain_gpu_warp": warm["value"] / plain["plain"]["value"],
-            "spectral_over_plain_gpu": value / plain["plain_wg"]["value"],
-            "target": ">= 3x the plain GPU kernel at equal accuracy"}
     if rank == 0:
         line["accuracy"] = mixed_accuracy(stacks, stats["cost"].cpu().numpy(),
                                           args.accuracy_tiles)

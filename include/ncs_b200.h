@@ -62,6 +62,14 @@ extern "C" {
 #define NCSB_MODE_PLAIN_WG 1  /* FP32 SIMT, one warp group per tile (comparison form) */
 #define NCSB_MODE_SPECTRAL 2  /* FP32 SIMT, one warp per tile, L-BFGS with the spectral
                                  initial inverse Hessian (lambda I + 2 alpha Q)^-1; m <= 4 */
+/* Tensor-core forms: the spectral form's algorithm with every 16x16 transform
+   of the noise term Q u = (1/256) F^H diag(M^2) F u (and of the initial
+   inverse Hessian) done as four tcgen05 GEMMs over 8 tiles at a time, FP32
+   accumulation; m = 1.  They replace the FFT noise term and its gradient of
+   cuda/ncs.cu:743-817 and clib/pyCNCS/ncs.c:220-299.  The per-tile cost they
+   report is the solver's running value (v = 2 alpha Q u kept by updates). */
+#define NCSB_MODE_TC_TF32 3   /* TF32 operands */
+#define NCSB_MODE_TC_BF16X3 4 /* three-way BF16 split: hi*hi + lo*hi + hi*lo */
 
 /* Tile geometry is fixed: 16x16 tiles, 14x14 interiors, stride 14. */
 #define NCSB_TILE 16
@@ -262,7 +270,7 @@ int ncsb_genfilter(const ncsb_optics *optics, int n, float *masks_centred, void 
  * the device, FP64: pupil = |k| on the centred R x R grid (genkspace), 0 above
  * NA / lambda; PSF = |fftshift(fft2(pupil))|^2 normalised to unit sum;
  * OTF = |fftshift(ifft2(PSF))| normalised to unit maximum.  Outputs are device
- * [R][R] FP32 arrays, any of them NULL to skip; 2 <= R <= 256. */
+ * [R][R] FP32 arrays, any of them NULL to skip; 2 <= R <= 1024. */
 int ncsb_genpsfparam(int R, double pixel_size, double na, double wavelength, float *psf,
                      float *pupil, float *otf, void *stream);
 
@@ -289,6 +297,16 @@ int ncsb_sim_render(const float *emitters_sorted, const int *cell_start, int hei
 int ncsb_sim_camera(const float *ideal, int n_frames, int height, int width, const float *offset,
                     const float *gain, const float *variance, uint64_t seed, float *adu,
                     float *photo_electrons, void *stream);
+
+/* The reference simulator's ideal image (genidealimage,
+ * python3-6/pyNCS/denoisetools.py:150-186): n positions (xs -> row, ys ->
+ * column) already on the fine grid of (R zoom)^2 pixels, their occupancy,
+ * the 'same' convolution with the ksz x ksz PSF kernel (the centre of
+ * genpsfparam's PSF), |.|, and zoom x zoom binning divided by zoom, into
+ * out [R][R] (zoom 1: transposed, as the reference).  fine: device scratch
+ * of (R zoom)^2 floats, overwritten. */
+int ncsb_sim_ideal_image(const float *xs, const float *ys, int n, int R, int zoom,
+                         const float *kernel, int ksz, float *fine, float *out, void *stream);
 
 /* The generator's uniform deviates in (0, 1) for counters (i, frame, 0, 0),
  * i < n (for statistical tests of the generator). */
@@ -463,10 +481,13 @@ int ncsb_net_infer_tiles(const float *params, const float *d, const float *gamma
  *
  * The first call on a device does a one-time set-up (it looks up the
  * array's device address with cudaGetSymbolAddress and caches the launch
- * geometry) and should come before any stream capture.  Every call shares the
- * array and re-initialises it on its own stream (mask table copy, counter
- * reset) before its launch, so calls that overlap on the GPU -- on two
- * streams or from two host threads -- race and must be serialised by the
+ * geometry) and should come before any stream capture; the cached address is
+ * kept until the process exits, so the entry must not be used across
+ * cudaDeviceReset.  Every call shares the array and re-initialises it on its
+ * own stream before its launch -- a one-block kernel writes the mask table,
+ * passed to it by value, and resets the work counter -- so a call never waits
+ * for the stream on the host, and calls that overlap on the GPU (on two
+ * streams or from two host threads) race and must be serialised by the
  * caller.
  */
 int ncsb_reduce_noise_noalloc(const ncsb_params *p, const float *mask_shifted_host,

@@ -124,7 +124,7 @@ EXPORTS = [
     "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms", "ncsb_reduce_noise_normalized",
     "ncsb_net_infer_stack_tc", "ncsb_net_infer_tiles_tc", "ncsb_genpsfparam",
     "ncsb_net_infer_batch_tc", "ncsb_reduce_noise_host",
-    "ncsb_reduce_noise_adu_typed", "ncsb_reduce_noise_adu_host",
+    "ncsb_reduce_noise_adu_typed", "ncsb_reduce_noise_adu_host", "ncsb_sim_ideal_image",
 ]
 
 _lib = None
@@ -196,6 +196,8 @@ def load():
     lib.ncsb_sim_render.restype = ctypes.c_int
     lib.ncsb_sim_camera.argtypes = [vp, ci, ci, ci, vp, vp, vp, ctypes.c_uint64, vp, vp, vp]
     lib.ncsb_sim_camera.restype = ctypes.c_int
+    lib.ncsb_sim_ideal_image.argtypes = [vp, vp, ci, ci, ci, vp, ci, vp, vp, vp]
+    lib.ncsb_sim_ideal_image.restype = ctypes.c_int
     lib.ncsb_sim_uniforms.argtypes = [i64, ctypes.c_uint32, ctypes.c_uint64, vp, vp]
     lib.ncsb_sim_uniforms.restype = ctypes.c_int
     lib.ncsb_reduce_noise_normalized.argtypes = [vp, ci, ci, ci, vp, ci, P(ctypes.c_float),

@@ -19,6 +19,8 @@ cudaError_t launch_warp_blocks(const SolveArgs& args, int grid, int blocks, cuda
 int warp_max_ctas_per_sm(int m, int blocks);
 cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream);
 int spectral_max_ctas_per_sm(int m, int blocks, bool warm, bool batch);
+cudaError_t launch_tc(const SolveArgs& args, bool bf16x3, int grid, cudaStream_t stream);
+int tc_max_ctas_per_sm(bool bf16x3, bool warm);
 namespace masks {
 bool valid(const ncsb_optics& o);
 cudaError_t launch_masks(const ncsb_optics* d_optics, int n, float* centred, float* lane,
@@ -106,8 +108,9 @@ struct ncsb_handle {
     int device = 0;
     int num_sms = 1;
     bool has_mask = false;
-    float* d_msq = nullptr;                 // [256] M^2/256, kernel spectral layout
+    float* d_msq = nullptr;                 // [256] M^2/256, natural [kr][kc] order
     unsigned long long* d_queue = nullptr;  // work counter
+    int32_t* d_flag = nullptr;              // tensor-core forms: 1 after a wait ran out
     // batched launch (ncsb_batch_set): stack descriptors, per-stack lane-layout
     // M^2/256 tables, capacity in stacks, current count and total tiles
     ncsb::StackDesc* d_stacks = nullptr;
@@ -163,7 +166,7 @@ int check_params(const ncsb_params* p, std::string* why) {
     if (!(p->epsilon >= 0.0)) { *why = "epsilon must be >= 0"; return NCSB_EINVAL; }
     if (!(p->c1 > 0.0 && p->c1 < 1.0)) { *why = "c1 must be in (0, 1)"; return NCSB_EINVAL; }
     if (!(p->min_step > 0.0)) { *why = "min_step must be > 0"; return NCSB_EINVAL; }
-    if (p->mode != NCSB_MODE_PLAIN && p->mode != NCSB_MODE_PLAIN_WG && p->mode != NCSB_MODE_SPECTRAL) { *why = "unsupported mode"; return NCSB_EINVAL; }
+    if (p->mode < NCSB_MODE_PLAIN || p->mode > NCSB_MODE_TC_BF16X3) { *why = "unsupported mode"; return NCSB_EINVAL; }
     if (p->ctas_per_sm < 0) { *why = "ctas_per_sm must be >= 0"; return NCSB_EINVAL; }
     return NCSB_OK;
 }
@@ -208,6 +211,22 @@ int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s, unsigned long lon
     a.m = h->p.m;
     const bool wg = h->p.mode == NCSB_MODE_PLAIN_WG;
     const bool spec = h->p.mode == NCSB_MODE_SPECTRAL;
+    if (h->p.mode == NCSB_MODE_TC_TF32 || h->p.mode == NCSB_MODE_TC_BF16X3) {
+        if (a.stacks) return fail(h, NCSB_EINVAL, "batched launches use the spectral form");
+        const bool bf = h->p.mode == NCSB_MODE_TC_BF16X3;
+        e = cudaMemsetAsync(h->d_flag, 0, sizeof(int32_t), s);
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemsetAsync(flag)");
+        a.flag = h->d_flag;
+        const int per = h->p.ctas_per_sm > 0 ? h->p.ctas_per_sm
+                                              : ncsb::tc_max_ctas_per_sm(bf, a.u0 != nullptr);
+        // 8 tiles per CTA
+        long long grid = (long long)per * h->num_sms;
+        if (grid > (a.n_tiles + 7) / 8) grid = (a.n_tiles + 7) / 8;
+        if (grid < 1) grid = 1;
+        e = ncsb::launch_tc(a, bf, (int)grid, s);
+        if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
+        return NCSB_OK;
+    }
     int per_sm = h->p.ctas_per_sm > 0
                      ? h->p.ctas_per_sm
                      : (wg ? ncsb::plain_max_ctas_per_sm()
@@ -257,9 +276,12 @@ int ncsb_create(ncsb_handle** out, const ncsb_params* p) {
         e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_msq, ncsb::kPix * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&h->d_queue, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_flag, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(h->d_flag, 0, sizeof(int32_t));
     if (e != cudaSuccess) {
         cudaFree(h->d_msq);
         cudaFree(h->d_queue);
+        cudaFree(h->d_flag);
         delete h;
         return NCSB_ECUDA;
     }
@@ -282,6 +304,7 @@ int ncsb_destroy(ncsb_handle* h) {
     cudaFree(h->d_adu);
     cudaFree(h->d_msq);
     cudaFree(h->d_queue);
+    cudaFree(h->d_flag);
     cudaFree(h->d_stacks);
     cudaFree(h->d_mk_lane);
     delete h;
@@ -522,8 +545,9 @@ int ncsb_reduce_noise_start(ncsb_handle* h, const float* images, int n_frames, i
                             int32_t* tile_status, double* tile_cost, int32_t* tile_evals,
                             int32_t* tile_start, void* stream) {
     if (!h) return NCSB_EINVAL;
-    if (h->p.mode != NCSB_MODE_SPECTRAL)
-        return fail(h, NCSB_EINVAL, "a proposed start needs the spectral form");
+    if (h->p.mode != NCSB_MODE_SPECTRAL && h->p.mode != NCSB_MODE_TC_TF32 &&
+        h->p.mode != NCSB_MODE_TC_BF16X3)
+        return fail(h, NCSB_EINVAL, "a proposed start needs the spectral or a tensor-core form");
     if (!h->has_mask) return fail(h, NCSB_ENOMASK, "call ncsb_set_otf_mask first");
     if (n_frames < 0 || height <= 0 || width <= 0) return fail(h, NCSB_EINVAL, "bad shape");
     if (height < NCSB_TILE - 2 || width < NCSB_TILE - 2)

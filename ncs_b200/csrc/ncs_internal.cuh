@@ -65,6 +65,8 @@ struct SolveArgs {
     const StackDesc* stacks;
     int n_stacks;
     const float* mk_lane;          // [n_stacks][256]
+    // tensor-core form: set to 1 when a tensor-core wait ran out of time
+    int32_t* flag;
 };
 
 // ---- tile geometry (segmentation of ncs.c:66-113, shared by every kernel) ----

@@ -60,7 +60,8 @@ def launch_stream(stream, device, *tensors):
 _ADU_TYPES = {torch.float32: _lib.ADU_F32, torch.uint16: _lib.ADU_U16, torch.uint8: _lib.ADU_U8}
 
 _MODES = {"plain": _lib.MODE_PLAIN, "plain_wg": _lib.MODE_PLAIN_WG,
-          "spectral": _lib.MODE_SPECTRAL}
+          "spectral": _lib.MODE_SPECTRAL, "tc_tf32": _lib.MODE_TC_TF32,
+          "tc_bf16x3": _lib.MODE_TC_BF16X3}
 
 
 class Solver:
@@ -72,8 +73,10 @@ class Solver:
     The default ``epsilon`` is libLBFGS's 1e-5 (the pyCNCS path) rather than
     the reference kernel's 1e-4.  ``mode``: "spectral" (default; L-BFGS with
     the spectral initial inverse Hessian), "plain" (the reference's L-BFGS
-    with a scalar initial matrix, one warp per tile) or "plain_wg" (one warp
-    group per tile).
+    with a scalar initial matrix, one warp per tile), "plain_wg" (one warp
+    group per tile), or the tensor-core forms "tc_tf32" and "tc_bf16x3" (the
+    spectral algorithm with the noise term's transforms as tcgen05 GEMMs,
+    TF32 operands or a three-way BF16 split; m = 1).
     """
 
     def __init__(self, alpha=0.2, max_iters=200, m=1, epsilon=1e-5, c1=1e-4, min_step=1e-6,
@@ -183,7 +186,7 @@ class Solver:
         return out
 
     def reduce_noise_from(self, images, gamma, u0_tiles, out=None, stream=None):
-        """reduce_noise starting each tile at a proposal (spectral form only).
+        """reduce_noise starting each tile at a proposal (spectral and tensor-core forms).
 
         ``u0_tiles`` is [n_tiles, 16, 16] in (frame, tile-row, tile-col) order
         (``WarmStartNet.propose_stack``).  A tile whose proposal costs more

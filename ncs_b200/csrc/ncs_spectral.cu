@@ -28,10 +28,12 @@
 // (ncs.cu:980-984) compensates for an identity start.
 //
 // Proposed start (a.u0, tile or stack mode): the first pass transforms the
-// proposal, a second one the photon image d, and the solve starts from
-// whichever has the lower cost, so a proposal never makes a tile start worse
-// than the reference's u = d; the photon-image start is then bit-identical to
-// a solve without a proposal.
+// proposal u0, which gives an upper bound of f(u0) - f(d) without a transform
+// of the photon image d; a proposal the bound accepts starts at once.  Only
+// otherwise a second pass transforms d and the solve starts from whichever
+// has the lower cost, so a proposal never makes a tile start worse than the
+// reference's u = d; the photon-image start is then bit-identical to a solve
+// without a proposal.
 #include "ncs_warp_common.cuh"
 
 namespace ncsb {
@@ -277,11 +279,33 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 }
             }
             if (first) {
-                if (start_pass == 2) {  // keep 2 alpha Q u0, transform d next
+                if (start_pass == 2) {
+                    // p = v0 = 2 alpha Q u0.  With delta = u0 - d,
+                    //   alpha d'Q d = alpha u0'Q u0 - delta'v0 + alpha delta'Q delta
+                    //              >= alpha u0'Q u0 - delta'v0,
+                    // so f(u0) - f(d) <= LL(u0) - LL(d) + delta'v0: when that
+                    // bound is <= 0 the proposal is accepted at once, without
+                    // transforming d.  Otherwise keep v0 and transform d next
+                    // for the exact comparison.
+                    float dd[8];
+                    load_d(dd);
+                    float dl = 0.0f, dq = 0.0f;
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) w[i] = p[i];
-                    start_pass = 1;
-                    continue;
+                    for (int i = 0; i < 8; ++i) {
+                        const float lr = __fsub_rn(__logf(fmaxf(u[i] + gm[i], kFitMin)),
+                                                   __logf(fmaxf(dd[i] + gm[i], kFitMin)));
+                        dl += fmaf(-c[i], lr, u[i] - dd[i]);
+                        dq += __fmul_rn(__fsub_rn(u[i], dd[i]), p[i]);
+                    }
+                    const double bound = warp_sum_d((double)dl + (double)dq);
+                    if (bound <= 0.0) {
+                        start_pass = 0;  // accepted: v = v0 below
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) w[i] = p[i];
+                        start_pass = 1;
+                        continue;
+                    }
                 }
                 if (start_pass == 1) {
                     // f(u0) - f(d) = sum[(u0 - d) - c (log(u0 + gamma) - log(d + gamma))]

@@ -93,7 +93,7 @@ cudaError_t launch_masks(const ncsb_optics* d_optics, int n, float* centred, flo
 // ---- genpsfparam (denoisetools.py:103-115) ----------------------------------
 // pupil = |k| on the centred grid (genkspace), 0 above NA / lambda;
 // PSF = |fftshift(fft2(pupil))|^2 / its sum; OTF = |fftshift(ifft2(PSF))| / its max.
-// Separable DFTs in FP64, one thread per output element (R <= 256).
+// Separable DFTs in FP64, one thread per output element (R <= 1024).
 
 __global__ void psf_pupil(int R, double px, double fmax, double2* __restrict__ z,
                           float* __restrict__ pupil) {
@@ -164,7 +164,7 @@ extern "C" {
 
 int ncsb_genpsfparam(int R, double pixel_size, double na, double wavelength, float* psf,
                      float* pupil, float* otf, void* stream) {
-    if (R < 2 || R > 256 || !(pixel_size > 0.0) || !(na > 0.0) || !(wavelength > 0.0))
+    if (R < 2 || R > 1024 || !(pixel_size > 0.0) || !(na > 0.0) || !(wavelength > 0.0))
         return NCSB_EINVAL;
     if (!psf && !pupil && !otf) return NCSB_EINVAL;
     using namespace ncsb::masks;

@@ -178,6 +178,51 @@ __global__ void uniforms(long long n, uint32_t frame, uint32_t k0, uint32_t k1, 
     out[i] = st.next();
 }
 
+// ---- genidealimage (denoisetools.py:150-186) --------------------------------
+// Occupancy of the positions on the fine grid (x -> row), then, per output
+// pixel of the R x R image, the zoom x zoom fine pixels' |'same' convolution|
+// with the PSF kernel summed in a fixed order and divided by zoom (binimage,
+// whose block order undoes genidealimage's transpose); zoom 1 keeps the
+// transpose.  FP64 sums, so the image matches the reference's FP64 FFT
+// convolution to FP32 rounding.
+
+__global__ void occupancy_kernel(const float* __restrict__ xs, const float* __restrict__ ys, int n,
+                                 int sz, float* __restrict__ fine) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float fx = floorf(xs[i]), fy = floorf(ys[i]);
+    if (!(fx >= 0.0f && fx < (float)sz && fy >= 0.0f && fy < (float)sz)) return;  // also NaN
+    fine[(long long)(int)fx * sz + (int)fy] = 1.0f;
+}
+
+// one block of zoom x zoom threads per output pixel (a, b)
+__global__ void ideal_kernel(const float* __restrict__ fine, int R, int zoom,
+                             const float* __restrict__ k, int ksz, float* __restrict__ out) {
+    extern __shared__ double part[];
+    const int a = blockIdx.x / R, b = blockIdx.x - (blockIdx.x / R) * R;
+    const int t = threadIdx.x, i = a * zoom + t / zoom, j = b * zoom + t % zoom;
+    const int sz = R * zoom, off = (ksz - 1) / 2;
+    double acc = 0.0;
+    for (int u = 0; u < ksz; ++u) {
+        const int y = i + off - u;
+        if (y < 0 || y >= sz) continue;
+        for (int v = 0; v < ksz; ++v) {
+            const int x = j + off - v;
+            if (x < 0 || x >= sz) continue;
+            const float f = fine[(long long)y * sz + x];
+            if (f != 0.0f) acc += (double)k[u * ksz + v];
+        }
+    }
+    part[t] = fabs(acc);
+    __syncthreads();
+    if (t == 0) {
+        double sum = 0.0;
+        for (int q = 0; q < zoom * zoom; ++q) sum += part[q];
+        if (zoom == 1) out[(long long)b * R + a] = (float)sum;
+        else out[(long long)a * R + b] = (float)(sum / zoom);
+    }
+}
+
 }  // namespace simk
 }  // namespace ncsb
 
@@ -211,6 +256,20 @@ int ncsb_sim_camera(const float* ideal, int n_frames, int height, int width, con
     camera<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
         ideal, n_frames, HW, offset, gain, variance, (uint32_t)seed, (uint32_t)(seed >> 32), adu,
         photo_electrons);
+    return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
+}
+
+int ncsb_sim_ideal_image(const float* xs, const float* ys, int n, int R, int zoom,
+                         const float* kernel, int ksz, float* fine, float* out, void* stream) {
+    if (n < 0 || R < 1 || zoom < 1 || zoom > 32 || ksz < 1 || !kernel || !fine || !out)
+        return NCSB_EINVAL;
+    if (n > 0 && (!xs || !ys)) return NCSB_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long sz = (long long)R * zoom;
+    if (cudaMemsetAsync(fine, 0, sizeof(float) * sz * sz, s) != cudaSuccess) return NCSB_ECUDA;
+    if (n > 0) ncsb::simk::occupancy_kernel<<<(n + 255) / 256, 256, 0, s>>>(xs, ys, n, (int)sz, fine);
+    ncsb::simk::ideal_kernel<<<R * R, zoom * zoom, sizeof(double) * zoom * zoom, s>>>(
+        fine, R, zoom, kernel, ksz, out);
     return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
 }
 

@@ -279,3 +279,36 @@ def make_stack_gpu(name="stack512", T=None, device="cuda", seed=1234, pixel=0.1,
                    gain=torch.as_tensor(gain, dtype=torch.float32, device=dev),
                    var=torch.as_tensor(var, dtype=torch.float32, device=dev))
     return out
+
+
+def ideal_image_gpu(xcor, ycor, R, pixelsize=0.1, zoom=8, NA=1.4, wavelength=0.7,
+                    device="cuda"):
+    """The reference simulator's normalised ideal image (genidealimage,
+    python3-6/pyNCS/denoisetools.py:150-186) on the GPU: chain coordinates
+    (e.g. the worm-like chains of the reference's randwlcposition.mat)
+    shifted to 0, rounded and scaled onto the fine grid of (R zoom)^2 pixels
+    (host, as the reference), then occupancy, convolution with the central
+    2 Ri x 2 Ri (Ri = 5 zoom // 2) of the device genpsfparam PSF and binning
+    (ncsb_sim_ideal_image).  Returns a float32 [R, R] tensor."""
+    import ctypes
+    from . import _lib
+    from .otf import device_psf
+    sz = int(R) * int(zoom)
+    xco = numpy.round(numpy.asarray(xcor, float) - numpy.min(xcor))
+    yco = numpy.round(numpy.asarray(ycor, float) - numpy.min(ycor))
+    scale = max(xco.max(), yco.max()) / sz
+    xs = torch.as_tensor(xco / scale, dtype=torch.float32, device=device)
+    ys = torch.as_tensor(yco / scale, dtype=torch.float32, device=device)
+    psf = device_psf(sz, pixelsize / zoom, NA, wavelength, device=device)[0]
+    cc, ri = sz // 2, int(zoom) * 5 // 2
+    kernel = psf[cc - ri:cc + ri, cc - ri:cc + ri].contiguous()
+    fine = torch.empty((sz, sz), dtype=torch.float32, device=device)
+    out = torch.empty((R, R), dtype=torch.float32, device=device)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+    with torch.cuda.device(out.device):
+        rc = _lib.load().ncsb_sim_ideal_image(
+            vp(xs), vp(ys), int(xs.numel()), int(R), int(zoom), vp(kernel), 2 * ri, vp(fine),
+            vp(out), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    if rc != _lib.NCSB_OK:
+        raise RuntimeError("ncsb_sim_ideal_image failed with code %d" % rc)
+    return out

@@ -72,3 +72,19 @@ def test_argument_checks(ncs):
     with pytest.raises(ValueError):
         ncs.reduce_noise_normalized(im, torch.ones((8, 8), device="cuda"), numpy.ones((3, 3)),
                                     alpha=-1.0)
+
+
+def test_cost_known_answer_from_calcost(ncs):
+    """The kernel's cost at the start u = d for the centre pixel of a 3 x 3
+    frame -- whose segment is the whole frame -- equals the value derived by
+    hand from calcost.m (tests/test_normalized_cpu.py states the derivation):
+    u = d = [[2, 3, 1], [1, 1, 1], [1, 1, 1]], gamma 2, alpha 1/2, mask
+    [[1, 2, 1], [1, 1/2, 1], [1, 2, 1]]; within 1e-6 relative."""
+    from test_normalized_cpu import KNOWN_COST, KNOWN_MASK, KNOWN_U
+    im = torch.tensor([KNOWN_U], dtype=torch.float32, device="cuda")
+    gam = torch.full((3, 3), 2.0, dtype=torch.float32, device="cuda")
+    out, it, st, cost = ncs.reduce_noise_normalized(im, gam, numpy.array(KNOWN_MASK),
+                                                    alpha=0.5, max_iters=0, stats=True)
+    assert int(it[0, 1, 1].item()) == 0
+    c = float(cost[0, 1, 1].item())
+    assert abs(c - KNOWN_COST) <= 1e-6 * abs(KNOWN_COST), (c, KNOWN_COST)

@@ -135,3 +135,55 @@ def test_simulated_raw_frames_through_the_fused_prologue(sim):
     g = (w["var"] / (w["gain"] * w["gain"])).contiguous()
     b = s.reduce_noise(w["images"], g)
     assert torch.equal(a, b)
+
+
+def _sim_golden():
+    import os
+    return numpy.load(os.path.join(os.path.dirname(__file__), "golden", "sim_vectors.npz"))
+
+
+def test_ideal_image_matches_the_reference_simulator(sim):
+    """sim.ideal_image_gpu (device genpsfparam, occupancy, convolution,
+    binning) against the reference's own genidealimage
+    (python3-6/pyNCS/denoisetools.py:150-186) on its worm-like-chain
+    positions (randwlcposition.mat): every pixel within 1e-6 of the image's
+    maximum (FP32 kernel and output, FP64 sums)."""
+    d = _sim_golden()
+    for key in [k[:-len("_params")] for k in d.files if k.endswith("_params")]:
+        R, zoom, px, na, lam = d[key + "_params"]
+        got = sim.ideal_image_gpu(d["xcor"], d["ycor"], int(R), px, int(zoom), na, lam)
+        ref = d[key + "_img"]
+        err = numpy.abs(got.cpu().numpy().astype(numpy.float64) - ref).max()
+        assert err <= 1e-6 * numpy.abs(ref).max(), (key, err)
+
+
+def test_camera_moments_match_addnoise(sim):
+    """The camera model against the reference's addnoise
+    (python3-6/pyNCS/denoisetools.py:205-213) on the reference simulator's
+    ideal image (I = 100 photons, bg = 10): E[ADU] = gain ideal + offset and
+    Var[ADU] = gain^2 ideal + var per pixel (oracle/sim_ref.py), checked by
+    the standardised residuals pooled over pixels and frames (mean within 6
+    standard errors of 0, variance within 6 of 1), and per pixel the sample
+    mean within 6 standard errors."""
+    from oracle import sim_ref
+    d = _sim_golden()
+    ideal = d["R64_z4_img"] * 100.0 + 10.0
+    R = ideal.shape[0]
+    rng = numpy.random.default_rng(17)
+    offset = rng.normal(100.0, 2.0, size=(R, R))
+    gain = rng.normal(2.0, 0.2, size=(R, R))
+    var = rng.exponential(60.0, size=(R, R))
+    T = 400
+    _, adu = sim.camera_gpu(torch.as_tensor(ideal, dtype=torch.float32, device="cuda"), T,
+                            offset, gain, var, seed=99, adu=True, photons=False)
+    a = adu.cpu().numpy().astype(numpy.float64)
+    mean, variance = sim_ref.camera_moments(ideal.astype(numpy.float32).astype(numpy.float64),
+                                            gain.astype(numpy.float32),
+                                            var.astype(numpy.float32),
+                                            offset.astype(numpy.float32))
+    z = (a - mean) / numpy.sqrt(variance)
+    n = z.size
+    assert abs(z.mean()) <= 6 / numpy.sqrt(n)
+    assert abs(z.var() - 1.0) <= 6 * numpy.sqrt(2.0 / n)
+    per_pixel = (a.mean(axis=0) - mean) / numpy.sqrt(variance / T)
+    assert numpy.abs(per_pixel).max() <= 6.0

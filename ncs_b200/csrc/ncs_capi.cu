@@ -21,6 +21,7 @@ cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStr
 int spectral_max_ctas_per_sm(int m, int blocks, bool warm, bool batch);
 cudaError_t launch_tc(const SolveArgs& args, bool bf16x3, int grid, cudaStream_t stream);
 int tc_max_ctas_per_sm(bool bf16x3, bool warm);
+int tc_tiles_per_cta();
 namespace masks {
 bool valid(const ncsb_optics& o);
 cudaError_t launch_masks(const ncsb_optics* d_optics, int n, float* centred, float* lane,
@@ -219,9 +220,9 @@ int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s, unsigned long lon
         a.flag = h->d_flag;
         const int per = h->p.ctas_per_sm > 0 ? h->p.ctas_per_sm
                                               : ncsb::tc_max_ctas_per_sm(bf, a.u0 != nullptr);
-        // 8 tiles per CTA
+        const long long tpc = ncsb::tc_tiles_per_cta();
         long long grid = (long long)per * h->num_sms;
-        if (grid > (a.n_tiles + 7) / 8) grid = (a.n_tiles + 7) / 8;
+        if (grid > (a.n_tiles + tpc - 1) / tpc) grid = (a.n_tiles + tpc - 1) / tpc;
         if (grid < 1) grid = 1;
         e = ncsb::launch_tc(a, bf, (int)grid, s);
         if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");

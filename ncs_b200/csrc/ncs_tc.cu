@@ -9,7 +9,7 @@
 // h = 1 / (lambda + 2 alpha M^2) gives p = H0 q in an iteration (the
 // spectral initial inverse Hessian; 2 alpha Q H0 q = q - lambda H0 q needs no
 // transform of its own, nor does any line-search trial).  Here that operator
-// is four GEMMs over the eight tiles of a CTA (M = 128 = 8 tiles x 16 rows):
+// is four GEMMs over the tiles of a CTA (M = 16 rows per tile, 4 tiles):
 //   1. row DFT, real -> packed half spectrum:    [x]      (K 16)  x B1 (N 16)
 //   2. column DFT, complex, per column 0..8:     [Y^T]    (K 32)  x B2 (N 32)
 //      then the weights h, elementwise
@@ -39,11 +39,13 @@
 // preconditioner.  The final per-tile cost reported is the model's; callers
 // that want the exact cost of the result evaluate it from u.
 //
-// Lock step: the eight warps of a CTA each own a tile and pass through the
+// Lock step: the warps of a CTA each own a tile and pass through the
 // four stages together (one CTA barrier before each stage's MMAs; thread 0
-// issues them and commits to an mbarrier all threads wait on).  A warp whose
+// issues them and commits to an mbarrier all threads wait on, suspended
+// rather than spinning).  A warp whose
 // tile finishes takes the next one from the work queue at the start of the
-// next pass, so every pass carries eight tiles until the queue runs dry.
+// next pass, so every pass carries a full set of tiles until the queue runs
+// dry.
 // Waits are bounded: a wait that runs out sets a.flag, every thread leaves
 // the pass loop at the next barrier, the outstanding MMAs get a bounded wait
 // and tensor memory is freed.
@@ -56,13 +58,27 @@ using namespace warp;
 
 namespace tcs {
 
-constexpr int kTcWarps = 8;
+// Tiles (warps) per CTA: the GEMMs have M = 16 kTiles rows.  With 4 tiles
+// (M = 64) four CTAs share an SM, and the tensor core writes a CTA's 64
+// accumulator rows to lanes 0-15 of each 32-lane quarter of tensor memory,
+// rows 16 w .. 16 w + 15 to the quarter of warp w -- so each warp reads its
+// own tile.  (With 8 tiles, M = 128 and two CTAs per SM, row m is lane m.)
+constexpr int kTiles = 4;
+constexpr int kM = 16 * kTiles;
+constexpr int kTcWarps = kTiles;
 constexpr int kTcThreads = 32 * kTcWarps;
+constexpr int kMinBlocks = 16 / kTiles;  // 128 registers a thread fill the register file
 constexpr uint32_t kTmemCols = 128;        // D of stages 1..4 at columns 0, 32, 64, 96
-constexpr long long kWaitTries = 1ll << 22;  // mbarrier polls before giving up (seconds)
+constexpr long long kWaitTries = 1ll << 17;  // mbarrier polls of <= 20 us before giving up
+
+// Operand A (kM rows): groups of 8 rows, 128 B apart; K chunks (16 bytes of
+// K per row) kALbo apart.  The extra 16 bytes move consecutive chunks to the
+// next 16-byte bank group, so the epilogue stores of a warp (lanes spread
+// over chunks and rows) spread over all banks.
+constexpr int kALbo = (kM / 8) * 128 + 16;
 
 // Shared-memory plan for element size ES (4: TF32, 2: BF16) and parts NP
-// (1: TF32, 2: BF16 hi and lo).  Operand A (M = 128): chunk stride 2048 B.
+// (1: TF32, 2: BF16 hi and lo).
 template <bool BF>
 struct Plan {
     static constexpr int ES = BF ? 2 : 4;
@@ -73,8 +89,8 @@ struct Plan {
     static constexpr int B4 = 16 * 32 * ES;             // N 16 x K 32
     static constexpr int BPART = B1 + 2 * B2 + B4;      // one part of B1..B4
     static constexpr int OFF_B = 0;
-    static constexpr int A1 = 128 * 16 * ES;            // stage-1 operand, one part
-    static constexpr int A2 = 128 * 32 * ES;            // stages 2-4 operand, one part
+    static constexpr int A1 = (16 / KPC) * kALbo;       // stage-1 operand (K 16), one part
+    static constexpr int A2 = (32 / KPC) * kALbo;       // stages 2-4 operand (K 32), one part
     static constexpr int OFF_A1 = OFF_B + NP * BPART;
     static constexpr int OFF_A2 = OFF_A1 + NP * A1;
     static constexpr int OFF_HIST = OFF_A2 + NP * A2;   // per warp: s, y, Q s (1 KB each)
@@ -114,7 +130,7 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t&
 template <bool BF>
 __device__ __forceinline__ void st2(unsigned char* buf, int part_bytes, int row, int k0,
                                     float x0, float x1) {
-    const int o = koff<Plan<BF>::ES>(row, k0, 2048);
+    const int o = koff<Plan<BF>::ES>(row, k0, kALbo);
     if constexpr (BF) {
         uint32_t hi, lo;
         split2(x0, x1, hi, lo);
@@ -127,7 +143,7 @@ __device__ __forceinline__ void st2(unsigned char* buf, int part_bytes, int row,
 template <bool BF>
 __device__ __forceinline__ void st4(unsigned char* buf, int part_bytes, int row, int k0, float x0,
                                     float x1, float x2, float x3) {
-    const int o = koff<Plan<BF>::ES>(row, k0, 2048);
+    const int o = koff<Plan<BF>::ES>(row, k0, kALbo);
     if constexpr (BF) {
         uint32_t h0, l0, h1, l1;
         split2(x0, x1, h0, l0);
@@ -143,16 +159,16 @@ template <bool BF>
 __device__ __forceinline__ void st8(unsigned char* buf, int part_bytes, int row, int k0,
                                     const float (&x)[8]) {
     if constexpr (BF) {
-        const int o = koff<2>(row, k0, 2048);
+        const int o = koff<2>(row, k0, kALbo);
         uint32_t h[4], l[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) split2(x[2 * i], x[2 * i + 1], h[i], l[i]);
         *reinterpret_cast<uint4*>(buf + o) = make_uint4(h[0], h[1], h[2], h[3]);
         *reinterpret_cast<uint4*>(buf + part_bytes + o) = make_uint4(l[0], l[1], l[2], l[3]);
     } else {
-        *reinterpret_cast<float4*>(buf + koff<4>(row, k0, 2048)) =
+        *reinterpret_cast<float4*>(buf + koff<4>(row, k0, kALbo)) =
             make_float4(tf32r(x[0]), tf32r(x[1]), tf32r(x[2]), tf32r(x[3]));
-        *reinterpret_cast<float4*>(buf + koff<4>(row, k0 + 4, 2048)) =
+        *reinterpret_cast<float4*>(buf + koff<4>(row, k0 + 4, kALbo)) =
             make_float4(tf32r(x[4]), tf32r(x[5]), tf32r(x[6]), tf32r(x[7]));
     }
 }
@@ -226,17 +242,17 @@ __device__ __forceinline__ void issue_stage(int stage, uint32_t tmem, uint32_t s
     // K steps of 2 chunks (TF32: K 8; BF16: K 16) -- stage 4 only up to K 24 / 32
     const int steps = BF ? (stage == 1 ? 1 : 2) : (stage == 1 ? 2 : (stage == 4 ? 3 : 4));
     for (int s = 0; s < steps; ++s) {
-        const uint64_t ad = tc::sdesc(a + 2 * s * 2048, 2048, 128);
+        const uint64_t ad = tc::sdesc(a + 2 * s * kALbo, kALbo, 128);
         const uint64_t bd = tc::sdesc(sb + boff + 2 * s * lbo_b, lbo_b, 128);
         if constexpr (BF) {
-            const uint32_t id = tc::idesc_bf16(128, N);
-            const uint64_t adl = tc::sdesc(a + apart + 2 * s * 2048, 2048, 128);
+            const uint32_t id = tc::idesc_bf16(kM, N);
+            const uint64_t adl = tc::sdesc(a + apart + 2 * s * kALbo, kALbo, 128);
             const uint64_t bdl = tc::sdesc(sb + PL::BPART + boff + 2 * s * lbo_b, lbo_b, 128);
             tc::mma_bf16(tmem + col, ad, bd, id, s > 0);  // hi x hi
             tc::mma_bf16(tmem + col, adl, bd, id, 1u);    // lo x hi
             tc::mma_bf16(tmem + col, ad, bdl, id, 1u);    // hi x lo
         } else {
-            tc::mma_tf32(tmem + col, ad, bd, tc::idesc_tf32(128, N), s > 0);
+            tc::mma_tf32(tmem + col, ad, bd, tc::idesc_tf32(kM, N), s > 0);
         }
     }
 }
@@ -255,7 +271,7 @@ struct Geo {
 using namespace tcs;
 
 template <bool BF, bool Warm>
-__global__ void __launch_bounds__(kTcThreads, 2) ncs_tc_kernel(const SolveArgs a) {
+__global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const SolveArgs a) {
     using PL = Plan<BF>;
     extern __shared__ __align__(1024) unsigned char dsm[];
     __shared__ __align__(8) uint64_t s_bar;
@@ -264,8 +280,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) ncs_tc_kernel(const SolveArgs a
     const float eps2 = a.eps * a.eps;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int P = lane >> 2, Qd = lane & 3;
-    const int ts = 2 * (wid & 3) + (wid >> 2);  // the warp's tile slot: M rows 16 ts .. 16 ts + 15
+    // the warp's tile slot: M rows 16 ts .. 16 ts + 15, in tensor-memory lanes
+    // tl .. tl + 15 of the warp's quarter
+    const int ts = kTiles == 8 ? 2 * (wid & 3) + (wid >> 2) : wid;
     const int row0 = 16 * ts;
+    const int tl = kTiles == 8 ? row0 : 32 * wid;
     unsigned char* sB = dsm + PL::OFF_B;
     unsigned char* sA1 = dsm + PL::OFF_A1;
     unsigned char* sA2 = dsm + PL::OFF_A2;
@@ -290,7 +309,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) ncs_tc_kernel(const SolveArgs a
     __syncthreads();
     tc::fence_after();
     const uint32_t tmem = s_tmem;
-    const uint32_t tlane = tmem + ((uint32_t)row0 << 16);
+    const uint32_t tlane = tmem + ((uint32_t)tl << 16);
     const uint32_t sbu = tc::smem_u32(sB), sa1u = tc::smem_u32(sA1), sa2u = tc::smem_u32(sA2);
     const uint32_t bar = tc::smem_u32(&s_bar);
     uint32_t phase = 0;
@@ -803,32 +822,50 @@ size_t tc_smem_bytes(bool bf16x3) {
 
 }  // namespace
 
-// Grid: CTAs of 8 tiles; `blocks` resident CTAs per SM (0: 2).
+int tc_tiles_per_cta() { return kTiles; }
+
+namespace {
+cudaError_t prepare(TcKernel fn, size_t smem) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // all of the unified L1 as shared memory: two CTAs per SM need 2 x ~62 KB
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    return e;
+}
+}  // namespace
+
+// Grid: CTAs of kTiles tiles, persistent over the work queue.
 cudaError_t launch_tc(const SolveArgs& args, bool bf16x3, int grid, cudaStream_t stream) {
     const TcKernel fn = tc_variant(bf16x3, args.u0 != nullptr);
     const size_t smem = tc_smem_bytes(bf16x3);
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = prepare(fn, smem);
     if (e != cudaSuccess) return e;
     fn<<<grid, kTcThreads, smem, stream>>>(args);
     return cudaGetLastError();
 }
 
+// Resident CTAs per SM: kMinBlocks (the register file at 128 registers a
+// thread; 128 tensor-memory columns each fill the SM's 512 at four); fewer if
+// shared memory does not hold them.
 int tc_max_ctas_per_sm(bool bf16x3, bool warm) {
     const TcKernel fn = tc_variant(bf16x3, warm);
     const size_t smem = tc_smem_bytes(bf16x3);
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-        return 1;
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTcThreads, smem) != cudaSuccess)
-        return 1;
-    // tensor memory: 128 columns per CTA, 512 per SM
-    n = n > 4 ? 4 : n;
+    if (prepare(fn, smem) != cudaSuccess) return 1;
+    int dev = 0, per_sm = 0, reserved = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    const int by_smem = per_sm / (int)(smem + 1024 + reserved);  // + static shared memory
+    const int n = by_smem < kMinBlocks ? by_smem : kMinBlocks;
     return n > 0 ? n : 1;
 }
 
-static_assert(Plan<false>::BYTES <= 100 * 1024 && Plan<true>::BYTES <= 100 * 1024,
-              "two CTAs per SM");
+static_assert(kMinBlocks * (Plan<false>::BYTES + 2048) <= 228 * 1024 &&
+                  kMinBlocks * (Plan<true>::BYTES + 2048) <= 228 * 1024,
+              "kMinBlocks CTAs per SM");
+static_assert(kMinBlocks * kTmemCols <= 512, "tensor memory of kMinBlocks CTAs");
+static_assert(kTiles == 4 || kTiles == 8, "M = 64 or 128");
 static_assert(Plan<false>::OFF_A1 % 1024 == 0 && Plan<true>::OFF_A1 % 1024 == 0, "alignment");
 
 }  // namespace ncsb

@@ -81,11 +81,26 @@ __device__ __forceinline__ bool try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// At most `tries` polls (each try_wait may suspend the thread for a while):
-// false when the phase did not complete in time.
+// try_wait that may suspend the thread for up to `ns` nanoseconds; a
+// suspended thread wakes when the phase completes, so waiting warps stop
+// taking issue slots from the warps that have work.
+__device__ __forceinline__ bool try_wait_sleep(uint32_t bar, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
+// At most `tries` polls of up to 20 us each: false when the phase did not
+// complete in time (tries = 1 << 17 bounds a wait by about 2.6 s).
 __device__ __forceinline__ bool wait_bounded(uint32_t bar, uint32_t parity, long long tries) {
     for (long long i = 0; i < tries; ++i)
-        if (try_wait(bar, parity)) return true;
+        if (try_wait_sleep(bar, parity, 20000u)) return true;
     return false;
 }
 

@@ -726,7 +726,7 @@ def run_ours(args, world, rank, local):
         for k in range(nws):
             net.propose_stack_tc(images, gamma, out=u0)
             we[2 * k + 1].record(stream)
-            solver.reduce_noise_from(images, gamma, u0, out=out)
+            solver.reduce_noise_from(images, gamma, u0, out=out, stats=False)
             we[2 * k + 2].record(stream)
         torch.cuda.synchronize()
         assert int(tc_status.item()) == 0, "tensor-core inference timed out"
@@ -763,7 +763,7 @@ def run_ours(args, world, rank, local):
             for k in range(nws):
                 net.propose_stack_tc(images, gamma, out=u0)
                 wt[2 * k + 1].record(stream)
-                tsv.reduce_noise_from(images, gamma, u0, out=out)
+                tsv.reduce_noise_from(images, gamma, u0, out=out, stats=False)
                 wt[2 * k + 2].record(stream)
             torch.cuda.synchronize()
             wt_tot = max_over_ranks(wt[0].elapsed_time(wt[-1]), world) / nws

@@ -185,14 +185,17 @@ class Solver:
             return out, iters, status, cost
         return out
 
-    def reduce_noise_from(self, images, gamma, u0_tiles, out=None, stream=None):
+    def reduce_noise_from(self, images, gamma, u0_tiles, out=None, stream=None, stats=True):
         """reduce_noise starting each tile at a proposal (spectral and tensor-core forms).
 
         ``u0_tiles`` is [n_tiles, 16, 16] in (frame, tile-row, tile-col) order
         (``WarmStartNet.propose_stack``).  A tile whose proposal costs more
         than its photon image starts at the photon image instead.  Returns
         (out, iters, status, cost, evals, fell_back) with the per-tile arrays
-        on the device; fell_back is 1 where the photon-image start was used."""
+        on the device; fell_back is 1 where the photon-image start was used.
+        With ``stats=False`` only (out, fell_back): the kernel then skips the
+        per-tile statistics, whose FP64 final cost is a measurable part of a
+        solve."""
         images = self._tensor(images, "images")
         T, H, W = images.shape
         gamma = self._tensor(gamma, "gamma")
@@ -205,10 +208,12 @@ class Solver:
         n = self.num_tiles(T, H, W)
         u0_tiles = self._tensor(u0_tiles, "u0_tiles", (n, 16, 16))
         out = torch.empty_like(images) if out is None else self._tensor(out, "out", (T, H, W))
-        iters = torch.empty(n, dtype=torch.int32, device=self.device)
-        status = torch.empty(n, dtype=torch.int32, device=self.device)
-        cost = torch.empty(n, dtype=torch.float64, device=self.device)
-        evals = torch.empty(n, dtype=torch.int32, device=self.device)
+        iters = status = cost = evals = None
+        if stats:
+            iters = torch.empty(n, dtype=torch.int32, device=self.device)
+            status = torch.empty(n, dtype=torch.int32, device=self.device)
+            cost = torch.empty(n, dtype=torch.float64, device=self.device)
+            evals = torch.empty(n, dtype=torch.int32, device=self.device)
         start = torch.empty(n, dtype=torch.int32, device=self.device)
         s = launch_stream(stream, self.device, images, gamma, u0_tiles, out, iters, status, cost,
                           evals, start)
@@ -217,6 +222,8 @@ class Solver:
                 self._handle, _ptr(images), T, H, W, _ptr(gamma), per_frame, _ptr(u0_tiles),
                 _ptr(out), _ptr(iters), _ptr(status), _ptr(cost), _ptr(evals), _ptr(start),
                 ctypes.c_void_p(s.cuda_stream)))
+        if not stats:
+            return out, start
         return out, iters, status, cost, evals, start
 
     def _calibration(self, offset, gain, variance, levels, H, W):

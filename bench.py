@@ -1043,6 +1043,41 @@ def run_mixed(args, world, rank, local):
                 "fallback_frac": w_stats["start"].double().mean().item(),
                 "speedup_vs_photon_start": (total_ms / args.steps) / w_ms,
                 "_cost": w_stats["cost"].cpu().numpy()}
+        # the same with the TF32 tensor-core form solving the batch from the
+        # proposals (the mixed workload's warm start + tensor-core noise term)
+        tsolver = ncs_b200.Solver(max_iters=200, mode="tc_tf32")
+        touts = tsolver.batch_set(stacks)
+        t_stats = tsolver.batch_stats()
+        net.propose_batch_tc(tsolver, out=u0, status=tc_status)
+        tsolver.batch_reduce_noise(u0_tiles=u0, stats=t_stats)
+        torch.cuda.synchronize()
+        tgraph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(tgraph):
+            net.propose_batch_tc(tsolver, out=u0, status=tc_status)
+            tsolver.batch_reduce_noise(u0_tiles=u0)
+        for _ in range(args.warmup):
+            tgraph.replay()
+        barrier(world)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(nws):
+            tgraph.replay()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        assert int(tc_status.item()) == 0, "tensor-core inference timed out"
+        t_ms = max_over_ranks(t0.elapsed_time(t1), world) / nws
+        st_t = t_stats["status"].cpu().numpy()
+        warm["tc_form"] = {
+            "kernels": "ncsb::nettc::infer_tc, then ncs_tc_kernel<TF32, Warm, Batch>, one "
+                       "CUDA graph",
+            "ms_per_step": t_ms, "value": sum_over_ranks(px, world) / (t_ms / 1e3) / 1e6,
+            "mean_iters": t_stats["iters"].double().mean().item(),
+            "fallback_frac": t_stats["start"].double().mean().item(),
+            "status": {str(k): int((st_t == k).sum()) for k in range(-5, 1) if (st_t == k).any()},
+            "_cost": t_stats["cost"].cpu().numpy()}
+        del tgraph, touts
+        tsolver.close()
         del wgraph, u0
 
     sides = sorted({st["side"] for st in stacks})
@@ -1067,12 +1102,19 @@ def run_mixed(args, world, rank, local):
     }
     if warm is not None:
         line["warm_start"] = {k: v for k, v in warm.items() if not k.startswith("_")}
+        line["warm_start"]["tc_form"] = {k: v for k, v in warm["tc_form"].items()
+                                         if not k.startswith("_")}
     if rank == 0:
         line["accuracy"] = mixed_accuracy(stacks, stats["cost"].cpu().numpy(),
                                           args.accuracy_tiles)
         if warm is not None:
             line["warm_start"]["accuracy"] = mixed_accuracy(stacks, warm["_cost"],
                                                             args.accuracy_tiles)
+            # the tensor-core form reports its running cost (v = 2 alpha Q u kept
+            # by updates), which differs from the exact cost by its transform error
+            line["warm_start"]["tc_form"]["accuracy"] = mixed_accuracy(
+                stacks, warm["tc_form"]["_cost"], args.accuracy_tiles)
+            line["warm_start"]["tc_form"]["accuracy"]["cost"] = "the kernel's running cost"
         print(json.dumps(line), flush=True)
     del graph
     return 0

@@ -213,7 +213,6 @@ int launch(ncsb_handle* h, ncsb::SolveArgs& a, cudaStream_t s, unsigned long lon
     const bool wg = h->p.mode == NCSB_MODE_PLAIN_WG;
     const bool spec = h->p.mode == NCSB_MODE_SPECTRAL;
     if (h->p.mode == NCSB_MODE_TC_TF32 || h->p.mode == NCSB_MODE_TC_BF16X3) {
-        if (a.stacks) return fail(h, NCSB_EINVAL, "batched launches use the spectral form");
         const bool bf = h->p.mode == NCSB_MODE_TC_BF16X3;
         e = cudaMemsetAsync(h->d_flag, 0, sizeof(int32_t), s);
         if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemsetAsync(flag)");
@@ -782,8 +781,9 @@ int ncsb_batch_reduce_noise(ncsb_handle* h, const float* u0_tiles, int32_t* tile
                             int32_t* tile_status, double* tile_cost, int32_t* tile_evals,
                             int32_t* tile_start, void* stream) {
     if (!h) return NCSB_EINVAL;
-    if (h->p.mode != NCSB_MODE_SPECTRAL)
-        return fail(h, NCSB_EINVAL, "batched launches need the spectral form");
+    if (h->p.mode != NCSB_MODE_SPECTRAL && h->p.mode != NCSB_MODE_TC_TF32 &&
+        h->p.mode != NCSB_MODE_TC_BF16X3)
+        return fail(h, NCSB_EINVAL, "batched launches need the spectral or a tensor-core form");
     if (h->n_stacks < 1) return fail(h, NCSB_EINVAL, "call ncsb_batch_set first");
     ncsb::SolveArgs a{};
     a.tile_mode = 0;

@@ -270,10 +270,14 @@ struct Geo {
 
 using namespace tcs;
 
-template <bool BF, bool Warm>
+// Batch: tiles of several stacks (own shape, alpha and mask each, a.stacks)
+// in one queue; a warp finds its tile's stack by binary search over the
+// stacks' first tiles and keeps the descriptor in a shared slot.
+template <bool BF, bool Warm, bool Batch>
 __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const SolveArgs a) {
     using PL = Plan<BF>;
     extern __shared__ __align__(1024) unsigned char dsm[];
+    __shared__ StackDesc s_stack[kTcWarps];
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
@@ -315,15 +319,36 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
     uint32_t phase = 0;
 
     // M^2/256 at this lane's stage-2 bins: row kc = P at kr = 4q + Qd, and
-    // (lanes with P = 0) row kc = 8
+    // (lanes with P = 0) row kc = 8.  A batch reads them per tile from its
+    // stack's table in the spectral form's lane layout: bin (kr, kc) sits at
+    // 8 (2 kc + kr % 2) + bitrev3(kr / 2).
     float mkA[4], mkB[4];
+    auto load_bins = [&](const float* tab, bool lane_layout) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        mkA[q] = __ldg(a.msq + (4 * q + Qd) * 16 + P);
-        mkB[q] = __ldg(a.msq + (4 * q + Qd) * 16 + 8);
-    }
-    const float alpha = a.alpha, two_alpha = 2.0f * a.alpha, a512 = 512.0f * a.alpha;
-    const Geo sg{a.data, a.gamma, a.out, a.gamma_frame_stride, a.H, a.W, a.tiles_x, a.tiles_y};
+        for (int q = 0; q < 4; ++q) {
+            const int kr = 4 * q + Qd;
+            if (lane_layout) {
+                mkA[q] = __ldg(tab + 8 * (2 * P + (kr & 1)) + bitrev3(kr >> 1));
+                mkB[q] = __ldg(tab + 8 * (16 + (kr & 1)) + bitrev3(kr >> 1));
+            } else {
+                mkA[q] = __ldg(tab + kr * 16 + P);
+                mkB[q] = __ldg(tab + kr * 16 + 8);
+            }
+        }
+    };
+    if (!Batch) load_bins(a.msq, false);
+    float alpha = a.alpha, two_alpha = 2.0f * a.alpha, a512 = 512.0f * a.alpha;
+    // the warp's stack geometry: the launch's, or its current stack's
+    auto geo = [&]() -> Geo {
+        if constexpr (Batch) {
+            const StackDesc& sd = s_stack[wid];
+            return Geo{sd.data, sd.gamma, sd.out, sd.gamma_frame_stride, sd.H, sd.W, sd.tiles_x,
+                       sd.tiles_y};
+        } else {
+            return Geo{a.data, a.gamma, a.out, a.gamma_frame_stride, a.H, a.W, a.tiles_x,
+                       a.tiles_y};
+        }
+    };
 
     // One stage: everyone's operand rows are in shared memory; thread 0
     // issues the stage's MMAs; all wait for them.  False: abort.
@@ -366,6 +391,7 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                 for (int s = 0; s < 2; ++s)
                     dst[2 * j + s] = __ldg(dt + (P + 8 * s) * kTile + Qd + 4 * j);
         } else {
+            const Geo sg = geo();
             const float* img = sg.data + (long long)f * sg.H * sg.W;
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
@@ -386,6 +412,23 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
             tile = (long long)__shfl_sync(kFull, tk, 0);
             if (tile < a.n_tiles) {
                 has_tile = true;
+                long long lt = tile;  // index of the tile within its stack
+                if constexpr (Batch) {
+                    int lo = 0, hi = a.n_stacks - 1;
+                    while (lo < hi) {  // last stack whose first tile is <= tile
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (__ldg(&a.stacks[mid].tile_begin) <= tile) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    __syncwarp();  // every lane is done with the previous descriptor
+                    if (lane == 0) s_stack[wid] = a.stacks[lo];
+                    __syncwarp();
+                    lt = tile - s_stack[wid].tile_begin;
+                    alpha = s_stack[wid].alpha;
+                    two_alpha = 2.0f * alpha;
+                    a512 = 512.0f * alpha;
+                    load_bins(a.mk_lane + (size_t)lo * 256, true);
+                }
                 if (a.tile_mode) {
                     const long long base = tile * kPix;
 #pragma unroll
@@ -398,9 +441,10 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                             u[2 * j + s] = Warm ? __ldg(a.u0 + base + off) : d[2 * j + s];
                         }
                 } else {
+                    const Geo sg = geo();
                     const long long per_frame = (long long)sg.tiles_x * sg.tiles_y;
-                    f = (int)(tile / per_frame);
-                    const int rem = (int)(tile - (long long)f * per_frame);
+                    f = (int)(lt / per_frame);
+                    const int rem = (int)(lt - (long long)f * per_frame);
                     const int ti = rem / sg.tiles_y, tj = rem - (rem / sg.tiles_y) * sg.tiles_y;
                     ox = tile_origin(ti, sg.H);
                     oy = tile_origin(tj, sg.W);
@@ -777,6 +821,7 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                 for (int s = 0; s < 2; ++s)
                     a.out[base + (P + 8 * s) * kTile + Qd + 4 * j] = u[2 * j + s];
         } else {
+            const Geo sg = geo();
             float* o = sg.out + (long long)f * sg.H * sg.W;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -811,9 +856,14 @@ namespace {
 
 using TcKernel = void (*)(SolveArgs);
 
-TcKernel tc_variant(bool bf16x3, bool warm) {
-    if (bf16x3) return warm ? ncs_tc_kernel<true, true> : ncs_tc_kernel<true, false>;
-    return warm ? ncs_tc_kernel<false, true> : ncs_tc_kernel<false, false>;
+template <bool BF>
+TcKernel tc_variant_p(bool warm, bool batch) {
+    if (batch) return warm ? ncs_tc_kernel<BF, true, true> : ncs_tc_kernel<BF, false, true>;
+    return warm ? ncs_tc_kernel<BF, true, false> : ncs_tc_kernel<BF, false, false>;
+}
+
+TcKernel tc_variant(bool bf16x3, bool warm, bool batch) {
+    return bf16x3 ? tc_variant_p<true>(warm, batch) : tc_variant_p<false>(warm, batch);
 }
 
 size_t tc_smem_bytes(bool bf16x3) {
@@ -837,7 +887,7 @@ cudaError_t prepare(TcKernel fn, size_t smem) {
 
 // Grid: CTAs of kTiles tiles, persistent over the work queue.
 cudaError_t launch_tc(const SolveArgs& args, bool bf16x3, int grid, cudaStream_t stream) {
-    const TcKernel fn = tc_variant(bf16x3, args.u0 != nullptr);
+    const TcKernel fn = tc_variant(bf16x3, args.u0 != nullptr, args.stacks != nullptr);
     const size_t smem = tc_smem_bytes(bf16x3);
     cudaError_t e = prepare(fn, smem);
     if (e != cudaSuccess) return e;
@@ -849,7 +899,7 @@ cudaError_t launch_tc(const SolveArgs& args, bool bf16x3, int grid, cudaStream_t
 // thread; 128 tensor-memory columns each fill the SM's 512 at four); fewer if
 // shared memory does not hold them.
 int tc_max_ctas_per_sm(bool bf16x3, bool warm) {
-    const TcKernel fn = tc_variant(bf16x3, warm);
+    const TcKernel fn = tc_variant(bf16x3, warm, false);
     const size_t smem = tc_smem_bytes(bf16x3);
     if (prepare(fn, smem) != cudaSuccess) return 1;
     int dev = 0, per_sm = 0, reserved = 0;

@@ -237,3 +237,66 @@ def test_warm_start_with_tc_form(ncs, form):
     good = torch.from_numpy(td.astype(numpy.float32)).cuda()  # the photon image itself
     out2, it2, st2, _, _, fb2 = s.reduce_noise_from(x, g, good)
     assert (st2.cpu().numpy() == 0).all() and it2.numel() == n
+
+
+@pytest.mark.parametrize("form", TC_FORMS)
+def test_batch_equals_single_stack_solves(ncs, form):
+    """The batched launch (many stacks, each with its own shape, alpha and
+    mask, one queue) in a tensor-core form: every stack's result, iterations
+    and status equal a single-stack solve of the same form bit for bit, with
+    and without proposed starts; the batch can be captured in a CUDA graph."""
+    from ncs_b200 import sim, warmstart
+    stacks = sim.make_mixed(6, seed=31, sides=(64, 128), frames=(1, 3))
+    ref = []
+    for st in stacks:
+        s1 = ncs.Solver(alpha=st["alpha"], max_iters=60, mode=form)
+        s1.set_otf_mask(st["mask"])
+        o, it, sta = s1.reduce_noise(st["images"], st["gamma"], tile_stats="status")
+        ref.append((o, it, sta))
+        s1.close()
+    s = ncs.Solver(max_iters=60, mode=form)
+    outs = s.batch_set(stacks)
+    stats = s.batch_stats()
+    s.batch_reduce_noise(stats=stats)
+    torch.cuda.synchronize()
+    off = 0
+    for (o, it, sta), out in zip(ref, outs):
+        n = it.numel()
+        assert torch.equal(out, o)
+        assert torch.equal(stats["iters"][off:off + n], it)
+        assert torch.equal(stats["status"][off:off + n], sta)
+        off += n
+    assert off == s.batch_tiles
+    # proposals from the batched network inference, solved in the same form
+    net = warmstart.WarmStartNet.load()
+    u0 = net.propose_batch(s)
+    stats2 = s.batch_stats()
+    s.batch_reduce_noise(u0_tiles=u0, stats=stats2)
+    torch.cuda.synchronize()
+    assert (stats2["status"].cpu().numpy() == 0).all()
+    off = 0
+    for st, out in zip(stacks, outs):
+        s1 = ncs.Solver(alpha=st["alpha"], max_iters=60, mode=form)
+        s1.set_otf_mask(st["mask"])
+        n = s1.num_tiles(*st["images"].shape)
+        o, it, sta, _, _, fb = s1.reduce_noise_from(st["images"], st["gamma"],
+                                                    u0[off:off + n].contiguous())
+        assert torch.equal(out, o) and torch.equal(stats2["iters"][off:off + n], it)
+        assert torch.equal(stats2["start"][off:off + n], fb)
+        off += n
+        s1.close()
+    # graph capture and replay of the batched launch
+    graph = torch.cuda.CUDAGraph()
+    stats3 = s.batch_stats()
+    s.batch_reduce_noise(stats=stats3)  # warm-up outside the capture
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph):
+        s.batch_reduce_noise(stats=stats3)
+    for o in outs:
+        o.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+    for (o, it, sta), out in zip(ref, outs):
+        assert torch.equal(out, o)
+    del graph
+    s.close()

@@ -687,16 +687,19 @@ def run_ours(args, world, rank, local):
                 "status": {str(k): int((st_t == k).sum()) for k in range(-5, 1)
                            if (st_t == k).any()},
                 "vs_spectral_fft": (total_ms / args.steps) / t_ms,
-                "tensor": {"executed_flop_per_pass": TC_EXEC_FLOP_PER_PASS[tform],
-                           "dense_q_flop_per_pass": DENSE_Q_FLOP_PER_PASS,
-                           "executed_tflops": exec_tflops,
-                           "dense_q_equiv_tflops": passes * DENSE_Q_FLOP_PER_PASS
-                           / (t_ms / 1e3) / 1e12,
-                           "peak_tflops": peak_t,
-                           "frac": exec_tflops / peak_t,
-                           "peak_source": "dense BF16 measured burst%s"
-                                          % ("" if tform == "tc_bf16x3"
-                                             else " x 1/2 (TF32 runs at half the BF16 rate)")},
+                "roofline": {"bound": "tensor", "achieved": exec_tflops, "peak": peak_t,
+                             "unit": "TFLOP/s", "frac": exec_tflops / peak_t,
+                             "traffic": None, "kernel": KERNEL[tform],
+                             "executed_flop_per_pass": TC_EXEC_FLOP_PER_PASS[tform],
+                             "dense_q_flop_per_pass": DENSE_Q_FLOP_PER_PASS,
+                             "dense_q_equiv_tflops": passes * DENSE_Q_FLOP_PER_PASS
+                             / (t_ms / 1e3) / 1e12,
+                             "peak_source": "dense BF16, measured burst%s"
+                                            % ("" if tform == "tc_bf16x3"
+                                               else " x 1/2 (TF32 runs at half the BF16 rate)"),
+                             "note": "executed MMA FLOPs over the whole launch; the kernel "
+                                     "waits on its four MMA round trips per pass, so the "
+                                     "tensor pipe is far from its bound"},
                 "_solver": ts_}
 
     # learned warm start: network inference on the stack, then the spectral

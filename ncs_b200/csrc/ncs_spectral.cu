@@ -264,8 +264,10 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             }
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
+                // (1/512) / (lam + 512 alpha mk) = 1 / (512 lam + 512^2 alpha mk): the
+                // power-of-two factor moves inside exactly
                 const float wgt = first ? alpha * mk[i]
-                                        : (1.0f / 512.0f) * rcp_fast(fmaf(two_alpha_256, mk[i], lam));
+                                        : rcp_fast(fmaf(512.0f * two_alpha_256, mk[i], 512.0f * lam));
                 spec[i] = make_float2(spec[i].x * wgt, spec[i].y * wgt);
             }
             warp_fft_inv(spec, p, ws, G);

@@ -707,13 +707,15 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                     bool cross = false;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
+                        // log(max(ni, F)) - log(max(ai, F)) = log1p((max(ni, F) - A) / A),
+                        // A = max(ai, F); above the floor the numerator is the exact
+                        // step tp (branch free: one select instead of a branch)
                         const float ai = u[i] + gm[i];
                         const float tp = t * p[i];
                         const float ni = ai + tp;
                         const bool in_dom = ai >= kFitMin && ni >= kFitMin;
                         const float A = fmaxf(ai, kFitMin);
-                        const float l =
-                            log1p_ls((in_dom ? tp : fmaxf(ni, kFitMin) - A) * rcp_fast(A));
+                        const float l = log1p_ls((in_dom ? tp : fmaxf(ni, kFitMin) - A) * rcp_fast(A));
                         cross |= (ai >= kFitMin) && (ni < kBarrierFrac * ai);
                         term += fmaf(-c[i], l, tp);
                     }

@@ -190,8 +190,10 @@ __device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8]
         const float sx = Z.x + Zm.x, dx = Z.x - Zm.x, sy = Z.y + Zm.y, dy = Z.y - Zm.y;
         float2 ev = make_float2(fmaf(L.sH, sy, sx), fmaf(-L.sH, dx, dy));
         if (Halve) ev = make_float2(0.5f * ev.x, 0.5f * ev.y);
-        const float2 w = w16(p);
-        e[p] = L.H ? cmul(ev, w) : ev;
+        // odd half: twiddle W16^p (p = 0: 1; p = 4: -i, exact)
+        if (p == 0) e[p] = ev;
+        else if (p == 4) e[p] = L.H ? mul_mi(ev) : ev;
+        else e[p] = L.H ? cmul(ev, w16(p)) : ev;
     }
     fft8_fwd(e);
 }
@@ -203,11 +205,10 @@ __device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8]
 // E_r - O_r.  The reader combines them, which costs no shuffles.
 __device__ __forceinline__ void warp_ifft_cols(float2 (&e)[8], WarpSmem& ws, const LaneGeo& L) {
     fft8_inv(e);
+    // odd half: conjugate twiddle (r = 0: 1; r = 4: i, exact)
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const float2 w = w16(r);
-        e[r] = L.H ? conjmul(e[r], w) : e[r];
-    }
+    for (int r = 1; r < 8; ++r)
+        e[r] = L.H ? (r == 4 ? mul_i(e[r]) : conjmul(e[r], w16(r))) : e[r];
     __syncwarp();  // every lane has read the row spectra
 #pragma unroll
     for (int r = 0; r < 8; ++r) ws.fb[r + 8 * L.H][L.KC] = e[r];
@@ -222,14 +223,16 @@ __device__ __forceinline__ void warp_ifft_row(float2 (&V)[4], float2 (&z)[4], co
         const float2 p = shfl_xor2(V[k], 1);
         V[k] = make_float2(fmaf(L.sB, V[k].x, p.x), fmaf(L.sB, V[k].y, p.y));
     }
-    const bool lower = L.Qd < 2, odd = (L.Qd & 1) != 0;
+    // butterfly of lanes Qd and Qd ^ 2: lower = own + i^odd partner, upper =
+    // partner - i^odd own.  The upper lane twiddles its own value before the
+    // exchange, so each lane adds sA times its (twiddled) value to what it
+    // receives: one select pair instead of three.
+    const bool upper_odd = L.Qd == 3;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const float2 p = shfl_xor2(V[k], 2);
-        const float2 src = lower ? p : V[k];
-        const float2 b = odd ? mul_i(src) : src;
-        const float2 other = lower ? V[k] : p;
-        V[k] = make_float2(fmaf(L.sA, b.x, other.x), fmaf(L.sA, b.y, other.y));
+        const float2 y = upper_odd ? mul_i(V[k]) : V[k];
+        const float2 p = shfl_xor2(y, 2);
+        V[k] = make_float2(fmaf(L.sA, y.x, p.x), fmaf(L.sA, y.y, p.y));
     }
     V[1] = conjmul(V[1], L.tw1);
     V[2] = conjmul(V[2], L.tw2);

@@ -42,9 +42,41 @@ using namespace warp;
 
 namespace {
 
-// Per-warp shared memory: the common block, then s, y and Q s history.
+// Per-warp shared memory: the common block, the s, y and Q s history, then
+// the tile's pixel terms c = d + gamma and gamma.
 __host__ __device__ constexpr size_t spec_warp_bytes(int m) {
-    return ((sizeof(WarpSmem) + 15) / 16) * 16 + 3 * (size_t)m * 32 * 2 * sizeof(float4);
+    return ((sizeof(WarpSmem) + 15) / 16) * 16 + (3 * (size_t)m + 2) * 32 * 2 * sizeof(float4);
+}
+
+// A history vector (s, y or Q s) is stored as [half][lane] float4s, so that
+// each 128-bit access of the warp covers 512 consecutive bytes without bank
+// conflicts (lane-major pairs of float4s would put two lanes on each bank).
+__device__ __forceinline__ void load_hist(const float4* h, int lane, float (&x)[8]) {
+    const float4 a = h[lane], b = h[32 + lane];
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+__device__ __forceinline__ void store_hist(float4* h, int lane, const float (&x)[8]) {
+    h[lane] = make_float4(x[0], x[1], x[2], x[3]);
+    h[32 + lane] = make_float4(x[4], x[5], x[6], x[7]);
+}
+
+// The pixel terms c and gamma of a lane's 8 pixels live in the warp's shared
+// memory as [c low, c high, gamma low, gamma high][lane] float4s (each
+// access is 32 consecutive 16-byte words) and are re-read at every use.
+// Keeping them out of the loop-carried registers measured 2.6 % faster at
+// the same occupancy: the solver is issue-bound and the freed registers let
+// the compiler schedule the transforms and the line search more tightly.
+// The loads are volatile so that they are not hoisted back out of the loop
+// (the row-stage twiddles are re-read from a table the same way).
+__device__ __forceinline__ void load_terms(const float4* t, int lane, float (&c)[8],
+                                           float (&gm)[8]) {
+    const float4 c0 = lds_v4_volatile(t + lane), c1 = lds_v4_volatile(t + 32 + lane);
+    const float4 g0 = lds_v4_volatile(t + 64 + lane), g1 = lds_v4_volatile(t + 96 + lane);
+    c[0] = c0.x; c[1] = c0.y; c[2] = c0.z; c[3] = c0.w;
+    c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
+    gm[0] = g0.x; gm[1] = g0.y; gm[2] = g0.z; gm[3] = g0.w;
+    gm[4] = g1.x; gm[5] = g1.y; gm[6] = g1.z; gm[7] = g1.w;
 }
 
 // Per-stack pointers and geometry: the kernel parameters of a single-stack
@@ -86,20 +118,25 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
     float4* hs = reinterpret_cast<float4*>(wbase + ((sizeof(WarpSmem) + 15) / 16) * 16);
     float4* hy = hs + (size_t)mcap * 64;
     float4* hq = hy + (size_t)mcap * 64;
+    float4* terms = hq + (size_t)mcap * 64;  // c and gamma, see load_terms
 
     __shared__ StackDesc sdesc[kWarps];  // Batch: each warp's current stack
-    const LaneGeo G = lane_geo(lane);
-    // M^2/256 at this lane's 8 spectral positions: the CTA's shared table, or
-    // the current stack's lane-layout table (Batch); read once per pass
-    const float4* mkp = reinterpret_cast<const float4*>(mtab) + lane * 2;
+    __shared__ TwiddleTable s_tw;
+    fill_twiddles(s_tw, threadIdx.x);  // visible after the __syncthreads below
+    const LaneGeo G = lane_geo(lane);  // its twiddles are re-read from s_tw
+    // M^2/256 at this lane's 8 spectral positions, read once per pass: the
+    // CTA's shared table as [half][lane] float4s (conflict-free), or the
+    // current stack's table in global memory, lane-major (Batch)
+    const float4* mkp = Batch ? nullptr : reinterpret_cast<const float4*>(mtab) + lane;
     float alpha = a.alpha, two_alpha = 2.0f * a.alpha, two_alpha_256 = 512.0f * a.alpha;
     if constexpr (!Batch) {
         for (int idx = threadIdx.x; idx < 256; idx += blockDim.x) {
             const int L = idx >> 3, i = idx & 7;
-            mtab[idx] = a.msq[(2 * bitrev3(i) + (L & 1)) * 16 + (L >> 1)];
+            mtab[(i >> 2) * 128 + L * 4 + (i & 3)] =
+                a.msq[(2 * bitrev3(i) + (L & 1)) * 16 + (L >> 1)];
         }
-        __syncthreads();
     }
+    __syncthreads();
 
     for (;;) {
         unsigned long long tk = 0;
@@ -125,7 +162,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
         }
 
         // ---- gather the tile (segmentation, ncs.c:66-113) ---------------------
-        float d[8], gm[8], u[8];
+        float d[8], gam[8], u[8];
         int f = 0, ox = 0, oy = 0, own_r = 0, own_c = 0;
         if (a.tile_mode) {
             const long long base = tile * kPix;
@@ -135,7 +172,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 for (int s = 0; s < 2; ++s) {
                     const int off = (G.P + 8 * s) * kTile + G.Qd + 4 * j;
                     d[2 * j + s] = __ldg(a.data + base + off);
-                    gm[2 * j + s] = __ldg(a.gamma + base + off);
+                    gam[2 * j + s] = __ldg(a.gamma + base + off);
                     u[2 * j + s] = Warm ? __ldg(a.u0 + base + off) : d[2 * j + s];
                 }
         } else {
@@ -157,7 +194,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 for (int j = 0; j < 4; ++j) {
                     const int col = clampi(oy + G.Qd + 4 * j - 1, 0, sg.W - 1);
                     d[2 * j + s] = __ldg(img + row * sg.W + col);
-                    gm[2 * j + s] = __ldg(gmap + row * sg.W + col);
+                    gam[2 * j + s] = __ldg(gmap + row * sg.W + col);
                     u[2 * j + s] = d[2 * j + s];
                 }
             }
@@ -193,9 +230,12 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 }
             }
         };
-        float c[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) c[i] = d[i] + gm[i];
+        __syncwarp();  // the previous tile's terms are no longer read
+        terms[lane] = make_float4(d[0] + gam[0], d[1] + gam[1], d[2] + gam[2], d[3] + gam[3]);
+        terms[32 + lane] = make_float4(d[4] + gam[4], d[5] + gam[5], d[6] + gam[6], d[7] + gam[7]);
+        terms[64 + lane] = make_float4(gam[0], gam[1], gam[2], gam[3]);
+        terms[96 + lane] = make_float4(gam[4], gam[5], gam[6], gam[7]);
+        __syncwarp();
 
         // ---- preconditioned L-BFGS ---------------------------------------------
         // Pass 0 transforms u (v = 2 alpha Q u, initial gradient); later passes
@@ -238,7 +278,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                         if (i == 0 && sg_fresh) {
                             dot = -sg_newest;  // q = -g here
                         } else {
-                            load8(hs + slot * 64 + lane * 2, hv);
+                            load_hist(hs + slot * 64, lane, hv);
                             float acc = 0.0f;
 #pragma unroll
                             for (int e = 0; e < 8; ++e) acc = fmaf(hv[e], q[e], acc);
@@ -246,7 +286,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                         }
                         const float ai = rho[i] * dot;
                         al[i] = ai;
-                        load8(hy + slot * 64 + lane * 2, hv);
+                        load_hist(hy + slot * 64, lane, hv);
 #pragma unroll
                         for (int e = 0; e < 8; ++e) q[e] = fmaf(-ai, hv[e], q[e]);
                     }
@@ -255,10 +295,11 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             // spectral step: p = H0 q (pass 0: 2 alpha Q u) by one forward and
             // one inverse transform; the weights are real and symmetric in k.
             float2 spec[8];
-            warp_fft_fwd<false>(q, spec, ws, G);  // 2 F q: the weights hold the 1/2
+            warp_fft_fwd<false>(q, spec, ws, with_twiddles(G, s_tw));  // 2 F q: the weights hold the 1/2
             float mk[8];
             {
-                const float4 m0 = Batch ? __ldg(mkp) : mkp[0], m1 = Batch ? __ldg(mkp + 1) : mkp[1];
+                const float4 m0 = Batch ? __ldg(mkp) : mkp[0];
+                const float4 m1 = Batch ? __ldg(mkp + 1) : mkp[32];
                 mk[0] = m0.x; mk[1] = m0.y; mk[2] = m0.z; mk[3] = m0.w;
                 mk[4] = m1.x; mk[5] = m1.y; mk[6] = m1.z; mk[7] = m1.w;
             }
@@ -270,7 +311,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                                         : rcp_fast(fmaf(512.0f * two_alpha_256, mk[i], 512.0f * lam));
                 spec[i] = make_float2(spec[i].x * wgt, spec[i].y * wgt);
             }
-            warp_fft_inv(spec, p, ws, G);
+            warp_fft_inv(spec, p, ws, with_twiddles(G, s_tw));
             if (!first) {  // w = 2 alpha Q H0 q = q - lambda H0 q
                 if (two_alpha > 0.0f) {
 #pragma unroll
@@ -289,8 +330,9 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     // bound is <= 0 the proposal is accepted at once, without
                     // transforming d.  Otherwise keep v0 and transform d next
                     // for the exact comparison.
-                    float dd[8];
+                    float dd[8], c[8], gm[8];
                     load_d(dd);
+                    load_terms(terms, lane, c, gm);
                     float dl = 0.0f, dq = 0.0f;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
@@ -313,8 +355,9 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     // f(u0) - f(d) = sum[(u0 - d) - c (log(u0 + gamma) - log(d + gamma))]
                     //                + alpha (u0'Q u0 - d'Q d);  p = 2 alpha Q d,
                     //                w = 2 alpha Q u0
-                    float dd[8];
+                    float dd[8], c[8], gm[8];
                     load_d(dd);
+                    load_terms(terms, lane, c, gm);
                     float dl = 0.0f, dq = 0.0f;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
@@ -338,6 +381,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     start_pass = 0;
                 }
                 first = false;
+                float c[8], gm[8];
+                load_terms(terms, lane, c, gm);
                 float uu = 0.0f, gg = 0.0f, ll = 0.0f;
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
@@ -362,15 +407,15 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     int slot = newest - i;
                     if (slot < 0) slot += mcap;
                     float hv[8];
-                    load8(hy + slot * 64 + lane * 2, hv);
+                    load_hist(hy + slot * 64, lane, hv);
                     float acc = 0.0f;
 #pragma unroll
                     for (int e = 0; e < 8; ++e) acc = fmaf(hv[e], p[e], acc);
                     const float coef = al[i] - rho[i] * warp_sum_f(acc);
-                    load8(hs + slot * 64 + lane * 2, hv);
+                    load_hist(hs + slot * 64, lane, hv);
 #pragma unroll
                     for (int e = 0; e < 8; ++e) p[e] = fmaf(coef, hv[e], p[e]);
-                    load8(hq + slot * 64 + lane * 2, hv);
+                    load_hist(hq + slot * 64, lane, hv);
 #pragma unroll
                     for (int e = 0; e < 8; ++e) w[e] = fmaf(coef, hv[e], w[e]);
                 }
@@ -399,6 +444,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             float t = 1.0f;
             bool ok = false;
             for (int trial = 0; trial < 64; ++trial) {
+                float c[8], gm[8];
+                load_terms(terms, lane, c, gm);
                 float term = 0.0f;
                 bool cross = false;
 #pragma unroll
@@ -428,7 +475,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             if (!ok) { status = kMinimumStep; break; }
 
             // accept; new pair (s, y, Q s = t w)
-            float s[8], y[8];
+            float s[8], y[8], c[8], gm[8];
+            load_terms(terms, lane, c, gm);
             float sy = 0.0f, uu = 0.0f, gg = 0.0f, ll = 0.0f, mv = 0.0f, sg = 0.0f;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
@@ -467,9 +515,9 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             if (sy > 0.0f) {
                 sg_newest = sg;
                 newest = newest + 1 == mcap ? 0 : newest + 1;
-                store8(hs + newest * 64 + lane * 2, s);
-                store8(hy + newest * 64 + lane * 2, y);
-                store8(hq + newest * 64 + lane * 2, w);
+                store_hist(hs + newest * 64, lane, s);
+                store_hist(hy + newest * 64, lane, y);
+                store_hist(hq + newest * 64, lane, w);
 #pragma unroll
                 for (int i = MaxM - 1; i > 0; --i) rho[i] = rho[i - 1];
                 rho[0] = rcp_fast(sy);
@@ -479,6 +527,8 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 
         // ---- outputs -----------------------------------------------------------
         if (a.cost) {
+            float c[8], gm[8];
+            load_terms(terms, lane, c, gm);
             double e0 = 0.0, e1 = 0.0;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {

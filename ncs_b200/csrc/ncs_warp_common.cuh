@@ -144,6 +144,43 @@ __device__ __forceinline__ LaneGeo lane_geo(int lane) {
     return g;
 }
 
+// 128-bit shared-memory load that the compiler neither hoists out of a loop
+// nor merges with an earlier one: a value re-read where it is used instead of
+// held in a register across the solver's loop.
+__device__ __forceinline__ float4 lds_v4_volatile(const void* p) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"((unsigned)__cvta_generic_to_shared(p)));
+    return v;
+}
+
+// The row-stage twiddles of the four lane classes Qd, for kernels that re-read
+// them before each transform rather than keep six registers through the
+// solve: v[Qd][0] = (tw1, tw2), v[Qd][1] = (tw3, unused).
+struct TwiddleTable {
+    float4 v[4][2];
+};
+
+// Threads 0..3 of the CTA fill the table (a __syncthreads must follow).
+__device__ __forceinline__ void fill_twiddles(TwiddleTable& t, int tid) {
+    if (tid < 4) {
+        const LaneGeo g = lane_geo(tid);
+        t.v[tid][0] = make_float4(g.tw1.x, g.tw1.y, g.tw2.x, g.tw2.y);
+        t.v[tid][1] = make_float4(g.tw3.x, g.tw3.y, 0.0f, 0.0f);
+    }
+}
+
+// A copy of the lane geometry with the twiddles freshly read from the table.
+__device__ __forceinline__ LaneGeo with_twiddles(const LaneGeo& g, const TwiddleTable& t) {
+    LaneGeo r = g;
+    const float4 a = lds_v4_volatile(&t.v[g.Qd][0]), b = lds_v4_volatile(&t.v[g.Qd][1]);
+    r.tw1 = make_float2(a.x, a.y);
+    r.tw2 = make_float2(a.z, a.w);
+    r.tw3 = make_float2(b.x, b.y);
+    return r;
+}
+
 // Forward half of the 16x16 transform: lane (KC = L>>1, H = L&1) ends with
 // the spectrum X[2 bitrev3(i) + H][KC] of its 8 pixels' tile in e[i]
 // (unnormalised; with Halve = false, 2 X, for callers that fold the factor

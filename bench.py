@@ -67,13 +67,13 @@ for _f in ("tc_tf32", "tc_bf16x3"):
 # kernel on stack512 at 64 frames, at the commit named in WARP_INST_MEASURED.
 # Used for the issue-rate bound, the one that limits these kernels; a kernel
 # changed since that commit needs a new capture.
-WARP_INST_PER_PASS = {"spectral": 663587876 / (87616 * 6.047982),
+WARP_INST_PER_PASS = {"spectral": 633046900 / (87616 * 6.047982),
                       "plain": 2546982558 / (87616 * 15.5539),
                       "plain_wg": 7479161369 / (87616 * 15.5538)}
 # multiply-adds x 2 of the warm-start network per 16x16 tile:
 # 256 px x 9 taps x (2*32 + 32*32 + 32*32 + 32*1)
 INFER_FLOP_PER_TILE = 2 * 256 * 9 * (2 * 32 + 32 * 32 + 32 * 32 + 32 * 1)
-WARP_INST_MEASURED = {"spectral": "263df4b", "plain": "cf1c4d5", "plain_wg": "cf1c4d5"}
+WARP_INST_MEASURED = {"spectral": "04b93ce", "plain": "cf1c4d5", "plain_wg": "cf1c4d5"}
 KERNEL = {"plain": "ncs_warp_kernel", "plain_wg": "ncs_plain_kernel",
           "spectral": "ncs_spectral_kernel", "tc_tf32": "ncs_tc_kernel<TF32>",
           "tc_bf16x3": "ncs_tc_kernel<BF16x3>"}
@@ -718,16 +718,28 @@ def run_ours(args, world, rank, local):
         f1.record(stream)
         torch.cuda.synchronize()
         fp32_ms = f0.elapsed_time(f1)
+        fp8 = args.warm_precision == "fp8"
+        nws = max(1, min(args.steps, 3))
+        # tensor-core inference alone in both operand formats
+        infer_ms = {}
+        for prec in ("bf16", "fp8"):
+            net.propose_stack_tc(images, gamma, out=u0, fp8=prec == "fp8")
+            torch.cuda.synchronize()
+            f0.record(stream)
+            for _ in range(nws):
+                net.propose_stack_tc(images, gamma, out=u0, fp8=prec == "fp8")
+            f1.record(stream)
+            torch.cuda.synchronize()
+            infer_ms[prec] = f0.elapsed_time(f1) / nws
         # tensor-core inference + solve: the timed leg
-        u0, tc_status = net.propose_stack_tc(images, gamma, out=u0)
+        u0, tc_status = net.propose_stack_tc(images, gamma, out=u0, fp8=fp8)
         _, w_it, w_st, w_cost, w_ev, w_fb = solver.reduce_noise_from(images, gamma, u0, out=out)
         barrier(world)
         torch.cuda.synchronize()
-        nws = max(1, min(args.steps, 3))
         we = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nws + 1)]
         we[0].record(stream)
         for k in range(nws):
-            net.propose_stack_tc(images, gamma, out=u0)
+            net.propose_stack_tc(images, gamma, out=u0, fp8=fp8)
             we[2 * k + 1].record(stream)
             solver.reduce_noise_from(images, gamma, u0, out=out, stats=False)
             we[2 * k + 2].record(stream)
@@ -738,11 +750,15 @@ def run_ours(args, world, rank, local):
         tot_ms = max_over_ranks(we[0].elapsed_time(we[-1]), world) / nws
         inf_flops = n_tiles * INFER_FLOP_PER_TILE
         pk_tensor = peaks()[0].get("bf16_tflops", 1590.0)  # dense BF16, measured burst
-        warm = {"network": "4 x conv3x3 2-32-32-32-1, ReLU, %d params (BF16 on the tensor "
-                           "cores)" % warmstart.N_PARAMS,
-                "kernels": "ncsb::nettc::infer_tc (tcgen05, BF16 x BF16 -> FP32 in TMEM), "
-                           "ncs_spectral_kernel<.., Warm>",
+        warm = {"network": "4 x conv3x3 2-32-32-32-1, ReLU, %d params (%s on the tensor "
+                           "cores)" % (warmstart.N_PARAMS, "E4M3" if fp8 else "BF16"),
+                "kernels": "ncsb::nettc::infer_tc<%s> (tcgen05, %s -> FP32 in TMEM), "
+                           "ncs_spectral_kernel<.., Warm>"
+                           % (("F8", "kind::f8f6f4 E4M3 x E4M3") if fp8
+                              else ("BF16", "kind::f16 BF16 x BF16")),
+                "precision": args.warm_precision,
                 "ms_infer_fp32_simt": fp32_ms,
+                "ms_infer_tc": infer_ms,
                 "ms_per_step": tot_ms, "ms_infer": inf_ms, "ms_solve": sol_ms,
                 "value": px / (tot_ms / 1e3) / 1e6,
                 "mean_iters": w_it.double().mean().item(),
@@ -750,7 +766,10 @@ def run_ours(args, world, rank, local):
                 "mean_evals": w_ev.double().mean().item(),
                 "fallback_frac": w_fb.double().mean().item(),
                 "infer_tflops": inf_flops / (inf_ms / 1e3) / 1e12,
-                "infer_tensor_frac": inf_flops / (inf_ms / 1e3) / 1e12 / pk_tensor,
+                "infer_tensor_frac": inf_flops / (inf_ms / 1e3) / 1e12
+                / (pk_tensor * (2.0 if fp8 else 1.0)),
+                "infer_tensor_peak": "dense %s, measured BF16 burst%s"
+                                     % ("E4M3" if fp8 else "BF16", " x 2" if fp8 else ""),
                 "infer_flop_per_tile": INFER_FLOP_PER_TILE,
                 "speedup_vs_photon_start": (total_ms / args.steps) / tot_ms,
                 "_cost": w_cost.cpu().numpy()}
@@ -764,7 +783,7 @@ def run_ours(args, world, rank, local):
             wt = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nws + 1)]
             wt[0].record(stream)
             for k in range(nws):
-                net.propose_stack_tc(images, gamma, out=u0)
+                net.propose_stack_tc(images, gamma, out=u0, fp8=fp8)
                 wt[2 * k + 1].record(stream)
                 tsv.reduce_noise_from(images, gamma, u0, out=out, stats=False)
                 wt[2 * k + 2].record(stream)
@@ -773,7 +792,8 @@ def run_ours(args, world, rank, local):
             wt_sol = sum(wt[2 * k + 1].elapsed_time(wt[2 * k + 2]) for k in range(nws)) / nws
             st_w = wt_st.cpu().numpy()
             warm["tc_form"] = {
-                "kernels": "ncsb::nettc::infer_tc, ncs_tc_kernel<TF32, Warm>",
+                "kernels": "ncsb::nettc::infer_tc<%s>, ncs_tc_kernel<TF32, Warm>"
+                           % ("F8" if fp8 else "BF16"),
                 "ms_per_step": wt_tot, "ms_solve": wt_sol,
                 "value": px / (wt_tot / 1e3) / 1e6,
                 "mean_iters": wt_it.double().mean().item(),
@@ -1009,15 +1029,16 @@ def run_mixed(args, world, rank, local):
     from ncs_b200 import warmstart
     if not args.no_warm_start and os.path.exists(warmstart.DEFAULT_WEIGHTS):
         net = warmstart.WarmStartNet.load(device=dev)
+        fp8 = args.warm_precision == "fp8"
         u0 = torch.empty((solver.batch_tiles, 16, 16), dtype=torch.float32, device=dev)
         tc_status = torch.zeros(1, dtype=torch.int32, device=dev)
         w_stats = solver.batch_stats()
-        net.propose_batch_tc(solver, out=u0, status=tc_status)
+        net.propose_batch_tc(solver, out=u0, status=tc_status, fp8=fp8)
         solver.batch_reduce_noise(u0_tiles=u0, stats=w_stats)
         torch.cuda.synchronize()
         wgraph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(wgraph):
-            net.propose_batch_tc(solver, out=u0, status=tc_status)
+            net.propose_batch_tc(solver, out=u0, status=tc_status, fp8=fp8)
             solver.batch_reduce_noise(u0_tiles=u0)
         for _ in range(args.warmup):
             wgraph.replay()
@@ -1035,11 +1056,13 @@ def run_mixed(args, world, rank, local):
         # the inference alone, for the split
         i0, i1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         i0.record(stream)
-        net.propose_batch_tc(solver, out=u0, status=tc_status)
+        net.propose_batch_tc(solver, out=u0, status=tc_status, fp8=fp8)
         i1.record(stream)
         torch.cuda.synchronize()
-        warm = {"kernels": "ncsb::nettc::infer_tc over the batch's stack descriptors, then "
-                           "ncs_spectral_kernel<.., Warm, Batch>, one CUDA graph",
+        warm = {"kernels": "ncsb::nettc::infer_tc<%s> over the batch's stack descriptors, "
+                           "then ncs_spectral_kernel<.., Warm, Batch>, one CUDA graph"
+                           % ("F8" if fp8 else "BF16"),
+                "precision": args.warm_precision,
                 "ms_per_step": w_ms, "ms_infer": i0.elapsed_time(i1),
                 "value": sum_over_ranks(px, world) / (w_ms / 1e3) / 1e6,
                 "mean_iters": w_stats["iters"].double().mean().item(),
@@ -1051,12 +1074,12 @@ def run_mixed(args, world, rank, local):
         tsolver = ncs_b200.Solver(max_iters=200, mode="tc_tf32")
         touts = tsolver.batch_set(stacks)
         t_stats = tsolver.batch_stats()
-        net.propose_batch_tc(tsolver, out=u0, status=tc_status)
+        net.propose_batch_tc(tsolver, out=u0, status=tc_status, fp8=fp8)
         tsolver.batch_reduce_noise(u0_tiles=u0, stats=t_stats)
         torch.cuda.synchronize()
         tgraph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(tgraph):
-            net.propose_batch_tc(tsolver, out=u0, status=tc_status)
+            net.propose_batch_tc(tsolver, out=u0, status=tc_status, fp8=fp8)
             tsolver.batch_reduce_noise(u0_tiles=u0)
         for _ in range(args.warmup):
             tgraph.replay()
@@ -1072,8 +1095,8 @@ def run_mixed(args, world, rank, local):
         t_ms = max_over_ranks(t0.elapsed_time(t1), world) / nws
         st_t = t_stats["status"].cpu().numpy()
         warm["tc_form"] = {
-            "kernels": "ncsb::nettc::infer_tc, then ncs_tc_kernel<TF32, Warm, Batch>, one "
-                       "CUDA graph",
+            "kernels": "ncsb::nettc::infer_tc<%s>, then ncs_tc_kernel<TF32, Warm, Batch>, "
+                       "one CUDA graph" % ("F8" if fp8 else "BF16"),
             "ms_per_step": t_ms, "value": sum_over_ranks(px, world) / (t_ms / 1e3) / 1e6,
             "mean_iters": t_stats["iters"].double().mean().item(),
             "fallback_frac": t_stats["start"].double().mean().item(),
@@ -1345,6 +1368,8 @@ def main():
     ap.add_argument("--form", default="spectral", choices=sorted(KERNEL))
     ap.add_argument("--no-compare-plain", action="store_true",
                     help="skip timing the plain form on the same stack")
+    ap.add_argument("--warm-precision", choices=["fp8", "bf16"], default="fp8",
+                    help="operand format of the warm start's tensor-core inference")
     ap.add_argument("--no-warm-start", action="store_true",
                     help="skip the learned warm-start leg")
     ap.add_argument("--accuracy-tiles", type=int, default=256)

@@ -124,6 +124,7 @@ EXPORTS = [
     "ncsb_sim_render", "ncsb_sim_camera", "ncsb_sim_uniforms", "ncsb_reduce_noise_normalized",
     "ncsb_net_infer_stack_tc", "ncsb_net_infer_tiles_tc", "ncsb_genpsfparam",
     "ncsb_net_infer_batch_tc", "ncsb_reduce_noise_host",
+    "ncsb_net_infer_stack_tc_fp8", "ncsb_net_infer_tiles_tc_fp8", "ncsb_net_infer_batch_tc_fp8",
     "ncsb_reduce_noise_adu_typed", "ncsb_reduce_noise_adu_host", "ncsb_sim_ideal_image",
 ]
 
@@ -215,6 +216,12 @@ def load():
     lib.ncsb_net_infer_tiles_tc.restype = ctypes.c_int
     lib.ncsb_net_infer_batch_tc.argtypes = [vp, vp, vp, vp, vp]
     lib.ncsb_net_infer_batch_tc.restype = ctypes.c_int
+    lib.ncsb_net_infer_stack_tc_fp8.argtypes = [vp, vp, ci, ci, ci, vp, ci, vp, vp, vp]
+    lib.ncsb_net_infer_stack_tc_fp8.restype = ctypes.c_int
+    lib.ncsb_net_infer_tiles_tc_fp8.argtypes = [vp, vp, vp, i64, vp, vp, vp]
+    lib.ncsb_net_infer_tiles_tc_fp8.restype = ctypes.c_int
+    lib.ncsb_net_infer_batch_tc_fp8.argtypes = [vp, vp, vp, vp, vp]
+    lib.ncsb_net_infer_batch_tc_fp8.restype = ctypes.c_int
     lib.ncsb_reduce_noise_host.argtypes = [vp, vp, i32, i32, i32, vp, i32, vp, i32, i32, vp]
     lib.ncsb_reduce_noise_host.restype = ctypes.c_int
     lib.ncsb_net_infer_batch.argtypes = [vp, vp, vp, vp]

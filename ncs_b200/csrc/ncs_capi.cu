@@ -40,7 +40,7 @@ cudaError_t launch_gamma_map(const ncsb_calibration* cal, long long hw, float* g
 }  // namespace adu
 namespace nettc {
 int launch_batch(const float* params, const StackDesc* stacks, int n_stacks, long long n_tiles,
-                 float* u0, int32_t* status, cudaStream_t s);
+                 float* u0, int32_t* status, bool fp8, cudaStream_t s);
 }  // namespace nettc
 }  // namespace ncsb
 
@@ -813,7 +813,15 @@ int ncsb_net_infer_batch_tc(const float* params, const ncsb_handle* h, float* u0
     if (!params || !h || !u0_tiles) return NCSB_EINVAL;
     if (h->n_stacks < 1) return NCSB_EINVAL;
     return ncsb::nettc::launch_batch(params, h->d_stacks, h->n_stacks, h->batch_tiles, u0_tiles,
-                                     status, (cudaStream_t)stream);
+                                     status, false, (cudaStream_t)stream);
+}
+
+int ncsb_net_infer_batch_tc_fp8(const float* params, const ncsb_handle* h, float* u0_tiles,
+                                int32_t* status, void* stream) {
+    if (!params || !h || !u0_tiles) return NCSB_EINVAL;
+    if (h->n_stacks < 1) return NCSB_EINVAL;
+    return ncsb::nettc::launch_batch(params, h->d_stacks, h->n_stacks, h->batch_tiles, u0_tiles,
+                                     status, true, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -1,6 +1,7 @@
 // ncs_net_tc.cu -- warm-start network inference on the 5th-generation tensor
 // cores (tcgen05, sm_100a): the same network as ncs_net.cu's FP32 inference,
-// as implicit GEMMs with BF16 operands and FP32 accumulators in tensor memory.
+// as implicit GEMMs with BF16 or E4M3 (FP8) operands and FP32 accumulators in
+// tensor memory.
 //
 // Per 16x16 tile, positions live on the zero-bordered 18 x 18 plane
 // (row-major, index P).  The outputs of a 3x3 layer at the 288 positions
@@ -15,26 +16,45 @@
 // K = 18 taps x channels padded to 32.
 //
 // Shared-memory operands are K-major without swizzle: 8 consecutive
-// positions x 8 channels (16 B each) form a core matrix, so an activation
-// buffer is [channel chunk][position][8] BF16 with the leading byte offset
-// (between K halves) = the chunk stride and the stride byte offset (between
-// 8-row groups) = 128 B.  The epilogue reads each accumulator row from tensor
-// memory (thread t of the 128 owns row t of every M block), adds the bias,
-// applies ReLU, rounds to BF16 and writes the next layer's operand -- zeros at
-// the plane's border positions, which are the next layer's zero padding.
+// positions x 16 bytes (8 BF16 or 16 E4M3 channels) form a core matrix, so an
+// activation buffer is [channel chunk][position][16 B] with the leading byte
+// offset (between the K chunks of one MMA) = the chunk stride and the stride
+// byte offset (between 8-row groups) = 128 B.  The epilogue reads each
+// accumulator row from tensor memory (thread t of the 128 owns row t of every
+// M block), scales it, adds the bias, applies ReLU, rounds to the operand
+// format and writes the next layer's operand -- zeros at the plane's border
+// positions, which are the next layer's zero padding.
+//
+// E4M3 form (kind::f8f6f4, K = 32 per MMA: half the MMAs and half the
+// operand bytes of BF16, whose shared-memory reads bound that form): each
+// output channel's weights are scaled by max|w| / 448 before rounding, and each
+// layer's input by a fixed power of two (features x 8, hidden activations
+// x 4: 56 and 112 at E4M3's largest value, against 14 and 41 seen on full-
+// sensor tiles with hot pixels; larger values saturate).  The epilogue folds
+// both scales and the next layer's input scale into one multiply-add per
+// value.  Proposals differ from the FP32 network's by about 1e-2 of the
+// tile's scale s, and the solves from them take the same iterations.
 //
 // A layer's MMAs have finished reading their input before its epilogue
 // runs, so the epilogue overwrites that input in place: one activation
-// buffer per tile.  A CTA (4 warps) keeps two tiles in flight in two slots,
-// each with its buffer, 128 tensor-memory columns and an mbarrier, and
-// alternates between them: wait for a slot's MMAs, run its epilogue, issue
-// its next layer (or start its next tile), turn to the other slot -- so one
-// slot's epilogue runs while the other slot's MMAs do.  Two such CTAs share
-// an SM, persistent over tiles.  Thread 0 issues the MMAs and commits them
-// to the slot's mbarrier, which all threads wait on.  Every wait is bounded;
-// a timed-out wait sets the caller's status flag, drains the outstanding
-// MMAs with bounded waits, frees the tensor memory and ends the kernel.
+// buffer per tile.
+//
+// Warp-specialised and persistent, one CTA per SM (it holds all 512 tensor-
+// memory columns): four tile slots, each with its activation buffer, 128
+// tensor-memory columns and two mbarriers (full: the slot's MMAs of a layer
+// completed; ready: its next operand is written).  One warp issues MMAs: it
+// polls the slots' ready barriers in turn and issues the layer of whichever
+// slot is ready, committing to that slot's full barrier.  Two epilogue
+// warpgroups own two slots each and alternate between them: wait for the
+// slot's full barrier, read its accumulators, write the next operand (or the
+// proposal, after the last layer, and then the next tile's features), arrive
+// on its ready barrier.  No role waits for another at a CTA-wide barrier, so
+// the tensor core works on one slot while the epilogues of the others run.
+// Every wait is bounded; a timed-out wait sets the caller's status flag and
+// a shared abort flag that ends the other roles' loops, the outstanding MMAs
+// are drained with bounded waits and the tensor memory is freed.
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -45,34 +65,50 @@ namespace ncsb {
 namespace nettc {
 
 constexpr int kC = 32;
-constexpr int kThreads = 128;
+constexpr int kEpiGroups = 2;            // epilogue warpgroups per CTA
+constexpr int kCtaThreads = 128 * kEpiGroups + 32;  // + the MMA-issuing warp
 constexpr int kPlane = 18;
 constexpr int kQ = 384;                  // 3 M blocks of 128 output positions
 constexpr int kPos = 424;                // activation positions incl. shift margins
-constexpr int kChunkA = kPos * 16;       // bytes per 8-channel chunk of an activation buffer
-constexpr int kActBytes = 4 * kChunkA;   // 32 channels
-constexpr int kW1Bytes = 4 * 32 * 16;            // layer 1: K 32 x N 32
-constexpr int kWtapBytes = 4 * 32 * 16;          // layers 2, 3: per tap K 32 x N 32
-constexpr int kW4tapBytes = 4 * 16 * 16;         // layer 4: per tap K 32 x N 16
+constexpr int kChunkA = kPos * 16;       // bytes per 16-byte channel chunk of an activation buffer
 constexpr float kStartFrac = 0.05f;
-constexpr int kSlots = 2;                // tiles in flight per CTA
-constexpr unsigned kTmemCols = 256;      // 128 columns per slot
+constexpr int kSlots = 2 * kEpiGroups;   // tiles in flight per CTA, two per warpgroup
+constexpr unsigned kTmemCols = 512;      // 128 columns per slot
 constexpr long long kWaitTries = 1ll << 22;  // mbarrier polls before giving up (seconds)
-
-// shared-memory plan (bytes, all 128-B aligned)
-constexpr int kOffW1 = 0;
-constexpr int kOffW2 = kOffW1 + kW1Bytes;
-constexpr int kOffW3 = kOffW2 + 9 * kWtapBytes;
-constexpr int kOffW4 = kOffW3 + 9 * kWtapBytes;
-constexpr int kOffAct = kOffW4 + 9 * kW4tapBytes;             // one buffer per slot
+constexpr long long kIdlePolls = 1ll << 21;  // MMA warp: rounds over the slots with no work
 // the layer-1 im2col operand lives in the slot's activation buffer at
 // positions 19..402 -- the range every epilogue rewrites -- so the zero
 // border positions of the buffer are never touched
 constexpr int kIm2colPos = 19;
-constexpr int kOffBias = kOffAct + kSlots * kActBytes;        // 3 x 32 + 1 floats
-constexpr int kOffTile = kOffBias + 128 * 4;                  // per slot d, gamma, x0, x1
-constexpr int kTileBytes = 4 * 256 * 4;
-constexpr int kSmemBytes = kOffTile + kSlots * kTileBytes;
+constexpr int kTileBytes = 4 * 256 * 4;  // per slot d, gamma, x0, x1
+// E4M3 form: layer l's input is multiplied by this power of two before
+// rounding (the features, then the three hidden activations)
+__host__ __device__ constexpr float f8_in_scale(int l) { return l == 0 ? 8.0f : 4.0f; }
+constexpr float kF8Max = 448.0f;         // largest finite E4M3 value
+
+// Operand format and shared-memory plan (bytes, all 128-B aligned).  BF16:
+// 8 channels per 16-byte core-matrix row, K = 16 per MMA; E4M3: 16 channels
+// per row, K = 32 per MMA.  A B operand (weights) of N columns is
+// [K chunk][n][16 B], N x 16 bytes per chunk.
+template <bool F8>
+struct Fmt {
+    static constexpr int kPerChunk = F8 ? 16 : 8;    // channels per 16-byte row
+    static constexpr int kChunks = kC / kPerChunk;   // chunks per 32 channels
+    static constexpr int kKSteps = F8 ? 1 : 2;       // MMAs per 32 input channels
+    static constexpr int kActBytes = kChunks * kChunkA;
+    static constexpr int kW1Bytes = kChunks * 32 * 16;     // layer 1: K 32 x N 32
+    static constexpr int kWtapBytes = kChunks * 32 * 16;   // layers 2, 3: per tap K 32 x N 32
+    static constexpr int kW4tapBytes = kChunks * 16 * 16;  // layer 4: per tap K 32 x N 16
+    static constexpr int kOffW1 = 0;
+    static constexpr int kOffW2 = kOffW1 + kW1Bytes;
+    static constexpr int kOffW3 = kOffW2 + 9 * kWtapBytes;
+    static constexpr int kOffW4 = kOffW3 + 9 * kWtapBytes;
+    static constexpr int kOffAct = kOffW4 + 9 * kW4tapBytes;         // one buffer per slot
+    static constexpr int kOffScale = kOffAct + kSlots * kActBytes;   // 3 x 32 + 1 floats
+    static constexpr int kOffBias = kOffScale + 128 * 4;             // 3 x 32 + 1 floats
+    static constexpr int kOffTile = kOffBias + 128 * 4;
+    static constexpr int kSmemBytes = kOffTile + kSlots * kTileBytes;
+};
 
 struct Src {
     int tile_mode;
@@ -95,20 +131,34 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t 
            ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
-// kind::f16 instruction descriptor: D F32, A and B BF16, both K-major.
+// Instruction descriptors, D F32 (bits 4-5 = 1), A and B K-major, N / 8 at
+// bits 17-22, M / 16 at bits 24-28.  kind::f16: A and B BF16 (type 1 at bits
+// 7-9 and 10-12); kind::f8f6f4: A and B E4M3 (type 0).
+template <bool F8>
 __host__ __device__ constexpr uint32_t idesc(int M, int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+    return (1u << 4) | (F8 ? 0u : ((1u << 7) | (1u << 10))) | ((uint32_t)(N >> 3) << 17) |
            ((uint32_t)(M >> 4) << 24);
 }
 
+template <bool F8>
 __device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id,
                                     uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-        :
-        : "r"(tmem_d), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+    if constexpr (F8)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            :
+            : "r"(tmem_d), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(0u), "r"(0u), "r"(0u),
+              "r"(0u));
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            :
+            : "r"(tmem_d), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(0u), "r"(0u), "r"(0u),
+              "r"(0u));
 }
 
 __device__ __forceinline__ void commit(uint32_t bar) {
@@ -169,51 +219,116 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// Store 32 channels of one position into a [chunk][pos][8] BF16 buffer.
+// Two E4M3 values (round to nearest even, saturating at +-448), a in the
+// low byte.
+__device__ __forceinline__ uint32_t pack2_f8(float a, float b) {
+    return (uint32_t)__nv_cvt_float2_to_fp8x2(make_float2(a, b), __NV_SATFINITE, __NV_E4M3);
+}
+
+// Store 32 channels of one position into a [chunk][pos][16 B] buffer: 4
+// chunks of 8 BF16 or 2 chunks of 16 E4M3.
+template <bool F8>
 __device__ __forceinline__ void store_pos(unsigned char* buf, int chunk_bytes, int pos,
                                           const float (&v)[32]) {
+    if constexpr (F8) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        uint4 w;
-        w.x = pack2(v[8 * k + 0], v[8 * k + 1]);
-        w.y = pack2(v[8 * k + 2], v[8 * k + 3]);
-        w.z = pack2(v[8 * k + 4], v[8 * k + 5]);
-        w.w = pack2(v[8 * k + 6], v[8 * k + 7]);
-        *reinterpret_cast<uint4*>(buf + k * chunk_bytes + pos * 16) = w;
+        for (int k = 0; k < 2; ++k) {
+            uint4 w;
+            const float* c = v + 16 * k;
+            w.x = pack2_f8(c[0], c[1]) | (pack2_f8(c[2], c[3]) << 16);
+            w.y = pack2_f8(c[4], c[5]) | (pack2_f8(c[6], c[7]) << 16);
+            w.z = pack2_f8(c[8], c[9]) | (pack2_f8(c[10], c[11]) << 16);
+            w.w = pack2_f8(c[12], c[13]) | (pack2_f8(c[14], c[15]) << 16);
+            *reinterpret_cast<uint4*>(buf + k * chunk_bytes + pos * 16) = w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uint4 w;
+            w.x = pack2(v[8 * k + 0], v[8 * k + 1]);
+            w.y = pack2(v[8 * k + 2], v[8 * k + 3]);
+            w.z = pack2(v[8 * k + 4], v[8 * k + 5]);
+            w.w = pack2(v[8 * k + 6], v[8 * k + 7]);
+            *reinterpret_cast<uint4*>(buf + k * chunk_bytes + pos * 16) = w;
+        }
     }
 }
 
-// The 54 MMAs of a 3x3 layer over one slot: 3 M blocks x 9 taps x 2 K steps,
-// every operand offset and accumulate flag a compile-time constant (the
-// issuing thread is on the critical path: the other threads wait at the next
-// barrier while it issues).  NOut = 32, or 16 for the last layer.
-template <int NOut>
+// Element (k, n) of a weight operand with N columns, [K chunk][n][16 B]:
+// rounded to BF16, or divided by the column's scale and rounded to E4M3.
+template <bool F8>
+__device__ __forceinline__ void put_weight(unsigned char* base, int N, int k, int n, float w,
+                                           float inv_scale) {
+    if constexpr (F8) {
+        base[(k >> 4) * N * 16 + n * 16 + (k & 15)] =
+            __nv_cvt_float_to_fp8(w * inv_scale, __NV_SATFINITE, __NV_E4M3);
+    } else {
+        reinterpret_cast<__nv_bfloat16*>(base)[(k >> 3) * N * 8 + n * 8 + (k & 7)] =
+            __float2bfloat16_rn(w);
+    }
+}
+
+// The MMAs of a 3x3 layer over one slot: 3 M blocks x 9 taps x (2 K steps of
+// 16 BF16 channels, or 1 of 32 E4M3 channels), every operand offset and
+// accumulate flag a compile-time constant (the issuing thread is on the
+// critical path: the other threads wait at the next barrier while it
+// issues).  NOut = 32, or 16 for the last layer.
+template <bool F8, int NOut>
 __device__ __forceinline__ void issue_taps(uint32_t td, uint64_t a0, uint64_t b0) {
-    constexpr uint32_t id = idesc(128, NOut);
-    constexpr int tap_bytes = NOut == 32 ? kWtapBytes : kW4tapBytes;
+    using F = Fmt<F8>;
+    constexpr uint32_t id = idesc<F8>(128, NOut);
+    constexpr int tap_bytes = NOut == 32 ? F::kWtapBytes : F::kW4tapBytes;
     constexpr int wchunk = NOut * 16;
 #pragma unroll
     for (int m = 0; m < 3; ++m)
 #pragma unroll
         for (int tap = 0; tap < 9; ++tap)
 #pragma unroll
-            for (int ks = 0; ks < 2; ++ks) {
+            for (int ks = 0; ks < F::kKSteps; ++ks) {
                 const int pos = kPlane + 128 * m + (tap / 3 - 1) * kPlane + (tap % 3 - 1) + 1;
-                mma(td + m * NOut, a0 + (((2 * ks) * kChunkA + pos * 16) >> 4),
-                    b0 + ((tap * tap_bytes + (2 * ks) * wchunk) >> 4), id, (tap | ks) != 0);
+                mma<F8>(td + m * NOut, a0 + (((2 * ks) * kChunkA + pos * 16) >> 4),
+                        b0 + ((tap * tap_bytes + (2 * ks) * wchunk) >> 4), id, (tap | ks) != 0);
             }
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
+// Named barrier over one epilogue warpgroup (ids 1 and 2; 0 is __syncthreads).
+__device__ __forceinline__ void wg_sync(int id) {
+    asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory");
+}
+// The same barrier, true when p holds in all 128 threads.
+__device__ __forceinline__ bool wg_all(int id, bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(id)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+template <bool F8>
+__global__ void __launch_bounds__(kCtaThreads, 1)
     infer_tc(const Src src, const float* __restrict__ params, float* __restrict__ u0,
              int32_t* __restrict__ status) {
+    using F = Fmt<F8>;
     extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ __align__(8) uint64_t bar[kSlots];
+    __shared__ __align__(8) uint64_t full_bar[kSlots];   // a slot's layer MMAs completed
+    __shared__ __align__(8) uint64_t ready_bar[kSlots];  // a slot's next operand written
     __shared__ uint32_t tmem_base_s;
-    __shared__ float red[8];
-    const int t = threadIdx.x, warp = t >> 5;
+    __shared__ float red[kEpiGroups][8];
+    __shared__ float inv_wscale[4 * kC];  // E4M3: 1 / (column max |w| / 448), per layer
+    __shared__ int issued_s[kSlots], consumed_s[kSlots];
+    __shared__ volatile int abort_s;
+    const int t = threadIdx.x, warp = t >> 5, nthr = blockDim.x;
 
-    // ---- weights -> BF16 operand layouts, biases, zeroed activations --------
+    // ---- weights -> operand layouts, epilogue scales and biases, zeroed
+    //      activations ----------------------------------------------------------
     const float* w1 = params;
     const float* b1 = w1 + 2 * 9 * kC;
     const float* w2 = b1 + kC;
@@ -222,39 +337,72 @@ __global__ void __launch_bounds__(kThreads, 2)
     const float* b3 = w3 + kC * 9 * kC;
     const float* w4 = b3 + kC;
     const float* b4 = w4 + kC * 9;
-    __nv_bfloat16* sW1 = reinterpret_cast<__nv_bfloat16*>(sm + kOffW1);
-    // layer 1, B[k][co] with k = tap * 2 + ci (18 used of 32): [k chunk][co][8]
-    for (int i = t; i < 32 * 32; i += kThreads) {
+    // wt[ci][tap][co] of layer l (cin = 2 for layer 0; cout = 1 for layer 3)
+    auto weight = [&](int l, int ci, int tap, int co) -> float {
+        if (l == 0) return w1[(ci * 9 + tap) * kC + co];
+        if (l == 3) return co == 0 ? w4[ci * 9 + tap] : 0.0f;
+        return (l == 1 ? w2 : w3)[(ci * 9 + tap) * kC + co];
+    };
+    if (t < 4 * kC) {  // thread t: output column co = t & 31 of layer l = t >> 5
+        const int l = t >> 5, co = t & 31, cin = l == 0 ? 2 : kC;
+        float mx = 0.0f;
+        if (F8)
+            for (int ci = 0; ci < cin; ++ci)
+                for (int tap = 0; tap < 9; ++tap) mx = fmaxf(mx, fabsf(weight(l, ci, tap, co)));
+        inv_wscale[t] = mx > 0.0f ? kF8Max / mx : 1.0f;
+    }
+    __syncthreads();
+    // layer 1, B[k][co] with k = tap * 2 + ci (18 used of 32)
+    for (int i = t; i < 32 * 32; i += nthr) {
         const int k = i >> 5, co = i & 31;
-        const float v = k < 18 ? w1[((k & 1) * 9 + (k >> 1)) * kC + co] : 0.0f;
-        sW1[(k >> 3) * 256 + co * 8 + (k & 7)] = __float2bfloat16_rn(v);
+        put_weight<F8>(sm + F::kOffW1, 32, k, co, k < 18 ? weight(0, k & 1, k >> 1, co) : 0.0f,
+                       inv_wscale[co]);
     }
-    for (int l = 0; l < 2; ++l) {
-        const float* w = l == 0 ? w2 : w3;
-        __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(sm + (l == 0 ? kOffW2 : kOffW3));
-        for (int i = t; i < 9 * 32 * 32; i += kThreads) {
+    for (int l = 1; l < 3; ++l) {
+        unsigned char* sW = sm + (l == 1 ? F::kOffW2 : F::kOffW3);
+        for (int i = t; i < 9 * 32 * 32; i += nthr) {
             const int tap = i / 1024, rem = i - tap * 1024, ci = rem >> 5, co = rem & 31;
-            sW[tap * 1024 + (ci >> 3) * 256 + co * 8 + (ci & 7)] =
-                __float2bfloat16_rn(w[(ci * 9 + tap) * kC + co]);
+            put_weight<F8>(sW + tap * F::kWtapBytes, 32, ci, co, weight(l, ci, tap, co),
+                           inv_wscale[32 * l + co]);
         }
     }
-    {
-        __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(sm + kOffW4);
-        for (int i = t; i < 9 * 32 * 16; i += kThreads) {
-            const int tap = i / 512, rem = i - tap * 512, ci = rem >> 4, co = rem & 15;
-            sW[tap * 512 + (ci >> 3) * 128 + co * 8 + (ci & 7)] =
-                __float2bfloat16_rn(co == 0 ? w4[ci * 9 + tap] : 0.0f);
+    for (int i = t; i < 9 * 32 * 16; i += nthr) {
+        const int tap = i / 512, rem = i - tap * 512, ci = rem >> 4, co = rem & 15;
+        put_weight<F8>(sm + F::kOffW4 + tap * F::kW4tapBytes, 16, ci, co, weight(3, ci, tap, co),
+                       inv_wscale[96]);
+    }
+    // epilogue of layer l (0..2): act = max(acc * scale + bias, 0), stored as
+    // the next layer's operand; layer 3: y = acc * scale + bias.  E4M3: the
+    // accumulator carries the input and weight scales, the stored activation
+    // the next layer's input scale (a positive factor, so it commutes with
+    // the ReLU).
+    float* sScale = reinterpret_cast<float*>(sm + F::kOffScale);
+    float* sBias = reinterpret_cast<float*>(sm + F::kOffBias);
+    for (int i = t; i < 97; i += nthr) {
+        const int l = i >> 5;
+        const float b = i < 32 ? b1[i] : (i < 64 ? b2[i - 32] : (i < 96 ? b3[i - 64] : b4[0]));
+        if (F8) {
+            const float next = l < 3 ? f8_in_scale(l + 1) : 1.0f;
+            sScale[i] = next / (f8_in_scale(l) * inv_wscale[i]);
+            sBias[i] = b * next;
+        } else {
+            sScale[i] = 1.0f;
+            sBias[i] = b;
         }
     }
-    float* sBias = reinterpret_cast<float*>(sm + kOffBias);
-    for (int i = t; i < 97; i += kThreads)
-        sBias[i] = i < 32 ? b1[i] : (i < 64 ? b2[i - 32] : (i < 96 ? b3[i - 64] : b4[0]));
-    for (int i = t; i < kSlots * kActBytes / 16; i += kThreads)
-        reinterpret_cast<uint4*>(sm + kOffAct)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = t; i < kSlots * F::kActBytes / 16; i += nthr)
+        reinterpret_cast<uint4*>(sm + F::kOffAct)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (t == 0) {
-        for (int sl = 0; sl < kSlots; ++sl)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[sl]))
+        for (int sl = 0; sl < kSlots; ++sl) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full_bar[sl]))
                          : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(
+                             smem_u32(&ready_bar[sl]))
+                         : "memory");
+            issued_s[sl] = 0;
+            consumed_s[sl] = 0;
+        }
+        abort_s = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -267,248 +415,330 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
     fence_after();
     const uint32_t tmem = tmem_base_s;
-    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;  // this warp's TMEM lanes
-    const uint32_t sW1a = smem_u32(sm + kOffW1), sW2a = smem_u32(sm + kOffW2);
-    const uint32_t sW3a = smem_u32(sm + kOffW3), sW4a = smem_u32(sm + kOffW4);
-    const long long per_frame = (long long)src.tiles_x * src.tiles_y;
     const long long stride = (long long)kSlots * gridDim.x;  // tiles between a slot's tiles
-
-    // per-slot state, block-uniform: current tile, next layer to wait for,
-    // mbarrier phase, feature scale; and this thread's prefetched pixels
-    long long tile_s[kSlots] = {};
-    int layer_s[kSlots] = {};
-    uint32_t phase_s[kSlots] = {};
-    float scale_s[kSlots] = {};
-    float dv[kSlots][2] = {}, gv[kSlots][2] = {};
-    bool alive = true;
-
-    // this thread's two pixels of a tile (the solvers' segmentation)
-    auto gather = [&](long long tile, float (&dvo)[2], float (&gvo)[2]) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int p = t + 128 * h, r = p >> 4, c = p & 15;
-            if (src.tile_mode) {
-                dvo[h] = src.d[tile * 256 + p];
-                gvo[h] = src.gamma[tile * 256 + p];
-            } else {
-                const float* sd = src.d;
-                const float* sgam = src.gamma;
-                long long gstride = src.gamma_frame_stride, lt = tile, pf = per_frame;
-                int H = src.H, W = src.W, ty = src.tiles_y;
-                if (src.stacks) {  // batched: the last stack whose first tile is <= tile
-                    int lo = 0, hi = src.n_stacks - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (src.stacks[mid].tile_begin <= tile) lo = mid;
-                        else hi = mid - 1;
-                    }
-                    const StackDesc& st = src.stacks[lo];
-                    sd = st.data;
-                    sgam = st.gamma;
-                    gstride = st.gamma_frame_stride;
-                    lt = tile - st.tile_begin;
-                    H = st.H;
-                    W = st.W;
-                    ty = st.tiles_y;
-                    pf = (long long)st.tiles_x * st.tiles_y;
-                }
-                const int f = (int)(lt / pf);
-                const int rem = (int)(lt - (long long)f * pf);
-                const int ti = rem / ty, tj = rem - ti * ty;
-                const int yy = clampi(tile_origin(ti, H) + r - 1, 0, H - 1);
-                const int xx = clampi(tile_origin(tj, W) + c - 1, 0, W - 1);
-                dvo[h] = sd[(long long)f * H * W + (long long)yy * W + xx];
-                gvo[h] = sgam[(long long)f * gstride + (long long)yy * W + xx];
-            }
-        }
+    auto first_tile = [&](int sl) { return (long long)blockIdx.x * kSlots + sl; };
+    auto fail = [&]() {
+        abort_s = 1;
+        if (status) atomicExch(status, 1);
     };
 
-    // features of slot sl's tile from the gathered pixels, and the layer-1
-    // im2col operand in the slot's activation buffer (whose previous reader,
-    // the slot's last layer, has completed)
-    auto build = [&](int sl) {
-        float* sD = reinterpret_cast<float*>(sm + kOffTile + sl * kTileBytes);
-        float* sG = sD + 256;
-        float* sX0 = sG + 256;
-        float* sX1 = sX0 + 256;
-        float s1 = dv[sl][0] + dv[sl][1], s2 = dv[sl][0] * dv[sl][0] + dv[sl][1] * dv[sl][1];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-        }
-        __syncthreads();  // earlier readers of red and of this slot's tile data are done
+    if (warp == kEpiGroups * 4) {
+        // ==== the MMA-issuing warp: lane 0 serves the slots whose operand is
+        // ready, in turn; each slot runs layers 0..3 of its tiles in order ====
         if ((t & 31) == 0) {
-            red[warp] = s1;
-            red[4 + warp] = s2;
-        }
-        __syncthreads();
-        const float mu = (red[0] + red[1] + red[2] + red[3]) * (1.0f / 256.0f);
-        const float sd = sqrtf(fmaxf((red[4] + red[5] + red[6] + red[7]) * (1.0f / 256.0f) -
-                                     mu * mu, 0.0f)) + 1.0f;
-        scale_s[sl] = sd;
+            const uint32_t sW1a = smem_u32(sm + F::kOffW1), sW2a = smem_u32(sm + F::kOffW2);
+            const uint32_t sW3a = smem_u32(sm + F::kOffW3), sW4a = smem_u32(sm + F::kOffW4);
+            auto issue = [&](int sl, int ly) {
+                const uint32_t act_a = smem_u32(sm + F::kOffAct + sl * F::kActBytes);
+                const uint32_t td = tmem + (uint32_t)(sl * 128);
+                if (ly == 0) {
+                    constexpr uint32_t id = idesc<F8>(128, 32);
+                    const uint64_t a0 = sdesc(act_a + kIm2colPos * 16, kChunkA, 128);
+                    const uint64_t b0 = sdesc(sW1a, 512, 128);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int p = t + 128 * h;
-            sD[p] = dv[sl][h];
-            sG[p] = gv[sl][h];
-            sX0[p] = (dv[sl][h] - mu) / sd;
-            sX1[p] = sqrtf(fmaxf(dv[sl][h], 0.0f) + fmaxf(gv[sl][h], 0.0f)) / sd;
-        }
-        __syncthreads();
-        unsigned char* im2col = sm + kOffAct + sl * kActBytes + kIm2colPos * 16;
-#pragma unroll 1
-        for (int m = 0; m < 3; ++m) {
-            const int q = 128 * m + t, P = q + kPlane;
-            const int R = P / kPlane, Cc = P - R * kPlane;
-            float v[32];
+                    for (int m = 0; m < 3; ++m)
 #pragma unroll
-            for (int tap = 0; tap < 9; ++tap) {
-                const int rr = R + tap / 3 - 1, cc = Cc + tap % 3 - 1;
-                const bool in = rr >= 1 && rr <= 16 && cc >= 1 && cc <= 16;
-                const int px = in ? (rr - 1) * 16 + (cc - 1) : 0;
-                v[2 * tap] = in ? sX0[px] : 0.0f;
-                v[2 * tap + 1] = in ? sX1[px] : 0.0f;
+                        for (int ks = 0; ks < F::kKSteps; ++ks)
+                            mma<F8>(td + m * 32, a0 + (((2 * ks) * kChunkA + 128 * m * 16) >> 4),
+                                    b0 + (((2 * ks) * 512) >> 4), id, ks);
+                } else if (ly < 3) {
+                    issue_taps<F8, 32>(td, sdesc(act_a, kChunkA, 128),
+                                       sdesc(ly == 1 ? sW2a : sW3a, 512, 128));
+                } else {
+                    issue_taps<F8, 16>(td, sdesc(act_a, kChunkA, 128), sdesc(sW4a, 256, 128));
+                }
+                commit(smem_u32(&full_bar[sl]));
+                ++issued_s[sl];
+            };
+            // per-slot state (tile, layer, ready phase, slot) in registers,
+            // rotated so that the slot being polled is always the first
+            const long long n = src.n_tiles;
+            long long tA = first_tile(0), tB = first_tile(1), tC = first_tile(2),
+                      tD = first_tile(3);
+            int lA = 0, lB = 0, lC = 0, lD = 0, sA = 0, sB = 1, sC = 2, sD = 3;
+            uint32_t pA = 0, pB = 0, pC = 0, pD = 0;
+            int left = (tA < n) + (tB < n) + (tC < n) + (tD < n);
+            int misses = 0;
+            long long idle_rounds = 0;
+            while (left > 0) {
+                if (tA < n && try_wait(smem_u32(&ready_bar[sA]), pA)) {
+                    pA ^= 1u;
+                    fence_after();
+                    issue(sA, lA);
+                    if (++lA == 4) {
+                        lA = 0;
+                        tA += stride;
+                        left -= tA >= n;
+                    }
+                    misses = 0;
+                    idle_rounds = 0;
+                } else if (++misses == kSlots) {
+                    // a round over all slots found no work: back off so the
+                    // epilogue warps sharing this scheduler get its issue slots
+                    misses = 0;
+                    if (abort_s) break;
+                    if (++idle_rounds > kIdlePolls) {
+                        fail();
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                const long long tt = tA;
+                const int ll = lA, ss = sA;
+                const uint32_t pp = pA;
+                tA = tB; lA = lB; sA = sB; pA = pB;
+                tB = tC; lB = lC; sB = sC; pB = pC;
+                tC = tD; lC = lD; sC = sD; pC = pD;
+                tD = tt; lD = ll; sD = ss; pD = pp;
             }
-#pragma unroll
-            for (int k = 18; k < 32; ++k) v[k] = 0.0f;
-            store_pos(im2col, kChunkA, q, v);
         }
-    };
+    } else {
+        // ==== epilogue warpgroup g: slots 2g and 2g + 1 ======================
+        const int g = warp >> 2, tg = t & 127, bar_id = 1 + g;
+        const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;  // this warp's TMEM lanes
+        long long tile[2];
+        int layer[2] = {0, 0};
+        uint32_t phase[2] = {0u, 0u};
+        float scale[2] = {1.0f, 1.0f};
+        float dv[2][2] = {}, gv[2][2] = {};
 
-    // make the slot's operand writes visible to the tensor core, then thread
-    // 0 issues the layer's MMAs and commits them to the slot's mbarrier
-    auto issue = [&](int sl, int layer) {
-        fence_async_smem();
-        fence_before();
-        __syncthreads();
-        if (t == 0) {
-            // descriptors are built once per layer; an operand offset is added
-            // to the start-address field (shared addresses < 256 KB, so the
-            // 14-bit field never carries)
-            fence_after();
-            const uint32_t act_a = smem_u32(sm + kOffAct + sl * kActBytes);
-            const uint32_t td = tmem + (uint32_t)(sl * 128);
-            if (layer == 0) {
-                constexpr uint32_t id = idesc(128, 32);
-                const uint64_t a0 = sdesc(act_a + kIm2colPos * 16, kChunkA, 128);
-                const uint64_t b0 = sdesc(sW1a, 512, 128);
+        // this thread's two pixels of a tile (the solvers' segmentation)
+        auto gather = [&](long long tl, float (&dvo)[2], float (&gvo)[2]) {
 #pragma unroll
-                for (int m = 0; m < 3; ++m)
-#pragma unroll
-                    for (int ks = 0; ks < 2; ++ks)
-                        mma(td + m * 32, a0 + (((2 * ks) * kChunkA + 128 * m * 16) >> 4),
-                            b0 + (((2 * ks) * 512) >> 4), id, ks);
-            } else if (layer < 3) {
-                issue_taps<32>(td, sdesc(act_a, kChunkA, 128),
-                               sdesc(layer == 1 ? sW2a : sW3a, 512, 128));
-            } else {
-                issue_taps<16>(td, sdesc(act_a, kChunkA, 128), sdesc(sW4a, 256, 128));
-            }
-            commit(smem_u32(&bar[sl]));
-        }
-    };
-
-    // all threads: wait for the slot's committed MMAs (block-uniform outcome;
-    // on a timeout the phase stays, so the drain below waits on the same one)
-    auto sync_mma = [&](int sl) -> bool {
-        const bool ok = wait_bounded(smem_u32(&bar[sl]), phase_s[sl]);
-        const bool all = __syncthreads_and(ok) != 0;
-        if (all) phase_s[sl] ^= 1u;
-        fence_after();
-        return all;
-    };
-
-    // epilogue of slot sl's layer: this thread's accumulator row of each M block
-    auto epilogue = [&](int sl, int layer) {
-        const uint32_t td = tmem + lane_off + (uint32_t)(sl * 128);
-        if (layer < 3) {
-            const float* bias = sBias + 32 * layer;
-            unsigned char* dst = sm + kOffAct + sl * kActBytes;  // in place
-#pragma unroll 1
-            for (int m = 0; m < 3; ++m) {
-                const int q = 128 * m + t, P = q + kPlane;
-                const int R = P / kPlane, Cc = P - R * kPlane;
-                const bool valid = q < 288 && Cc >= 1 && Cc <= 16;
-                float v[32];
-                tmem_ld32(td + m * 32, v);
-#pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] = valid ? fmaxf(v[i] + bias[i], 0.0f) : 0.0f;
-                store_pos(dst, kChunkA, P + 1, v);
-            }
-        } else {
-            const float* sD = reinterpret_cast<const float*>(sm + kOffTile + sl * kTileBytes);
-            const float* sG = sD + 256;
-            const long long tile = tile_s[sl];
-            const float sd = scale_s[sl];
-#pragma unroll 1
-            for (int m = 0; m < 3; ++m) {
-                const int q = 128 * m + t, P = q + kPlane;
-                const int R = P / kPlane, Cc = P - R * kPlane;
-                float v[32];
-                tmem_ld32(td + m * 16, v);  // columns 0..15 used (+16 unused)
-                if (q < 288 && Cc >= 1 && Cc <= 16) {
-                    const int px = (R - 1) * 16 + (Cc - 1);
-                    const float y = v[0] + sBias[96];
-                    const float d = sD[px], g = sG[px];
-                    const float lo = kStartFrac * fmaxf(d + g, 1e-3f) - g;
-                    u0[tile * 256 + px] = fmaxf(fmaf(sd, y, d), lo);
+            for (int h = 0; h < 2; ++h) {
+                const int p = tg + 128 * h, r = p >> 4, c = p & 15;
+                if (src.tile_mode) {
+                    dvo[h] = src.d[tl * 256 + p];
+                    gvo[h] = src.gamma[tl * 256 + p];
+                } else {
+                    const float* sd = src.d;
+                    const float* sgam = src.gamma;
+                    long long gstride = src.gamma_frame_stride, lt = tl,
+                              pf = (long long)src.tiles_x * src.tiles_y;
+                    int H = src.H, W = src.W, ty = src.tiles_y;
+                    if (src.stacks) {  // batched: the last stack whose first tile is <= tl
+                        int lo = 0, hi = src.n_stacks - 1;
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (src.stacks[mid].tile_begin <= tl) lo = mid;
+                            else hi = mid - 1;
+                        }
+                        const StackDesc& st = src.stacks[lo];
+                        sd = st.data;
+                        sgam = st.gamma;
+                        gstride = st.gamma_frame_stride;
+                        lt = tl - st.tile_begin;
+                        H = st.H;
+                        W = st.W;
+                        ty = st.tiles_y;
+                        pf = (long long)st.tiles_x * st.tiles_y;
+                    }
+                    const int f = (int)(lt / pf);
+                    const int rem = (int)(lt - (long long)f * pf);
+                    const int ti = rem / ty, tj = rem - ti * ty;
+                    const int yy = clampi(tile_origin(ti, H) + r - 1, 0, H - 1);
+                    const int xx = clampi(tile_origin(tj, W) + c - 1, 0, W - 1);
+                    dvo[h] = sd[(long long)f * H * W + (long long)yy * W + xx];
+                    gvo[h] = sgam[(long long)f * gstride + (long long)yy * W + xx];
                 }
             }
-        }
-    };
+        };
 
-    // ---- start: each slot's first tile -------------------------------------
+        // features of slot sl's tile from the gathered pixels, and the layer-1
+        // im2col operand in the slot's activation buffer (whose previous
+        // reader, the slot's last layer, has completed)
+        auto build = [&](int k) {
+            const int sl = 2 * g + k;
+            float* sD = reinterpret_cast<float*>(sm + F::kOffTile + sl * kTileBytes);
+            float* sG = sD + 256;
+            float* sX0 = sG + 256;
+            float* sX1 = sX0 + 256;
+            float s1 = dv[k][0] + dv[k][1], s2 = dv[k][0] * dv[k][0] + dv[k][1] * dv[k][1];
 #pragma unroll
-    for (int sl = 0; sl < kSlots; ++sl) {
-        tile_s[sl] = (long long)blockIdx.x + (long long)sl * gridDim.x;
-        scale_s[sl] = 1.0f;
-        if (tile_s[sl] < src.n_tiles) gather(tile_s[sl], dv[sl], gv[sl]);
-    }
-#pragma unroll
-    for (int sl = 0; sl < kSlots; ++sl) {
-        if (tile_s[sl] >= src.n_tiles) continue;
-        build(sl);
-        issue(sl, 0);
-        if (tile_s[sl] + stride < src.n_tiles) gather(tile_s[sl] + stride, dv[sl], gv[sl]);
-    }
-
-    // ---- alternate between the slots until both run out of tiles ------------
-    for (;;) {
-        bool any = false;
-#pragma unroll
-        for (int sl = 0; sl < kSlots; ++sl) {
-            if (!alive || tile_s[sl] >= src.n_tiles) continue;
-            any = true;
-            if (!sync_mma(sl)) {
-                alive = false;
-                break;
+            for (int o = 16; o > 0; o >>= 1) {
+                s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                s2 += __shfl_xor_sync(0xffffffffu, s2, o);
             }
-            epilogue(sl, layer_s[sl]);
-            if (layer_s[sl] < 3) {
-                ++layer_s[sl];
-                issue(sl, layer_s[sl]);
+            wg_sync(bar_id);  // earlier readers of red and of this slot's tile data are done
+            if ((t & 31) == 0) {
+                red[g][warp & 3] = s1;
+                red[g][4 + (warp & 3)] = s2;
+            }
+            wg_sync(bar_id);
+            const float mu = (red[g][0] + red[g][1] + red[g][2] + red[g][3]) * (1.0f / 256.0f);
+            const float sd = sqrtf(fmaxf((red[g][4] + red[g][5] + red[g][6] + red[g][7]) *
+                                             (1.0f / 256.0f) - mu * mu,
+                                         0.0f)) + 1.0f;
+            scale[k] = sd;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int p = tg + 128 * h;
+                sD[p] = dv[k][h];
+                sG[p] = gv[k][h];
+                sX0[p] = (dv[k][h] - mu) / sd;
+                sX1[p] = sqrtf(fmaxf(dv[k][h], 0.0f) + fmaxf(gv[k][h], 0.0f)) / sd;
+            }
+            wg_sync(bar_id);
+            unsigned char* im2col = sm + F::kOffAct + sl * F::kActBytes + kIm2colPos * 16;
+            const float in_scale = F8 ? f8_in_scale(0) : 1.0f;
+#pragma unroll 1
+            for (int m = 0; m < 3; ++m) {
+                // rows 288..383 (block 2 beyond its first warp) are outside the
+                // plane: their layer-1 outputs are discarded, the operand unused
+                if (m == 2 && (warp & 3) != 0) break;
+                const int q = 128 * m + tg, P = q + kPlane;
+                const int R = P / kPlane, Cc = P - R * kPlane;
+                float v[32];
+#pragma unroll
+                for (int tap = 0; tap < 9; ++tap) {
+                    const int rr = R + tap / 3 - 1, cc = Cc + tap % 3 - 1;
+                    const bool in = rr >= 1 && rr <= 16 && cc >= 1 && cc <= 16;
+                    const int px = in ? (rr - 1) * 16 + (cc - 1) : 0;
+                    v[2 * tap] = in ? sX0[px] * in_scale : 0.0f;
+                    v[2 * tap + 1] = in ? sX1[px] * in_scale : 0.0f;
+                }
+#pragma unroll
+                for (int kk = 18; kk < 32; ++kk) v[kk] = 0.0f;
+                store_pos<F8>(im2col, kChunkA, q, v);
+            }
+        };
+
+        // the slot's operand writes (generic proxy) and tensor-memory reads
+        // are complete: hand the slot to the MMA warp
+        auto hand_over = [&](int k) {
+            fence_async_smem();
+            fence_before();
+            mbar_arrive(smem_u32(&ready_bar[2 * g + k]));
+        };
+
+        // epilogue of slot sl's layer: this thread's accumulator row of each M block
+        auto epilogue = [&](int k) {
+            const int sl = 2 * g + k, ly = layer[k];
+            const uint32_t td = tmem + lane_off + (uint32_t)(sl * 128);
+            if (ly < 3) {
+                float sc[32], bias[32];
+                {
+                    const float4* sc4 = reinterpret_cast<const float4*>(sScale + 32 * ly);
+                    const float4* b4 = reinterpret_cast<const float4*>(sBias + 32 * ly);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const float4 a = sc4[i], b = b4[i];
+                        sc[4 * i] = a.x; sc[4 * i + 1] = a.y; sc[4 * i + 2] = a.z; sc[4 * i + 3] = a.w;
+                        bias[4 * i] = b.x; bias[4 * i + 1] = b.y; bias[4 * i + 2] = b.z;
+                        bias[4 * i + 3] = b.w;
+                    }
+                }
+                unsigned char* dst = sm + F::kOffAct + sl * F::kActBytes;  // in place
+#pragma unroll 1
+                for (int m = 0; m < 3; ++m) {
+                    const int q = 128 * m + tg, P = q + kPlane;
+                    float v[32];
+                    if (m == 2 && (warp & 3) != 0) {
+                        // rows 288..383: the zero rows below the plane.  The
+                        // first layer's epilogue clears them (the im2col
+                        // operand had used them); later layers find them zero.
+                        if (ly == 0) {
+#pragma unroll
+                            for (int i = 0; i < 32; ++i) v[i] = 0.0f;
+                            store_pos<F8>(dst, kChunkA, P + 1, v);
+                        }
+                        break;
+                    }
+                    const int R = P / kPlane, Cc = P - R * kPlane;
+                    const bool valid = q < 288 && Cc >= 1 && Cc <= 16;
+                    tmem_ld32(td + m * 32, v);
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        v[i] = valid ? fmaxf(fmaf(v[i], sc[i], bias[i]), 0.0f) : 0.0f;
+                    store_pos<F8>(dst, kChunkA, P + 1, v);
+                }
             } else {
-                // tile done: its successor's pixels were gathered during its layers
-                tile_s[sl] += stride;
-                layer_s[sl] = 0;
-                if (tile_s[sl] < src.n_tiles) {
-                    build(sl);
-                    issue(sl, 0);
-                    if (tile_s[sl] + stride < src.n_tiles)
-                        gather(tile_s[sl] + stride, dv[sl], gv[sl]);
+                const float* sD =
+                    reinterpret_cast<const float*>(sm + F::kOffTile + sl * kTileBytes);
+                const float* sG = sD + 256;
+                const float sdv = scale[k];
+#pragma unroll 1
+                for (int m = 0; m < 3; ++m) {
+                    if (m == 2 && (warp & 3) != 0) break;  // rows 288..383: no pixels
+                    const int q = 128 * m + tg, P = q + kPlane;
+                    const int R = P / kPlane, Cc = P - R * kPlane;
+                    float v[32];
+                    tmem_ld32(td + m * 16, v);  // columns 0..15 used (+16 unused)
+                    if (q < 288 && Cc >= 1 && Cc <= 16) {
+                        const int px = (R - 1) * 16 + (Cc - 1);
+                        const float y = fmaf(v[0], sScale[96], sBias[96]);
+                        const float d = sD[px], gm = sG[px];
+                        const float lo = kStartFrac * fmaxf(d + gm, 1e-3f) - gm;
+                        u0[tile[k] * 256 + px] = fmaxf(fmaf(sdv, y, d), lo);
+                    }
                 }
             }
+        };
+
+        // ---- start: each slot's first tile ---------------------------------
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            tile[k] = first_tile(2 * g + k);
+            if (tile[k] < src.n_tiles) gather(tile[k], dv[k], gv[k]);
         }
-        if (!any || !alive) break;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (tile[k] >= src.n_tiles) continue;
+            build(k);
+            hand_over(k);
+            if (tile[k] + stride < src.n_tiles) gather(tile[k] + stride, dv[k], gv[k]);
+        }
+
+        // ---- alternate between the two slots until both run out of tiles ---
+        // (tile, layer and stop are uniform over the warpgroup: every branch
+        // below is taken by all 128 threads, as its named barriers require)
+        bool stop = false;
+        for (;;) {
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                if (tile[k] >= src.n_tiles) continue;
+                any = true;
+                const int sl = 2 * g + k;
+                bool ok = false;
+                for (long long i = 0; i < kWaitTries && !ok; ++i) {
+                    ok = try_wait(smem_u32(&full_bar[sl]), phase[k]);
+                    if (!ok && abort_s) break;
+                }
+                if (!wg_all(bar_id, ok)) {
+                    if (tg == 0) fail();
+                    stop = true;
+                    break;
+                }
+                phase[k] ^= 1u;
+                if (tg == 0) ++consumed_s[sl];
+                fence_after();
+                epilogue(k);
+                if (layer[k] < 3) {
+                    ++layer[k];
+                    hand_over(k);
+                } else {
+                    // tile done: its successor's pixels were gathered during its layers
+                    tile[k] += stride;
+                    layer[k] = 0;
+                    if (tile[k] < src.n_tiles) {
+                        build(k);
+                        hand_over(k);
+                        if (tile[k] + stride < src.n_tiles) gather(tile[k] + stride, dv[k], gv[k]);
+                    }
+                }
+            }
+            if (!any || stop) break;
+        }
     }
 
-    if (!alive) {
-        if (t == 0 && status) atomicExch(status, 1);
+    __syncwarp();
+    __syncthreads();
+    if (t == 0 && abort_s) {
         // drain: give every slot's outstanding MMAs a bounded time to complete
-#pragma unroll
         for (int sl = 0; sl < kSlots; ++sl)
-            if (tile_s[sl] < src.n_tiles) wait_bounded(smem_u32(&bar[sl]), phase_s[sl]);
+            for (int c = consumed_s[sl]; c < issued_s[sl]; ++c)
+                wait_bounded(smem_u32(&full_bar[sl]), (uint32_t)(c & 1));
     }
     fence_before();
     __syncthreads();
@@ -520,31 +750,34 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 }
 
-int launch(const Src& src, const float* params, float* u0, int32_t* status, cudaStream_t s) {
-    if (cudaFuncSetAttribute(infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) !=
-        cudaSuccess)
+template <bool F8>
+int launch_fmt(const Src& src, const float* params, float* u0, int32_t* status, cudaStream_t s) {
+    // at least 120 KB, so that a second CTA never shares an SM: each CTA
+    // allocates all of the SM's tensor memory
+    constexpr int kSmemBytes = Fmt<F8>::kSmemBytes > 120 * 1024 ? Fmt<F8>::kSmemBytes : 120 * 1024;
+    if (cudaFuncSetAttribute(infer_tc<F8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSmemBytes) != cudaSuccess)
         return NCSB_ECUDA;
-    // all of the unified L1 as shared memory, so two CTAs fit on an SM
-    cudaFuncSetAttribute(infer_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
+    cudaFuncSetAttribute(infer_tc<F8>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          cudaSharedmemCarveoutMaxShared);
     int dev = 0, sms = 1;
     if (cudaGetDevice(&dev) != cudaSuccess) return NCSB_ECUDA;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // CTAs per SM from the shared-memory budget (the occupancy query assumes the
-    // default carveout); more CTAs than fit only queue, results do not change
-    int per_sm_bytes = 0, reserved = 0;
-    cudaDeviceGetAttribute(&per_sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
-    int per_sm = per_sm_bytes / (kSmemBytes + 1024 + reserved);  // + static shared memory
-    per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
-    long long grid = (long long)sms * per_sm;
+    // one persistent CTA per SM (it allocates all 512 tensor-memory columns)
+    long long grid = sms;
     if (grid > (src.n_tiles + kSlots - 1) / kSlots) grid = (src.n_tiles + kSlots - 1) / kSlots;
-    infer_tc<<<(unsigned)grid, kThreads, kSmemBytes, s>>>(src, params, u0, status);
+    infer_tc<F8><<<(unsigned)grid, kCtaThreads, kSmemBytes, s>>>(src, params, u0, status);
     return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
 }
 
+int launch(const Src& src, const float* params, float* u0, int32_t* status, bool fp8,
+           cudaStream_t s) {
+    return fp8 ? launch_fmt<true>(src, params, u0, status, s)
+               : launch_fmt<false>(src, params, u0, status, s);
+}
+
 int launch_batch(const float* params, const StackDesc* stacks, int n_stacks, long long n_tiles,
-                 float* u0, int32_t* status, cudaStream_t s) {
+                 float* u0, int32_t* status, bool fp8, cudaStream_t s) {
     if (n_tiles == 0) return NCSB_OK;
     Src src{};
     src.stacks = stacks;
@@ -552,12 +785,19 @@ int launch_batch(const float* params, const StackDesc* stacks, int n_stacks, lon
     src.tiles_x = 1;
     src.tiles_y = 1;
     src.n_tiles = n_tiles;
-    return launch(src, params, u0, status, s);
+    return launch(src, params, u0, status, fp8, s);
 }
 
-static_assert(2 * (kSmemBytes + 2048) <= 228 * 1024, "two CTAs per SM");
-static_assert(2 * kTmemCols <= 512, "two CTAs' tensor memory fits an SM");
-static_assert(kOffAct % 16 == 0 && kActBytes % 16 == 0 && kOffTile % 16 == 0, "alignment");
+template <bool F8>
+constexpr bool plan_ok() {
+    using F = Fmt<F8>;
+    return F::kSmemBytes + 2048 <= 227 * 1024 && F::kOffAct % 128 == 0 &&
+           F::kActBytes % 128 == 0 && F::kOffScale % 16 == 0 && F::kOffTile % 16 == 0 &&
+           F::kOffW2 % 128 == 0 && F::kOffW3 % 128 == 0 && F::kOffW4 % 128 == 0;
+}
+static_assert(plan_ok<false>() && plan_ok<true>(), "one CTA per SM, aligned operands");
+static_assert(kTmemCols <= 512 && kSlots * 128 <= (int)kTmemCols, "slots' tensor memory");
+static_assert(kSlots == 4, "the MMA warp rotates four slots' state");
 static_assert(kIm2colPos + kQ <= kPos - 21, "im2col rows stay inside the rewritten range");
 
 }  // namespace nettc
@@ -566,11 +806,11 @@ static_assert(kIm2colPos + kQ <= kPos - 21, "im2col rows stay inside the rewritt
 using namespace ncsb::nettc;
 using ncsb::tiles_along;
 
-extern "C" {
+namespace {
 
-int ncsb_net_infer_stack_tc(const float* params, const float* images, int n_frames, int height,
-                            int width, const float* gamma, int gamma_per_frame, float* u0,
-                            int32_t* status, void* stream) {
+int infer_stack(const float* params, const float* images, int n_frames, int height, int width,
+                const float* gamma, int gamma_per_frame, float* u0, int32_t* status, bool fp8,
+                void* stream) {
     if (!params || !images || !gamma || !u0 || n_frames < 0 || height <= 0 || width <= 0)
         return NCSB_EINVAL;
     if (height < 14 || width < 14) return NCSB_ESIZE;
@@ -584,11 +824,11 @@ int ncsb_net_infer_stack_tc(const float* params, const float* images, int n_fram
     src.tiles_x = tiles_along(height);
     src.tiles_y = tiles_along(width);
     src.n_tiles = (long long)n_frames * src.tiles_x * src.tiles_y;
-    return launch(src, params, u0, status, (cudaStream_t)stream);
+    return launch(src, params, u0, status, fp8, (cudaStream_t)stream);
 }
 
-int ncsb_net_infer_tiles_tc(const float* params, const float* d, const float* gamma,
-                            int64_t n_tiles, float* u0, int32_t* status, void* stream) {
+int infer_tiles(const float* params, const float* d, const float* gamma, int64_t n_tiles,
+                float* u0, int32_t* status, bool fp8, void* stream) {
     if (!params || !d || !gamma || !u0 || n_tiles < 0) return NCSB_EINVAL;
     if (n_tiles == 0) return NCSB_OK;
     Src src{};
@@ -600,7 +840,35 @@ int ncsb_net_infer_tiles_tc(const float* params, const float* d, const float* ga
     src.H = 16;
     src.W = 16;
     src.n_tiles = n_tiles;
-    return launch(src, params, u0, status, (cudaStream_t)stream);
+    return launch(src, params, u0, status, fp8, (cudaStream_t)stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ncsb_net_infer_stack_tc(const float* params, const float* images, int n_frames, int height,
+                            int width, const float* gamma, int gamma_per_frame, float* u0,
+                            int32_t* status, void* stream) {
+    return infer_stack(params, images, n_frames, height, width, gamma, gamma_per_frame, u0,
+                       status, false, stream);
+}
+
+int ncsb_net_infer_stack_tc_fp8(const float* params, const float* images, int n_frames,
+                                int height, int width, const float* gamma, int gamma_per_frame,
+                                float* u0, int32_t* status, void* stream) {
+    return infer_stack(params, images, n_frames, height, width, gamma, gamma_per_frame, u0,
+                       status, true, stream);
+}
+
+int ncsb_net_infer_tiles_tc(const float* params, const float* d, const float* gamma,
+                            int64_t n_tiles, float* u0, int32_t* status, void* stream) {
+    return infer_tiles(params, d, gamma, n_tiles, u0, status, false, stream);
+}
+
+int ncsb_net_infer_tiles_tc_fp8(const float* params, const float* d, const float* gamma,
+                                int64_t n_tiles, float* u0, int32_t* status, void* stream) {
+    return infer_tiles(params, d, gamma, n_tiles, u0, status, true, stream);
 }
 
 }  // extern "C"

@@ -136,10 +136,10 @@ class WarmStartNet:
                 _stream_ptr(stream, self.device, self.params, out)), "ncsb_net_infer_batch")
         return out
 
-    def propose_stack_tc(self, images, gamma, out=None, stream=None):
-        """``propose_stack`` on the tensor cores (BF16 operands, FP32
-        accumulation).  Returns (proposals, status) with status a one-element
-        int32 device tensor, 1 if a tensor-core wait timed out."""
+    def propose_stack_tc(self, images, gamma, out=None, stream=None, fp8=False):
+        """``propose_stack`` on the tensor cores (BF16 operands, or E4M3 with
+        ``fp8``; FP32 accumulation).  Returns (proposals, status) with status
+        a one-element int32 device tensor, 1 if a tensor-core wait timed out."""
         T, H, W = images.shape
         per_frame = 1 if gamma.dim() == 3 else 0
         n = _lib.num_tiles(T, H, W)
@@ -148,13 +148,14 @@ class WarmStartNet:
         status = torch.zeros(1, dtype=torch.int32, device=self.device)
         images, gamma = images.contiguous(), gamma.contiguous()
         sp = _stream_ptr(stream, self.device, self.params, images, gamma, out, status)
+        name = "ncsb_net_infer_stack_tc_fp8" if fp8 else "ncsb_net_infer_stack_tc"
         with torch.cuda.device(self.device):
-            self._check(self.lib.ncsb_net_infer_stack_tc(
+            self._check(getattr(self.lib, name)(
                 _ptr(self.params), _ptr(images), T, H, W, _ptr(gamma), per_frame, _ptr(out),
-                _ptr(status), sp), "ncsb_net_infer_stack_tc")
+                _ptr(status), sp), name)
         return out, status
 
-    def propose_batch_tc(self, solver, out=None, status=None, stream=None):
+    def propose_batch_tc(self, solver, out=None, status=None, stream=None, fp8=False):
         """``propose_batch`` on the tensor cores; returns (proposals, status).
         With ``out`` and ``status`` (int32 [1], zeroed by the caller) given,
         one kernel is issued and nothing is allocated, so the call can be
@@ -164,23 +165,23 @@ class WarmStartNet:
             out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
         if status is None:
             status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        name = "ncsb_net_infer_batch_tc_fp8" if fp8 else "ncsb_net_infer_batch_tc"
         with torch.cuda.device(self.device):
-            self._check(self.lib.ncsb_net_infer_batch_tc(
+            self._check(getattr(self.lib, name)(
                 _ptr(self.params), solver._handle, _ptr(out), _ptr(status),
-                _stream_ptr(stream, self.device, self.params, out, status)),
-                "ncsb_net_infer_batch_tc")
+                _stream_ptr(stream, self.device, self.params, out, status)), name)
         return out, status
 
-    def propose_tiles_tc(self, d, gamma, stream=None):
+    def propose_tiles_tc(self, d, gamma, stream=None, fp8=False):
         n = d.shape[0]
         out = torch.empty((n, 16, 16), dtype=torch.float32, device=self.device)
         status = torch.zeros(1, dtype=torch.int32, device=self.device)
         d, gamma = d.contiguous(), gamma.contiguous()
         sp = _stream_ptr(stream, self.device, self.params, d, gamma, out, status)
+        name = "ncsb_net_infer_tiles_tc_fp8" if fp8 else "ncsb_net_infer_tiles_tc"
         with torch.cuda.device(self.device):
-            self._check(self.lib.ncsb_net_infer_tiles_tc(
-                _ptr(self.params), _ptr(d), _ptr(gamma), n, _ptr(out), _ptr(status), sp),
-                "ncsb_net_infer_tiles_tc")
+            self._check(getattr(self.lib, name)(
+                _ptr(self.params), _ptr(d), _ptr(gamma), n, _ptr(out), _ptr(status), sp), name)
         return out, status
 
     def propose_tiles(self, d, gamma, stream=None):

@@ -101,6 +101,48 @@ def propose(params, d, gamma):
     return numpy.maximum(d + sd[:, None, None] * y, lo)
 
 
+def round_e4m3(x):
+    """Round to the nearest E4M3 value (OCP FP8: 1 sign, 4 exponent bits with
+    bias 7, 3 mantissa bits, no infinities), ties to even, saturating at
+    +-448: the spacing is 2^(e-3) for |x| in [2^e, 2^(e+1)), e >= -6, and
+    2^-9 below 2^-6 (subnormals)."""
+    x = numpy.clip(numpy.asarray(x, dtype=numpy.float64), -448.0, 448.0)
+    a = numpy.abs(x)
+    e = numpy.floor(numpy.log2(numpy.where(a > 0, a, 1.0)))
+    q = numpy.exp2(numpy.maximum(e, -6.0) - 3.0)
+    return numpy.clip(numpy.rint(x / q) * q, -448.0, 448.0)
+
+
+# E4M3 inference: layer l's input is multiplied by IN_SCALE_FP8[l] before
+# rounding; each output column's weights are divided by max|w| / 448
+IN_SCALE_FP8 = (8.0, 4.0, 4.0, 4.0)
+
+
+def forward_fp8(params, x):
+    """Output of the network with E4M3 operands: inputs and weights rounded
+    after their scaling, products accumulated exactly (FP64 here), scales
+    undone before the bias (ncs_b200/csrc/ncs_net_tc.cu, E4M3 form)."""
+    cur = numpy.asarray(x, dtype=numpy.float64)
+    for li, ((w, b), (_, _, relu)) in enumerate(zip(unpack(params), LAYERS)):
+        mx = numpy.abs(w).max(axis=(0, 1))
+        sw = numpy.where(mx > 0, mx / 448.0, 1.0)
+        wq = round_e4m3(w / sw[None, None, :]) * sw[None, None, :]
+        xq = round_e4m3(cur * IN_SCALE_FP8[li]) / IN_SCALE_FP8[li]
+        z = conv(xq, wq, b)
+        cur = numpy.maximum(z, 0.0) if relu else z
+    return cur
+
+
+def propose_fp8(params, d, gamma):
+    """Proposal u0 [n, 16, 16] of the E4M3 tensor-core inference."""
+    x, mu, sd = features(d, gamma)
+    y = forward_fp8(params, x)[:, 0]
+    d = numpy.asarray(d, dtype=numpy.float64).reshape(-1, 16, 16)
+    g = numpy.asarray(gamma, dtype=numpy.float64).reshape(-1, 16, 16)
+    lo = START_FRAC * numpy.maximum(d + g, 1e-3) - g
+    return numpy.maximum(d + sd[:, None, None] * y, lo)
+
+
 def loss_and_grad(params, x, target):
     """MSE over all outputs and its gradient as a packed vector."""
     ws = unpack(params)

@@ -118,17 +118,19 @@ def test_batch_proposals_and_warm_solve(ncs, stacks):
         ss.close()
 
 
-def test_batch_tensor_core_proposals_equal_per_stack(ncs, stacks):
-    """The tensor-core inference over a batch reads each tile's stack descriptor
-    and otherwise runs the per-stack arithmetic: equal bit for bit."""
+@pytest.mark.parametrize("fp8", [False, True])
+def test_batch_tensor_core_proposals_equal_per_stack(ncs, stacks, fp8):
+    """The tensor-core inference over a batch (BF16 or E4M3 operands) reads
+    each tile's stack descriptor and otherwise runs the per-stack arithmetic:
+    equal bit for bit."""
     from ncs_b200 import warmstart
     net = warmstart.WarmStartNet.load()
     s = ncs.Solver()
     s.batch_set(stacks)
-    u0, status = net.propose_batch_tc(s)
+    u0, status = net.propose_batch_tc(s, fp8=fp8)
     per = []
     for st in stacks:
-        u, st_status = net.propose_stack_tc(st["images"], st["gamma"])
+        u, st_status = net.propose_stack_tc(st["images"], st["gamma"], fp8=fp8)
         assert int(st_status.item()) == 0
         per.append(u)
     torch.cuda.synchronize()

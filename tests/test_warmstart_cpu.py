@@ -95,6 +95,28 @@ def test_proposal_clamp_keeps_start_feasible():
     assert (u0 + g >= wr.START_FRAC * numpy.maximum(d + g, 1e-3) - 1e-12).all()
 
 
+def test_e4m3_rounding_matches_torch_float8():
+    """The oracle's E4M3 rounding (the checker of the tensor-core inference's
+    FP8 form) equals torch's float8_e4m3fn conversion: ties to even, the
+    subnormal spacing 2^-9 below 2^-6, saturation at +-448."""
+    rng = numpy.random.default_rng(3)
+    x = rng.normal(0.0, 1.0, 50000) * 10.0 ** rng.uniform(-4.0, 3.0, 50000)
+    edge = [0.0, -0.0, 448.0, -448.0, 464.0, 1e4, -1e4, 2.0 ** -9, 2.0 ** -10,
+            3 * 2.0 ** -11, 2.0 ** -6, 1.0625, 1.1875, 15.5, 240.0, 248.0]
+    x = numpy.concatenate([x, edge]).astype(numpy.float32).astype(numpy.float64)
+    ref = torch.from_numpy(numpy.clip(x, -448.0, 448.0).astype(numpy.float32)).to(
+        torch.float8_e4m3fn).to(torch.float64).numpy()
+    assert numpy.array_equal(wr.round_e4m3(x), ref)
+
+
+def test_fp8_forward_reduces_to_the_network_without_rounding(monkeypatch):
+    """forward_fp8 with the rounding switched off is the FP64 network: its
+    scales cancel exactly."""
+    p, x, target, d, g = random_case(seed=4)
+    monkeypatch.setattr(wr, "round_e4m3", lambda v: numpy.asarray(v, dtype=numpy.float64))
+    assert numpy.allclose(wr.forward_fp8(p, x), wr.forward(p, x)[3], rtol=1e-12, atol=1e-12)
+
+
 def test_parameter_layout():
     from ncs_b200 import _lib, warmstart
     assert warmstart.N_PARAMS == 19393

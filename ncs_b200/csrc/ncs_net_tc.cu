@@ -66,7 +66,7 @@ namespace nettc {
 
 constexpr int kC = 32;
 constexpr int kEpiGroups = 2;            // epilogue warpgroups per CTA
-constexpr int kCtaThreads = 128 * kEpiGroups + 32;  // + the MMA-issuing warp
+constexpr int kCtaThreads = 160 * kEpiGroups;  // + one MMA-issuing warp per warpgroup
 constexpr int kPlane = 18;
 constexpr int kQ = 384;                  // 3 M blocks of 128 output positions
 constexpr int kPos = 424;                // activation positions incl. shift margins
@@ -81,6 +81,10 @@ constexpr long long kIdlePolls = 1ll << 21;  // MMA warp: rounds over the slots 
 // border positions of the buffer are never touched
 constexpr int kIm2colPos = 19;
 constexpr int kTileBytes = 4 * 256 * 4;  // per slot d, gamma, x0, x1
+// last layer: per-tap partial sums D[P][tap] of the plane positions 0..323,
+// staged per warpgroup as [tap][P] floats for the shifted sum over the taps
+constexpr int kStagePos = 324;
+constexpr int kStageBytes = 9 * kStagePos * 4;
 // E4M3 form: layer l's input is multiplied by this power of two before
 // rounding (the features, then the three hidden activations)
 __host__ __device__ constexpr float f8_in_scale(int l) { return l == 0 ? 8.0f : 4.0f; }
@@ -98,16 +102,17 @@ struct Fmt {
     static constexpr int kActBytes = kChunks * kChunkA;
     static constexpr int kW1Bytes = kChunks * 32 * 16;     // layer 1: K 32 x N 32
     static constexpr int kWtapBytes = kChunks * 32 * 16;   // layers 2, 3: per tap K 32 x N 32
-    static constexpr int kW4tapBytes = kChunks * 16 * 16;  // layer 4: per tap K 32 x N 16
+    static constexpr int kW4Bytes = kChunks * 16 * 16;     // layer 4: K 32 x N 16 (the taps)
     static constexpr int kOffW1 = 0;
     static constexpr int kOffW2 = kOffW1 + kW1Bytes;
     static constexpr int kOffW3 = kOffW2 + 9 * kWtapBytes;
     static constexpr int kOffW4 = kOffW3 + 9 * kWtapBytes;
-    static constexpr int kOffAct = kOffW4 + 9 * kW4tapBytes;         // one buffer per slot
+    static constexpr int kOffAct = kOffW4 + kW4Bytes;                // one buffer per slot
     static constexpr int kOffScale = kOffAct + kSlots * kActBytes;   // 3 x 32 + 1 floats
     static constexpr int kOffBias = kOffScale + 128 * 4;             // 3 x 32 + 1 floats
     static constexpr int kOffTile = kOffBias + 128 * 4;
-    static constexpr int kSmemBytes = kOffTile + kSlots * kTileBytes;
+    static constexpr int kOffStage = kOffTile + kSlots * kTileBytes; // one per warpgroup
+    static constexpr int kSmemBytes = kOffStage + kEpiGroups * kStageBytes;
 };
 
 struct Src {
@@ -214,6 +219,31 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// The same load without its wait: several loads can be in flight before one
+// tmem_wait32.  The registers must not be read before that wait.
+__device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+// Waits for this thread's tensor-memory loads; r (one load's registers) is
+// an operand so that no read of it moves above the wait.
+__device__ __forceinline__ void tmem_wait32(uint32_t (&r)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31]) : : "memory");
+}
+// r as an operand of an empty statement placed after tmem_wait32: reads of
+// another load's registers stay below the wait too.
+__device__ __forceinline__ void after_wait32(uint32_t (&r)[32]) {
+    asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31]));
+}
+// 16 consecutive accumulator columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];" : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]) : : "memory");
+}
+
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<const uint32_t*>(&h);
@@ -254,6 +284,55 @@ __device__ __forceinline__ void store_pos(unsigned char* buf, int chunk_bytes, i
     }
 }
 
+// max(a, 0) and max(b, 0) rounded to an E4M3 pair (saturating) or a BF16
+// pair in one conversion each, a in the low half (cvt d, x, y puts x in the
+// high half).
+__device__ __forceinline__ uint32_t relu_e4m3x2(float a, float b) {
+    uint16_t r;
+    asm("cvt.rn.satfinite.relu.e4m3x2.f32 %0, %1, %2;" : "=h"(r) : "f"(b), "f"(a));
+    return r;
+}
+__device__ __forceinline__ uint32_t relu_bf16x2(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+}
+
+// store_pos of max(v, 0): the hidden layers' activations.
+template <bool F8>
+__device__ __forceinline__ void store_pos_relu(unsigned char* buf, int chunk_bytes, int pos,
+                                               const float (&v)[32]) {
+    if constexpr (F8) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            uint32_t w[4];
+            const float* c = v + 16 * k;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                w[j] = __byte_perm(relu_e4m3x2(c[4 * j], c[4 * j + 1]),
+                                   relu_e4m3x2(c[4 * j + 2], c[4 * j + 3]), 0x5410);
+            *reinterpret_cast<uint4*>(buf + k * chunk_bytes + pos * 16) =
+                make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float* c = v + 8 * k;
+            *reinterpret_cast<uint4*>(buf + k * chunk_bytes + pos * 16) =
+                make_uint4(relu_bf16x2(c[0], c[1]), relu_bf16x2(c[2], c[3]),
+                           relu_bf16x2(c[4], c[5]), relu_bf16x2(c[6], c[7]));
+        }
+    }
+}
+
+// Zeros at one position of a [chunk][pos][16 B] buffer (32 channels).
+template <bool F8>
+__device__ __forceinline__ void store_pos_zero(unsigned char* buf, int chunk_bytes, int pos) {
+#pragma unroll
+    for (int k = 0; k < Fmt<F8>::kChunks; ++k)
+        *reinterpret_cast<uint4*>(buf + k * chunk_bytes + pos * 16) = make_uint4(0u, 0u, 0u, 0u);
+}
+
 // Element (k, n) of a weight operand with N columns, [K chunk][n][16 B]:
 // rounded to BF16, or divided by the column's scale and rounded to E4M3.
 template <bool F8>
@@ -277,7 +356,8 @@ template <bool F8, int NOut>
 __device__ __forceinline__ void issue_taps(uint32_t td, uint64_t a0, uint64_t b0) {
     using F = Fmt<F8>;
     constexpr uint32_t id = idesc<F8>(128, NOut);
-    constexpr int tap_bytes = NOut == 32 ? F::kWtapBytes : F::kW4tapBytes;
+    static_assert(NOut == 32, "3x3 layers with 32 outputs");
+    constexpr int tap_bytes = F::kWtapBytes;
     constexpr int wchunk = NOut * 16;
 #pragma unroll
     for (int m = 0; m < 3; ++m)
@@ -313,7 +393,7 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 }
 
 template <bool F8>
-__global__ void __launch_bounds__(kCtaThreads, 1)
+__global__ void __launch_bounds__(kCtaThreads)
     infer_tc(const Src src, const float* __restrict__ params, float* __restrict__ u0,
              int32_t* __restrict__ status) {
     using F = Fmt<F8>;
@@ -366,11 +446,16 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
                            inv_wscale[32 * l + co]);
         }
     }
-    for (int i = t; i < 9 * 32 * 16; i += nthr) {
-        const int tap = i / 512, rem = i - tap * 512, ci = rem >> 4, co = rem & 15;
-        put_weight<F8>(sm + F::kOffW4 + tap * F::kW4tapBytes, 16, ci, co, weight(3, ci, tap, co),
+    // layer 4 (one output channel), B[ci][n] with the tap n = 0..8 as the
+    // column (9..15 zero): the MMA gives per-tap partial sums at each position,
+    // the epilogue sums them over the taps' shifts
+    for (int i = t; i < 32 * 16; i += nthr) {
+        const int ci = i >> 4, n = i & 15;
+        put_weight<F8>(sm + F::kOffW4, 16, ci, n, n < 9 ? weight(3, ci, n, 0) : 0.0f,
                        inv_wscale[96]);
     }
+    for (int i = t; i < kEpiGroups * kStageBytes / 16; i += nthr)  // rows never written stay 0
+        reinterpret_cast<uint4*>(sm + F::kOffStage)[i] = make_uint4(0u, 0u, 0u, 0u);
     // epilogue of layer l (0..2): act = max(acc * scale + bias, 0), stored as
     // the next layer's operand; layer 3: y = acc * scale + bias.  E4M3: the
     // accumulator carries the input and weight scales, the stored activation
@@ -422,9 +507,11 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
         if (status) atomicExch(status, 1);
     };
 
-    if (warp == kEpiGroups * 4) {
-        // ==== the MMA-issuing warp: lane 0 serves the slots whose operand is
-        // ready, in turn; each slot runs layers 0..3 of its tiles in order ====
+    if (warp >= kEpiGroups * 4) {
+        // ==== MMA-issuing warp ig (one per epilogue warpgroup, for its two
+        // slots): lane 0 serves whichever slot's operand is ready; each slot
+        // runs layers 0..3 of its tiles in order =============================
+        const int ig = warp - kEpiGroups * 4;
         if ((t & 31) == 0) {
             const uint32_t sW1a = smem_u32(sm + F::kOffW1), sW2a = smem_u32(sm + F::kOffW2);
             const uint32_t sW3a = smem_u32(sm + F::kOffW3), sW4a = smem_u32(sm + F::kOffW4);
@@ -445,19 +532,27 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
                     issue_taps<F8, 32>(td, sdesc(act_a, kChunkA, 128),
                                        sdesc(ly == 1 ? sW2a : sW3a, 512, 128));
                 } else {
-                    issue_taps<F8, 16>(td, sdesc(act_a, kChunkA, 128), sdesc(sW4a, 256, 128));
+                    // layer 4: D[q][tap] over the positions themselves (no shift)
+                    constexpr uint32_t id = idesc<F8>(128, 16);
+                    const uint64_t a0 = sdesc(act_a + (kPlane + 1) * 16, kChunkA, 128);
+                    const uint64_t b0 = sdesc(sW4a, 256, 128);
+#pragma unroll
+                    for (int m = 0; m < 3; ++m)
+#pragma unroll
+                        for (int ks = 0; ks < F::kKSteps; ++ks)
+                            mma<F8>(td + m * 16, a0 + (((2 * ks) * kChunkA + 128 * m * 16) >> 4),
+                                    b0 + (((2 * ks) * 256) >> 4), id, ks);
                 }
                 commit(smem_u32(&full_bar[sl]));
                 ++issued_s[sl];
             };
             // per-slot state (tile, layer, ready phase, slot) in registers,
-            // rotated so that the slot being polled is always the first
+            // swapped so that the slot being polled is always the first
             const long long n = src.n_tiles;
-            long long tA = first_tile(0), tB = first_tile(1), tC = first_tile(2),
-                      tD = first_tile(3);
-            int lA = 0, lB = 0, lC = 0, lD = 0, sA = 0, sB = 1, sC = 2, sD = 3;
-            uint32_t pA = 0, pB = 0, pC = 0, pD = 0;
-            int left = (tA < n) + (tB < n) + (tC < n) + (tD < n);
+            long long tA = first_tile(2 * ig), tB = first_tile(2 * ig + 1);
+            int lA = 0, lB = 0, sA = 2 * ig, sB = 2 * ig + 1;
+            uint32_t pA = 0, pB = 0;
+            int left = (tA < n) + (tB < n);
             int misses = 0;
             long long idle_rounds = 0;
             while (left > 0) {
@@ -472,7 +567,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
                     }
                     misses = 0;
                     idle_rounds = 0;
-                } else if (++misses == kSlots) {
+                } else if (++misses == 2) {
                     // a round over all slots found no work: back off so the
                     // epilogue warps sharing this scheduler get its issue slots
                     misses = 0;
@@ -487,9 +582,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
                 const int ll = lA, ss = sA;
                 const uint32_t pp = pA;
                 tA = tB; lA = lB; sA = sB; pA = pB;
-                tB = tC; lB = lC; sB = sC; pB = pC;
-                tC = tD; lC = lD; sC = sD; pC = pD;
-                tD = tt; lD = ll; sD = ss; pD = pp;
+                tB = tt; lB = ll; sB = ss; pB = pp;
             }
         }
     } else {
@@ -629,48 +722,75 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
                     }
                 }
                 unsigned char* dst = sm + F::kOffAct + sl * F::kActBytes;  // in place
-#pragma unroll 1
-                for (int m = 0; m < 3; ++m) {
+                // block 2 holds plane rows only in the group's first warp (rows
+                // 256..287); rows 288..383 are the zero rows below the plane.
+                // The first layer's epilogue clears them (the im2col operand
+                // had used them); later layers find them zero.
+                const bool three = (warp & 3) == 0;
+                // block m's accumulator row -> the next layer's operand
+                auto finish = [&](int m, const uint32_t (&r)[32]) {
                     const int q = 128 * m + tg, P = q + kPlane;
-                    float v[32];
-                    if (m == 2 && (warp & 3) != 0) {
-                        // rows 288..383: the zero rows below the plane.  The
-                        // first layer's epilogue clears them (the im2col
-                        // operand had used them); later layers find them zero.
-                        if (ly == 0) {
-#pragma unroll
-                            for (int i = 0; i < 32; ++i) v[i] = 0.0f;
-                            store_pos<F8>(dst, kChunkA, P + 1, v);
-                        }
-                        break;
-                    }
                     const int R = P / kPlane, Cc = P - R * kPlane;
-                    const bool valid = q < 288 && Cc >= 1 && Cc <= 16;
-                    tmem_ld32(td + m * 32, v);
+                    if (q < 288 && Cc >= 1 && Cc <= 16) {
+                        float v[32];
 #pragma unroll
-                    for (int i = 0; i < 32; ++i)
-                        v[i] = valid ? fmaxf(fmaf(v[i], sc[i], bias[i]), 0.0f) : 0.0f;
-                    store_pos<F8>(dst, kChunkA, P + 1, v);
+                        for (int i = 0; i < 32; ++i)
+                            v[i] = fmaf(__uint_as_float(r[i]), sc[i], bias[i]);
+                        store_pos_relu<F8>(dst, kChunkA, P + 1, v);
+                    } else {
+                        store_pos_zero<F8>(dst, kChunkA, P + 1);  // border columns: padding
+                    }
+                };
+                // two loads in flight: blocks 0 and 1, then block 2 into the
+                // registers block 0 has freed
+                uint32_t ra[32], rb[32];
+                tmem_ld32_issue(td, ra);
+                tmem_ld32_issue(td + 32, rb);
+                tmem_wait32(ra);
+                after_wait32(rb);
+                finish(0, ra);
+                if (three) tmem_ld32_issue(td + 64, ra);
+                else if (ly == 0) store_pos_zero<F8>(dst, kChunkA, 256 + tg + kPlane + 1);
+                finish(1, rb);
+                if (three) {
+                    tmem_wait32(ra);
+                    finish(2, ra);
                 }
             } else {
+                // D[P][tap] (= sum_ci a[P][ci] w[ci][tap]) -> stage[tap][P] for
+                // P = 18..323; rows 0..17 and 306..323 (the zero rows above and
+                // below the plane, where a = 0) are never written and stay 0,
+                // as do the border columns' partial sums (a = 0 there)
+                float* stage = reinterpret_cast<float*>(sm + F::kOffStage + g * kStageBytes);
+#pragma unroll 1
+                for (int m = 0; m < 3; ++m) {
+                    if (m == 2 && (warp & 3) != 0) break;  // rows 288..383: below the plane
+                    const int P = 128 * m + tg + kPlane;
+                    uint32_t r[16];
+                    tmem_ld16(td + m * 16, r);
+                    if (P < kStagePos)
+#pragma unroll
+                        for (int tap = 0; tap < 9; ++tap)
+                            stage[tap * kStagePos + P] = __uint_as_float(r[tap]);
+                }
+                wg_sync(bar_id);
+                // y(P) = sum over the taps of D[P + (ky-1) 18 + (kx-1)][tap]
                 const float* sD =
                     reinterpret_cast<const float*>(sm + F::kOffTile + sl * kTileBytes);
                 const float* sG = sD + 256;
                 const float sdv = scale[k];
-#pragma unroll 1
-                for (int m = 0; m < 3; ++m) {
-                    if (m == 2 && (warp & 3) != 0) break;  // rows 288..383: no pixels
-                    const int q = 128 * m + tg, P = q + kPlane;
-                    const int R = P / kPlane, Cc = P - R * kPlane;
-                    float v[32];
-                    tmem_ld32(td + m * 16, v);  // columns 0..15 used (+16 unused)
-                    if (q < 288 && Cc >= 1 && Cc <= 16) {
-                        const int px = (R - 1) * 16 + (Cc - 1);
-                        const float y = fmaf(v[0], sScale[96], sBias[96]);
-                        const float d = sD[px], gm = sG[px];
-                        const float lo = kStartFrac * fmaxf(d + gm, 1e-3f) - gm;
-                        u0[tile[k] * 256 + px] = fmaxf(fmaf(sdv, y, d), lo);
-                    }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int px = tg + 128 * h;
+                    const int P = ((px >> 4) + 1) * kPlane + (px & 15) + 1;
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int tap = 0; tap < 9; ++tap)
+                        acc += stage[tap * kStagePos + P + (tap / 3 - 1) * kPlane + (tap % 3 - 1)];
+                    const float y = fmaf(acc, sScale[96], sBias[96]);
+                    const float d = sD[px], gm = sG[px];
+                    const float lo = kStartFrac * fmaxf(d + gm, 1e-3f) - gm;
+                    u0[tile[k] * 256 + px] = fmaxf(fmaf(sdv, y, d), lo);
                 }
             }
         };
@@ -797,7 +917,7 @@ constexpr bool plan_ok() {
 }
 static_assert(plan_ok<false>() && plan_ok<true>(), "one CTA per SM, aligned operands");
 static_assert(kTmemCols <= 512 && kSlots * 128 <= (int)kTmemCols, "slots' tensor memory");
-static_assert(kSlots == 4, "the MMA warp rotates four slots' state");
+static_assert(kSlots == 2 * kEpiGroups, "each MMA warp serves two slots");
 static_assert(kIm2colPos + kQ <= kPos - 21, "im2col rows stay inside the rewritten range");
 
 }  // namespace nettc

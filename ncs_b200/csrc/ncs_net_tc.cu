@@ -80,7 +80,11 @@ constexpr long long kIdlePolls = 1ll << 21;  // MMA warp: rounds over the slots 
 // positions 19..402 -- the range every epilogue rewrites -- so the zero
 // border positions of the buffer are never touched
 constexpr int kIm2colPos = 19;
-constexpr int kTileBytes = 4 * 256 * 4;  // per slot d, gamma, x0, x1
+// per slot: d and gamma [256] floats, then the features (x0, x1) as float2
+// on the zero-bordered 18 x 18 plane at index P + 1 (P = row * 18 + column),
+// 328 entries: every tap of every im2col row stays inside
+constexpr int kFeatPlane = 328;
+constexpr int kTileBytes = 2 * 256 * 4 + kFeatPlane * 8;
 // last layer: per-tap partial sums D[P][tap] of the plane positions 0..323,
 // staged per warpgroup as [tap][P] floats for the shifted sum over the taps
 constexpr int kStagePos = 324;
@@ -456,6 +460,8 @@ __global__ void __launch_bounds__(kCtaThreads)
     }
     for (int i = t; i < kEpiGroups * kStageBytes / 16; i += nthr)  // rows never written stay 0
         reinterpret_cast<uint4*>(sm + F::kOffStage)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = t; i < kSlots * kTileBytes / 16; i += nthr)  // the feature planes' border
+        reinterpret_cast<uint4*>(sm + F::kOffTile)[i] = make_uint4(0u, 0u, 0u, 0u);
     // epilogue of layer l (0..2): act = max(acc * scale + bias, 0), stored as
     // the next layer's operand; layer 3: y = acc * scale + bias.  E4M3: the
     // accumulator carries the input and weight scales, the stored activation
@@ -644,8 +650,7 @@ __global__ void __launch_bounds__(kCtaThreads)
             const int sl = 2 * g + k;
             float* sD = reinterpret_cast<float*>(sm + F::kOffTile + sl * kTileBytes);
             float* sG = sD + 256;
-            float* sX0 = sG + 256;
-            float* sX1 = sX0 + 256;
+            float2* sXP = reinterpret_cast<float2*>(sG + 256);
             float s1 = dv[k][0] + dv[k][1], s2 = dv[k][0] * dv[k][0] + dv[k][1] * dv[k][1];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -663,32 +668,32 @@ __global__ void __launch_bounds__(kCtaThreads)
                                              (1.0f / 256.0f) - mu * mu,
                                          0.0f)) + 1.0f;
             scale[k] = sd;
+            // E4M3: the features carry the layer's input scale (a power of two)
+            const float fs = (F8 ? f8_in_scale(0) : 1.0f) / sd;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int p = tg + 128 * h;
                 sD[p] = dv[k][h];
                 sG[p] = gv[k][h];
-                sX0[p] = (dv[k][h] - mu) / sd;
-                sX1[p] = sqrtf(fmaxf(dv[k][h], 0.0f) + fmaxf(gv[k][h], 0.0f)) / sd;
+                sXP[((p >> 4) + 1) * kPlane + (p & 15) + 2] =
+                    make_float2((dv[k][h] - mu) * fs,
+                                sqrtf(fmaxf(dv[k][h], 0.0f) + fmaxf(gv[k][h], 0.0f)) * fs);
             }
             wg_sync(bar_id);
             unsigned char* im2col = sm + F::kOffAct + sl * F::kActBytes + kIm2colPos * 16;
-            const float in_scale = F8 ? f8_in_scale(0) : 1.0f;
 #pragma unroll 1
             for (int m = 0; m < 3; ++m) {
                 // rows 288..383 (block 2 beyond its first warp) are outside the
                 // plane: their layer-1 outputs are discarded, the operand unused
                 if (m == 2 && (warp & 3) != 0) break;
-                const int q = 128 * m + tg, P = q + kPlane;
-                const int R = P / kPlane, Cc = P - R * kPlane;
+                const int q = 128 * m + tg;
                 float v[32];
 #pragma unroll
                 for (int tap = 0; tap < 9; ++tap) {
-                    const int rr = R + tap / 3 - 1, cc = Cc + tap % 3 - 1;
-                    const bool in = rr >= 1 && rr <= 16 && cc >= 1 && cc <= 16;
-                    const int px = in ? (rr - 1) * 16 + (cc - 1) : 0;
-                    v[2 * tap] = in ? sX0[px] * in_scale : 0.0f;
-                    v[2 * tap + 1] = in ? sX1[px] * in_scale : 0.0f;
+                    // plane index of position q + 18 plus the tap's shift, + 1
+                    const float2 x = sXP[q + kPlane + 1 + (tap / 3 - 1) * kPlane + (tap % 3 - 1)];
+                    v[2 * tap] = x.x;
+                    v[2 * tap + 1] = x.y;
                 }
 #pragma unroll
                 for (int kk = 18; kk < 32; ++kk) v[kk] = 0.0f;
@@ -919,6 +924,8 @@ static_assert(plan_ok<false>() && plan_ok<true>(), "one CTA per SM, aligned oper
 static_assert(kTmemCols <= 512 && kSlots * 128 <= (int)kTmemCols, "slots' tensor memory");
 static_assert(kSlots == 2 * kEpiGroups, "each MMA warp serves two slots");
 static_assert(kIm2colPos + kQ <= kPos - 21, "im2col rows stay inside the rewritten range");
+static_assert(287 + kPlane + 1 + kPlane + 1 < kFeatPlane, "im2col taps stay inside the plane");
+static_assert(kTileBytes % 16 == 0, "tile data alignment");
 
 }  // namespace nettc
 }  // namespace ncsb

@@ -48,37 +48,6 @@ __host__ __device__ constexpr size_t spec_warp_bytes(int m) {
     return ((sizeof(WarpSmem) + 15) / 16) * 16 + (3 * (size_t)m + 2) * 32 * 2 * sizeof(float4);
 }
 
-// A history vector (s, y or Q s) is stored as [half][lane] float4s, so that
-// each 128-bit access of the warp covers 512 consecutive bytes without bank
-// conflicts (lane-major pairs of float4s would put two lanes on each bank).
-__device__ __forceinline__ void load_hist(const float4* h, int lane, float (&x)[8]) {
-    const float4 a = h[lane], b = h[32 + lane];
-    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
-}
-__device__ __forceinline__ void store_hist(float4* h, int lane, const float (&x)[8]) {
-    h[lane] = make_float4(x[0], x[1], x[2], x[3]);
-    h[32 + lane] = make_float4(x[4], x[5], x[6], x[7]);
-}
-
-// The pixel terms c and gamma of a lane's 8 pixels live in the warp's shared
-// memory as [c low, c high, gamma low, gamma high][lane] float4s (each
-// access is 32 consecutive 16-byte words) and are re-read at every use.
-// Keeping them out of the loop-carried registers measured 2.6 % faster at
-// the same occupancy: the solver is issue-bound and the freed registers let
-// the compiler schedule the transforms and the line search more tightly.
-// The loads are volatile so that they are not hoisted back out of the loop
-// (the row-stage twiddles are re-read from a table the same way).
-__device__ __forceinline__ void load_terms(const float4* t, int lane, float (&c)[8],
-                                           float (&gm)[8]) {
-    const float4 c0 = lds_v4_volatile(t + lane), c1 = lds_v4_volatile(t + 32 + lane);
-    const float4 g0 = lds_v4_volatile(t + 64 + lane), g1 = lds_v4_volatile(t + 96 + lane);
-    c[0] = c0.x; c[1] = c0.y; c[2] = c0.z; c[3] = c0.w;
-    c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
-    gm[0] = g0.x; gm[1] = g0.y; gm[2] = g0.z; gm[3] = g0.w;
-    gm[4] = g1.x; gm[5] = g1.y; gm[6] = g1.z; gm[7] = g1.w;
-}
-
 // Per-stack pointers and geometry: the kernel parameters of a single-stack
 // launch, or the warp's current stack descriptor of a batched one.
 struct Geo {
@@ -231,10 +200,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             }
         };
         __syncwarp();  // the previous tile's terms are no longer read
-        terms[lane] = make_float4(d[0] + gam[0], d[1] + gam[1], d[2] + gam[2], d[3] + gam[3]);
-        terms[32 + lane] = make_float4(d[4] + gam[4], d[5] + gam[5], d[6] + gam[6], d[7] + gam[7]);
-        terms[64 + lane] = make_float4(gam[0], gam[1], gam[2], gam[3]);
-        terms[96 + lane] = make_float4(gam[4], gam[5], gam[6], gam[7]);
+        store_terms(terms, lane, d, gam);
         __syncwarp();
 
         // ---- preconditioned L-BFGS ---------------------------------------------

@@ -70,6 +70,7 @@ constexpr int kTcThreads = 32 * kTcWarps;
 constexpr int kMinBlocks = 16 / kTiles;  // 128 registers a thread fill the register file
 constexpr uint32_t kTmemCols = 128;        // D of stages 1..4 at columns 0, 32, 64, 96
 constexpr long long kWaitTries = 1ll << 17;  // mbarrier polls of <= 20 us before giving up
+constexpr long long kSpinTries = 1ll << 26;  // mbarrier polls without suspending (seconds)
 
 // Operand A (kM rows): groups of 8 rows, 128 B apart; K chunks (16 bytes of
 // K per row) kALbo apart.  The extra 16 bytes move consecutive chunks to the
@@ -93,8 +94,9 @@ struct Plan {
     static constexpr int A2 = (32 / KPC) * kALbo;       // stages 2-4 operand (K 32), one part
     static constexpr int OFF_A1 = OFF_B + NP * BPART;
     static constexpr int OFF_A2 = OFF_A1 + NP * A1;
-    static constexpr int OFF_HIST = OFF_A2 + NP * A2;   // per warp: s, y, Q s (1 KB each)
-    static constexpr int BYTES = OFF_HIST + kTcWarps * 3 * 1024;
+    // per warp: s, y, Q s (1 KB each), then the pixel terms c, gamma (2 KB)
+    static constexpr int OFF_HIST = OFF_A2 + NP * A2;
+    static constexpr int BYTES = OFF_HIST + kTcWarps * 5 * 1024;
 };
 
 // Byte offset of element (row, k) of a K-major operand whose 8-row groups
@@ -292,9 +294,10 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
     unsigned char* sB = dsm + PL::OFF_B;
     unsigned char* sA1 = dsm + PL::OFF_A1;
     unsigned char* sA2 = dsm + PL::OFF_A2;
-    float4* hs = reinterpret_cast<float4*>(dsm + PL::OFF_HIST + wid * 3 * 1024);
+    float4* hs = reinterpret_cast<float4*>(dsm + PL::OFF_HIST + wid * 5 * 1024);
     float4* hy = hs + 64;
     float4* hq = hy + 64;
+    float4* terms = hq + 64;  // c and gamma, see load_terms
 
     // ---- set-up: constant matrices, zeroed operands, mbarrier, tensor memory
     build_b<BF>(sB, 1, 16, 16);
@@ -362,7 +365,9 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
             issue_stage<BF>(stage, tmem, sbu, sa1u, sa2u);
             tc::commit(bar);
         }
-        const bool ok = tc::wait_bounded(bar, phase, kWaitTries);
+        // a polling wait: threads that sleep in the wait measured slower
+        bool ok = false;
+        for (long long i = 0; i < kSpinTries && !ok; ++i) ok = tc::try_wait(bar, phase);
         phase ^= 1u;
         if (!ok) {
             s_abort = 1;
@@ -375,7 +380,7 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
     // ---- per-warp solver state (the spectral form's, m = 1) -----------------
     bool has_tile = false;
     long long tile = 0;
-    float d[8], gm[8], u[8], c[8], v[8], g[8], p[8], w[8];
+    float u[8], v[8], g[8], p[8], w[8];  // c and gamma: in shared memory (terms)
     float rho = 0.0f, al = 0.0f, sg_newest = 0.0f, lam = 1.0f;
     bool sg_fresh = false, first = true;
     int status = kUnstarted, iters = 0, evals = 1, k = 0, start_pass = 0, fell_back = 0;
@@ -412,6 +417,7 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
             tile = (long long)__shfl_sync(kFull, tk, 0);
             if (tile < a.n_tiles) {
                 has_tile = true;
+                float d[8], gm[8];
                 long long lt = tile;  // index of the tile within its stack
                 if constexpr (Batch) {
                     int lo = 0, hi = a.n_stacks - 1;
@@ -472,8 +478,9 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                                 u[2 * j + s] = __ldg(ut + (P + 8 * s) * kTile + Qd + 4 * j);
                     }
                 }
-#pragma unroll
-                for (int i = 0; i < 8; ++i) c[i] = d[i] + gm[i];
+                __syncwarp();  // the previous tile's terms are no longer read
+                store_terms(terms, lane, d, gm);
+                __syncwarp();
                 rho = al = sg_newest = 0.0f;
                 lam = 1.0f;
                 sg_fresh = false;
@@ -508,14 +515,14 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                     if (sg_fresh) {
                         dot = -sg_newest;  // q = -g here
                     } else {
-                        load8(hs + lane * 2, hv);
+                        load_hist(hs, lane, hv);
                         float acc = 0.0f;
 #pragma unroll
                         for (int e = 0; e < 8; ++e) acc = fmaf(hv[e], q[e], acc);
                         dot = warp_sum_f(acc);
                     }
                     al = rho * dot;
-                    load8(hy + lane * 2, hv);
+                    load_hist(hy, lane, hv);
 #pragma unroll
                     for (int e = 0; e < 8; ++e) q[e] = fmaf(-al, hv[e], q[e]);
                 }
@@ -603,8 +610,9 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                 // the spectral form's bound: f(u0) - f(d) <= LL(u0) - LL(d) +
                 // (u0 - d)'v0, v0 = 2 alpha Q u0 = p; accept u0 when <= 0,
                 // else transform d next for the exact comparison
-                float dd[8];
+                float dd[8], c[8], gm[8];
                 load_d(dd);
+                load_terms(terms, lane, c, gm);
                 float dl = 0.0f, dq = 0.0f;
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
@@ -623,8 +631,9 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                     init = false;
                 }
             } else if (start_pass == 1) {
-                float dd[8];
+                float dd[8], c[8], gm[8];
                 load_d(dd);
+                load_terms(terms, lane, c, gm);
                 float dl = 0.0f, dq = 0.0f;
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
@@ -646,6 +655,8 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
             }
             if (init) {
                 first = false;
+                float c[8], gm[8];
+                load_terms(terms, lane, c, gm);
                 float uu = 0.0f, gg = 0.0f, ll = 0.0f;
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
@@ -669,15 +680,15 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
             // two-loop, second half: p += coef s, w += coef Q s
             if (k > 0) {
                 float hv[8];
-                load8(hy + lane * 2, hv);
+                load_hist(hy, lane, hv);
                 float acc = 0.0f;
 #pragma unroll
                 for (int e2 = 0; e2 < 8; ++e2) acc = fmaf(hv[e2], p[e2], acc);
                 const float coef = al - rho * warp_sum_f(acc);
-                load8(hs + lane * 2, hv);
+                load_hist(hs, lane, hv);
 #pragma unroll
                 for (int e2 = 0; e2 < 8; ++e2) p[e2] = fmaf(coef, hv[e2], p[e2]);
-                load8(hq + lane * 2, hv);
+                load_hist(hq, lane, hv);
 #pragma unroll
                 for (int e2 = 0; e2 < 8; ++e2) w[e2] = fmaf(coef, hv[e2], w[e2]);
             }
@@ -703,6 +714,8 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                 float t = 1.0f;
                 bool ok = false;
                 for (int trial = 0; trial < 64; ++trial) {
+                    float c[8], gm[8];
+                    load_terms(terms, lane, c, gm);
                     float term = 0.0f;
                     bool cross = false;
 #pragma unroll
@@ -737,7 +750,8 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                     done = true;
                 } else {
                     // accept; new pair (s, y, Q s = t w)
-                    float s[8], y[8];
+                    float s[8], y[8], c[8], gm[8];
+                    load_terms(terms, lane, c, gm);
                     float sy = 0.0f, uu = 0.0f, gg = 0.0f, ll = 0.0f, mv = 0.0f, sgv = 0.0f;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
@@ -780,9 +794,9 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                         sg_fresh = sy > 0.0f;
                         if (sy > 0.0f) {
                             sg_newest = sgv;
-                            store8(hs + lane * 2, s);
-                            store8(hy + lane * 2, y);
-                            store8(hq + lane * 2, w);
+                            store_hist(hs, lane, s);
+                            store_hist(hy, lane, y);
+                            store_hist(hq, lane, w);
                             rho = rcp_fast(sy);
                             k = 1;
                         }
@@ -799,6 +813,8 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
 
         // ---- outputs -------------------------------------------------------------
         if (a.cost) {
+            float c[8], gm[8];
+            load_terms(terms, lane, c, gm);
             double e0 = 0.0, e1 = 0.0;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {

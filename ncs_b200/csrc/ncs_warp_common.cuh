@@ -155,6 +155,45 @@ __device__ __forceinline__ float4 lds_v4_volatile(const void* p) {
     return v;
 }
 
+// A history vector (s, y or Q s) of the warp solvers is stored as
+// [half][lane] float4s, so that each 128-bit access of the warp covers 512
+// consecutive bytes without bank conflicts (lane-major pairs of float4s
+// would put two lanes on each bank).
+__device__ __forceinline__ void load_hist(const float4* h, int lane, float (&x)[8]) {
+    const float4 a = h[lane], b = h[32 + lane];
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+__device__ __forceinline__ void store_hist(float4* h, int lane, const float (&x)[8]) {
+    h[lane] = make_float4(x[0], x[1], x[2], x[3]);
+    h[32 + lane] = make_float4(x[4], x[5], x[6], x[7]);
+}
+
+// The pixel terms c = d + gamma and gamma of a lane's 8 pixels, kept in the
+// warp's shared memory as [c low, c high, gamma low, gamma high][lane]
+// float4s (each access is 32 consecutive 16-byte words) and re-read at
+// every use.  Keeping them out of the loop-carried registers measured 2.6 %
+// faster at the same occupancy: the solvers are issue-bound and the freed
+// registers let the compiler schedule the transforms and the line search
+// more tightly.  The loads are volatile so that they are not hoisted back
+// out of the loop.
+__device__ __forceinline__ void store_terms(float4* t, int lane, const float (&d)[8],
+                                            const float (&gm)[8]) {
+    t[lane] = make_float4(d[0] + gm[0], d[1] + gm[1], d[2] + gm[2], d[3] + gm[3]);
+    t[32 + lane] = make_float4(d[4] + gm[4], d[5] + gm[5], d[6] + gm[6], d[7] + gm[7]);
+    t[64 + lane] = make_float4(gm[0], gm[1], gm[2], gm[3]);
+    t[96 + lane] = make_float4(gm[4], gm[5], gm[6], gm[7]);
+}
+__device__ __forceinline__ void load_terms(const float4* t, int lane, float (&c)[8],
+                                           float (&gm)[8]) {
+    const float4 c0 = lds_v4_volatile(t + lane), c1 = lds_v4_volatile(t + 32 + lane);
+    const float4 g0 = lds_v4_volatile(t + 64 + lane), g1 = lds_v4_volatile(t + 96 + lane);
+    c[0] = c0.x; c[1] = c0.y; c[2] = c0.z; c[3] = c0.w;
+    c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
+    gm[0] = g0.x; gm[1] = g0.y; gm[2] = g0.z; gm[3] = g0.w;
+    gm[4] = g1.x; gm[5] = g1.y; gm[6] = g1.z; gm[7] = g1.w;
+}
+
 // The row-stage twiddles of the four lane classes Qd, for kernels that re-read
 // them before each transform rather than keep six registers through the
 // solve: v[Qd][0] = (tw1, tw2), v[Qd][1] = (tw3, unused).

@@ -1,19 +1,37 @@
 // ncs_net_tc.cu -- warm-start network inference on the 5th-generation tensor
 // cores (tcgen05, sm_100a): the same network as ncs_net.cu's FP32 inference,
 // as implicit GEMMs with BF16 or E4M3 (FP8) operands and FP32 accumulators in
-// tensor memory.
+// tensor memory.  Two kernels share the roles and the helpers below:
 //
-// Per 16x16 tile, positions live on the zero-bordered 18 x 18 plane
-// (row-major, index P).  The outputs of a 3x3 layer at the 288 positions
-// P = 18..305 (plane rows 1..16, all 18 columns; the two border columns are
-// computed and discarded) are, for each tap (ky, kx), a GEMM
+// infer_tc<false> (BF16 operands, kind::f16, K = 16 per MMA).  Per 16x16
+// tile, positions live on the zero-bordered 18 x 18 plane (row-major, index
+// P).  The outputs of a 3x3 layer at the 288 positions P = 18..305 (plane
+// rows 1..16, all 18 columns; the two border columns are computed and
+// discarded) are, for each tap (ky, kx), a GEMM
 //     D[q][co] += sum_ci A[q + 18 + (ky-1)*18 + (kx-1)][ci] * W[tap][ci][co]
 // so the tap is a shift of the A operand's start position: one shared-memory
 // matrix descriptor per tap over the same activation buffer.  M = 128
-// (3 blocks cover the 288 positions), N = 32 (N = 16 for the 1-channel last
-// layer, weights zero-padded), K = 16 per instruction, 2 per 32 channels.
-// The first layer (2 input channels) is one GEMM with an im2col operand,
-// K = 18 taps x channels padded to 32.
+// (3 blocks cover the 288 positions), N = 32.  Four slots of 128 tensor-
+// memory columns, two per epilogue warpgroup.
+//
+// infer_tc_w16 (E4M3 operands, kind::f8f6f4, K = 32 per MMA: half the
+// operand bytes of BF16).  Each activation is stored as three column-shifted
+// copies on 16-wide rows, so that 2 M blocks cover exactly the 256 pixels
+// (40 MMAs per tile instead of 60) and a slot needs 64 tensor-memory
+// columns: six slots, three per warpgroup (the description at the kernel).
+// Each output channel's weights are scaled by max|w| / 448 before rounding,
+// and each layer's input by a fixed power of two (features x 8, hidden
+// activations x 4: 56 and 112 at E4M3's largest value, against 14 and 41
+// seen on full-sensor tiles with hot pixels; larger values saturate).  The
+// epilogue folds both scales and the next layer's input scale into one
+// multiply-add per value.  Proposals differ from the FP32 network's by about
+// 0.1-0.2 of the tile's scale s at most, and the solves from them take the
+// same iterations.
+//
+// In both, the first layer (2 input channels) is one GEMM per block with an
+// im2col operand, K = 18 taps x channels padded to 32, and the last layer
+// (one output channel) is one GEMM per block with the 9 taps as the N = 16
+// columns: per-tap partial sums, added over the taps' shifts in the epilogue.
 //
 // Shared-memory operands are K-major without swizzle: 8 consecutive
 // positions x 16 bytes (8 BF16 or 16 E4M3 channels) form a core matrix, so an
@@ -21,38 +39,26 @@
 // offset (between the K chunks of one MMA) = the chunk stride and the stride
 // byte offset (between 8-row groups) = 128 B.  The epilogue reads each
 // accumulator row from tensor memory (thread t of the 128 owns row t of every
-// M block), scales it, adds the bias, applies ReLU, rounds to the operand
-// format and writes the next layer's operand -- zeros at the plane's border
-// positions, which are the next layer's zero padding.
-//
-// E4M3 form (kind::f8f6f4, K = 32 per MMA: half the MMAs and half the
-// operand bytes of BF16, whose shared-memory reads bound that form): each
-// output channel's weights are scaled by max|w| / 448 before rounding, and each
-// layer's input by a fixed power of two (features x 8, hidden activations
-// x 4: 56 and 112 at E4M3's largest value, against 14 and 41 seen on full-
-// sensor tiles with hot pixels; larger values saturate).  The epilogue folds
-// both scales and the next layer's input scale into one multiply-add per
-// value.  Proposals differ from the FP32 network's by about 1e-2 of the
-// tile's scale s, and the solves from them take the same iterations.
-//
-// A layer's MMAs have finished reading their input before its epilogue
-// runs, so the epilogue overwrites that input in place: one activation
-// buffer per tile.
+// M block), scales it, adds the bias, applies ReLU and rounds to the operand
+// format in one conversion, and writes the next layer's operand -- zeros at
+// the padding positions.  A layer's MMAs have finished reading their input
+// before its epilogue runs, so the epilogue overwrites that input in place.
 //
 // Warp-specialised and persistent, one CTA per SM (it holds all 512 tensor-
-// memory columns): four tile slots, each with its activation buffer, 128
-// tensor-memory columns and two mbarriers (full: the slot's MMAs of a layer
-// completed; ready: its next operand is written).  One warp issues MMAs: it
-// polls the slots' ready barriers in turn and issues the layer of whichever
-// slot is ready, committing to that slot's full barrier.  Two epilogue
-// warpgroups own two slots each and alternate between them: wait for the
-// slot's full barrier, read its accumulators, write the next operand (or the
-// proposal, after the last layer, and then the next tile's features), arrive
-// on its ready barrier.  No role waits for another at a CTA-wide barrier, so
-// the tensor core works on one slot while the epilogues of the others run.
-// Every wait is bounded; a timed-out wait sets the caller's status flag and
-// a shared abort flag that ends the other roles' loops, the outstanding MMAs
-// are drained with bounded waits and the tensor memory is freed.
+// memory columns): tile slots, each with its activation buffer, its tensor-
+// memory columns and two mbarriers (full: the slot's MMAs of a layer
+// completed; ready: its next operand is written).  Two epilogue warpgroups
+// own half of the slots each and rotate over them: wait for the slot's full
+// barrier, read its accumulators, write the next operand (or the proposal,
+// after the last layer, and then the next tile's features), arrive on its
+// ready barrier.  Each warpgroup has an MMA-issuing warp that polls its
+// slots' ready barriers in turn and issues the layer of whichever slot is
+// ready, committing to that slot's full barrier.  No role waits for another
+// at a CTA-wide barrier, so the tensor core works on one slot while the
+// epilogues of the others run.  Every wait is bounded; a timed-out wait sets
+// the caller's status flag and a shared abort flag that ends the other
+// roles' loops, the outstanding MMAs are drained with bounded waits and the
+// tensor memory is freed.
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 #include <cuda_runtime.h>
@@ -396,23 +402,23 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+// The network's operands and epilogue tables in shared memory, for either
+// operand format: W1 (B[k][co], k = tap * 2 + ci, 18 of 32 used), W2 and W3
+// (per tap B[ci][co], `tap_bytes` apart), W4 (B[ci][n] with the tap n = 0..8
+// as the column, 9..15 zero: the MMA gives per-tap partial sums at each
+// position, the epilogue sums them over the taps' shifts), and per output
+// column the epilogue's scale and bias: layer l (0..2) stores
+// max(acc * scale + bias, 0) as the next layer's operand, layer 3 gives
+// y = acc * scale + bias.  E4M3: the accumulator carries the input and
+// weight scales, the stored activation the next layer's input scale (a
+// positive factor, so it commutes with the ReLU).  All threads of the CTA
+// take part; inv_wscale (128 floats, shared) is scratch.  Ends with
+// __syncthreads.
 template <bool F8>
-__global__ void __launch_bounds__(kCtaThreads)
-    infer_tc(const Src src, const float* __restrict__ params, float* __restrict__ u0,
-             int32_t* __restrict__ status) {
-    using F = Fmt<F8>;
-    extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ __align__(8) uint64_t full_bar[kSlots];   // a slot's layer MMAs completed
-    __shared__ __align__(8) uint64_t ready_bar[kSlots];  // a slot's next operand written
-    __shared__ uint32_t tmem_base_s;
-    __shared__ float red[kEpiGroups][8];
-    __shared__ float inv_wscale[4 * kC];  // E4M3: 1 / (column max |w| / 448), per layer
-    __shared__ int issued_s[kSlots], consumed_s[kSlots];
-    __shared__ volatile int abort_s;
-    const int t = threadIdx.x, warp = t >> 5, nthr = blockDim.x;
-
-    // ---- weights -> operand layouts, epilogue scales and biases, zeroed
-    //      activations ----------------------------------------------------------
+__device__ void load_network(const float* __restrict__ params, unsigned char* sW1,
+                             unsigned char* sW2, unsigned char* sW3, int tap_bytes,
+                             unsigned char* sW4, float* sScale, float* sBias, float* inv_wscale,
+                             int t, int nthr) {
     const float* w1 = params;
     const float* b1 = w1 + 2 * 9 * kC;
     const float* w2 = b1 + kC;
@@ -436,39 +442,23 @@ __global__ void __launch_bounds__(kCtaThreads)
         inv_wscale[t] = mx > 0.0f ? kF8Max / mx : 1.0f;
     }
     __syncthreads();
-    // layer 1, B[k][co] with k = tap * 2 + ci (18 used of 32)
     for (int i = t; i < 32 * 32; i += nthr) {
         const int k = i >> 5, co = i & 31;
-        put_weight<F8>(sm + F::kOffW1, 32, k, co, k < 18 ? weight(0, k & 1, k >> 1, co) : 0.0f,
+        put_weight<F8>(sW1, 32, k, co, k < 18 ? weight(0, k & 1, k >> 1, co) : 0.0f,
                        inv_wscale[co]);
     }
     for (int l = 1; l < 3; ++l) {
-        unsigned char* sW = sm + (l == 1 ? F::kOffW2 : F::kOffW3);
+        unsigned char* sW = l == 1 ? sW2 : sW3;
         for (int i = t; i < 9 * 32 * 32; i += nthr) {
             const int tap = i / 1024, rem = i - tap * 1024, ci = rem >> 5, co = rem & 31;
-            put_weight<F8>(sW + tap * F::kWtapBytes, 32, ci, co, weight(l, ci, tap, co),
+            put_weight<F8>(sW + tap * tap_bytes, 32, ci, co, weight(l, ci, tap, co),
                            inv_wscale[32 * l + co]);
         }
     }
-    // layer 4 (one output channel), B[ci][n] with the tap n = 0..8 as the
-    // column (9..15 zero): the MMA gives per-tap partial sums at each position,
-    // the epilogue sums them over the taps' shifts
     for (int i = t; i < 32 * 16; i += nthr) {
         const int ci = i >> 4, n = i & 15;
-        put_weight<F8>(sm + F::kOffW4, 16, ci, n, n < 9 ? weight(3, ci, n, 0) : 0.0f,
-                       inv_wscale[96]);
+        put_weight<F8>(sW4, 16, ci, n, n < 9 ? weight(3, ci, n, 0) : 0.0f, inv_wscale[96]);
     }
-    for (int i = t; i < kEpiGroups * kStageBytes / 16; i += nthr)  // rows never written stay 0
-        reinterpret_cast<uint4*>(sm + F::kOffStage)[i] = make_uint4(0u, 0u, 0u, 0u);
-    for (int i = t; i < kSlots * kTileBytes / 16; i += nthr)  // the feature planes' border
-        reinterpret_cast<uint4*>(sm + F::kOffTile)[i] = make_uint4(0u, 0u, 0u, 0u);
-    // epilogue of layer l (0..2): act = max(acc * scale + bias, 0), stored as
-    // the next layer's operand; layer 3: y = acc * scale + bias.  E4M3: the
-    // accumulator carries the input and weight scales, the stored activation
-    // the next layer's input scale (a positive factor, so it commutes with
-    // the ReLU).
-    float* sScale = reinterpret_cast<float*>(sm + F::kOffScale);
-    float* sBias = reinterpret_cast<float*>(sm + F::kOffBias);
     for (int i = t; i < 97; i += nthr) {
         const int l = i >> 5;
         const float b = i < 32 ? b1[i] : (i < 64 ? b2[i - 32] : (i < 96 ? b3[i - 64] : b4[0]));
@@ -481,6 +471,79 @@ __global__ void __launch_bounds__(kCtaThreads)
             sBias[i] = b;
         }
     }
+    __syncthreads();
+}
+
+// Pixels p = tg and tg + 128 of a tile (the solvers' segmentation: edge-
+// replicated halo; batched stacks found by binary search over their first
+// tiles).
+__device__ __forceinline__ void gather_pixels(const Src& src, long long tl, int tg,
+                                              float (&dvo)[2], float (&gvo)[2]) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int p = tg + 128 * h, r = p >> 4, c = p & 15;
+        if (src.tile_mode) {
+            dvo[h] = src.d[tl * 256 + p];
+            gvo[h] = src.gamma[tl * 256 + p];
+        } else {
+            const float* sd = src.d;
+            const float* sgam = src.gamma;
+            long long gstride = src.gamma_frame_stride, lt = tl,
+                      pf = (long long)src.tiles_x * src.tiles_y;
+            int H = src.H, W = src.W, ty = src.tiles_y;
+            if (src.stacks) {  // batched: the last stack whose first tile is <= tl
+                int lo = 0, hi = src.n_stacks - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (src.stacks[mid].tile_begin <= tl) lo = mid;
+                    else hi = mid - 1;
+                }
+                const StackDesc& st = src.stacks[lo];
+                sd = st.data;
+                sgam = st.gamma;
+                gstride = st.gamma_frame_stride;
+                lt = tl - st.tile_begin;
+                H = st.H;
+                W = st.W;
+                ty = st.tiles_y;
+                pf = (long long)st.tiles_x * st.tiles_y;
+            }
+            const int f = (int)(lt / pf);
+            const int rem = (int)(lt - (long long)f * pf);
+            const int ti = rem / ty, tj = rem - ti * ty;
+            const int yy = clampi(tile_origin(ti, H) + r - 1, 0, H - 1);
+            const int xx = clampi(tile_origin(tj, W) + c - 1, 0, W - 1);
+            dvo[h] = sd[(long long)f * H * W + (long long)yy * W + xx];
+            gvo[h] = sgam[(long long)f * gstride + (long long)yy * W + xx];
+        }
+    }
+}
+
+template <bool F8>
+__global__ void __launch_bounds__(kCtaThreads)
+    infer_tc(const Src src, const float* __restrict__ params, float* __restrict__ u0,
+             int32_t* __restrict__ status) {
+    using F = Fmt<F8>;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ __align__(8) uint64_t full_bar[kSlots];   // a slot's layer MMAs completed
+    __shared__ __align__(8) uint64_t ready_bar[kSlots];  // a slot's next operand written
+    __shared__ uint32_t tmem_base_s;
+    __shared__ float red[kEpiGroups][8];
+    __shared__ float inv_wscale[4 * kC];  // E4M3: 1 / (column max |w| / 448), per layer
+    __shared__ int issued_s[kSlots], consumed_s[kSlots];
+    __shared__ volatile int abort_s;
+    const int t = threadIdx.x, warp = t >> 5, nthr = blockDim.x;
+
+    // ---- weights -> operand layouts, epilogue scales and biases, zeroed
+    //      activations ----------------------------------------------------------
+    float* sScale = reinterpret_cast<float*>(sm + F::kOffScale);
+    float* sBias = reinterpret_cast<float*>(sm + F::kOffBias);
+    load_network<F8>(params, sm + F::kOffW1, sm + F::kOffW2, sm + F::kOffW3, F::kWtapBytes,
+                     sm + F::kOffW4, sScale, sBias, inv_wscale, t, nthr);
+    for (int i = t; i < kEpiGroups * kStageBytes / 16; i += nthr)  // rows never written stay 0
+        reinterpret_cast<uint4*>(sm + F::kOffStage)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = t; i < kSlots * kTileBytes / 16; i += nthr)  // the feature planes' border
+        reinterpret_cast<uint4*>(sm + F::kOffTile)[i] = make_uint4(0u, 0u, 0u, 0u);
     for (int i = t; i < kSlots * F::kActBytes / 16; i += nthr)
         reinterpret_cast<uint4*>(sm + F::kOffAct)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (t == 0) {
@@ -601,46 +664,8 @@ __global__ void __launch_bounds__(kCtaThreads)
         float scale[2] = {1.0f, 1.0f};
         float dv[2][2] = {}, gv[2][2] = {};
 
-        // this thread's two pixels of a tile (the solvers' segmentation)
         auto gather = [&](long long tl, float (&dvo)[2], float (&gvo)[2]) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int p = tg + 128 * h, r = p >> 4, c = p & 15;
-                if (src.tile_mode) {
-                    dvo[h] = src.d[tl * 256 + p];
-                    gvo[h] = src.gamma[tl * 256 + p];
-                } else {
-                    const float* sd = src.d;
-                    const float* sgam = src.gamma;
-                    long long gstride = src.gamma_frame_stride, lt = tl,
-                              pf = (long long)src.tiles_x * src.tiles_y;
-                    int H = src.H, W = src.W, ty = src.tiles_y;
-                    if (src.stacks) {  // batched: the last stack whose first tile is <= tl
-                        int lo = 0, hi = src.n_stacks - 1;
-                        while (lo < hi) {
-                            const int mid = (lo + hi + 1) >> 1;
-                            if (src.stacks[mid].tile_begin <= tl) lo = mid;
-                            else hi = mid - 1;
-                        }
-                        const StackDesc& st = src.stacks[lo];
-                        sd = st.data;
-                        sgam = st.gamma;
-                        gstride = st.gamma_frame_stride;
-                        lt = tl - st.tile_begin;
-                        H = st.H;
-                        W = st.W;
-                        ty = st.tiles_y;
-                        pf = (long long)st.tiles_x * st.tiles_y;
-                    }
-                    const int f = (int)(lt / pf);
-                    const int rem = (int)(lt - (long long)f * pf);
-                    const int ti = rem / ty, tj = rem - ti * ty;
-                    const int yy = clampi(tile_origin(ti, H) + r - 1, 0, H - 1);
-                    const int xx = clampi(tile_origin(tj, W) + c - 1, 0, W - 1);
-                    dvo[h] = sd[(long long)f * H * W + (long long)yy * W + xx];
-                    gvo[h] = sgam[(long long)f * gstride + (long long)yy * W + xx];
-                }
-            }
+            gather_pixels(src, tl, tg, dvo, gvo);
         };
 
         // features of slot sl's tile from the gathered pixels, and the layer-1
@@ -875,6 +900,446 @@ __global__ void __launch_bounds__(kCtaThreads)
     }
 }
 
+// ---- E4M3 form on 16-wide rows ----------------------------------------------
+// The plane above spends 3 M blocks (384 rows) on 256 pixels: its rows are 18
+// wide so that the column shifts of the taps read the zero border.  Here each
+// activation is stored three times instead, as copies X_j[r][c] = X[r][c + j - 1]
+// (zero outside the tile) on 16-wide rows with a zero row above and below
+// (18 x 16 positions, [chunk][position][16 B]).  Tap (ky, kx) of the 128
+// pixels of block b (rows 8b .. 8b + 7) is then the window of copy kx that
+// starts at row 8b + ky: 2 M blocks per layer cover exactly the 256 pixels,
+// 40 MMAs per tile instead of 60, and a slot needs 64 tensor-memory columns,
+// so a CTA holds six slots, three per epilogue warpgroup.  The epilogue
+// writes each value three times (the copies' zero columns and rows are
+// never written and stay zero).  The layer-1 im2col operand lives in copy 1's
+// interior; layer 4's per-tap partial sums are summed over the taps' shifts
+// with the tile's edge tested per tap.
+namespace w16 {
+constexpr int kSlotsW = 6;                      // tiles in flight, three per warpgroup
+constexpr int kPerGroup = kSlotsW / kEpiGroups;
+constexpr int kRowPos = 18 * 16;               // positions of one copy
+constexpr int kChunk = kRowPos * 16;           // bytes per 16-channel chunk (the LBO)
+constexpr int kCopyBytes = 2 * kChunk;         // 32 E4M3 channels
+constexpr int kSlotBytes = 3 * kCopyBytes;     // the copies for shifts -1, 0, +1
+constexpr int kSlotCols = 64;                  // tensor-memory columns per slot
+constexpr int kStageW = 9 * 256 * 4;       // per warpgroup: partial sums [tap][pixel]
+constexpr int kFeatBytes = kFeatPlane * 8;     // per warpgroup: the feature plane
+constexpr int kWtapBytes = 2 * 32 * 16;        // per tap K 32 x N 32, E4M3
+constexpr int kOffW1 = 0;
+constexpr int kOffW2 = kOffW1 + 2 * 32 * 16;
+constexpr int kOffW3 = kOffW2 + 9 * kWtapBytes;
+constexpr int kOffW4 = kOffW3 + 9 * kWtapBytes;
+constexpr int kOffCopies = kOffW4 + 2 * 16 * 16;
+constexpr int kOffScale = kOffCopies + kSlotsW * kSlotBytes;
+constexpr int kOffBias = kOffScale + 128 * 4;
+constexpr int kOffTile = kOffBias + 128 * 4;   // per slot: d and gamma, 256 floats each
+constexpr int kOffFeat = kOffTile + kSlotsW * 2048;
+constexpr int kOffStage = kOffFeat + kEpiGroups * kFeatBytes;
+constexpr int kSmemBytes = kOffStage + kEpiGroups * kStageW;
+static_assert(kOffCopies % 128 == 0 && kSlotBytes % 128 == 0 && kOffTile % 16 == 0 &&
+                  kOffFeat % 16 == 0 && kOffStage % 16 == 0,
+              "operand and table alignment");
+static_assert(kSmemBytes + 2048 <= 227 * 1024, "one CTA per SM");
+static_assert(kSlotsW * kSlotCols <= (int)kTmemCols && kSlotsW % kEpiGroups == 0, "slots");
+}  // namespace w16
+
+__global__ void __launch_bounds__(kCtaThreads)
+    infer_tc_w16(const Src src, const float* __restrict__ params, float* __restrict__ u0,
+                 int32_t* __restrict__ status) {
+    using namespace w16;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ __align__(8) uint64_t full_bar[kSlotsW];   // a slot's layer MMAs completed
+    __shared__ __align__(8) uint64_t ready_bar[kSlotsW];  // a slot's next operand written
+    __shared__ uint32_t tmem_base_s;
+    __shared__ float red[kEpiGroups][8];
+    __shared__ float inv_wscale[4 * kC];
+    __shared__ int issued_s[kSlotsW], consumed_s[kSlotsW];
+    __shared__ volatile int abort_s;
+    const int t = threadIdx.x, warp = t >> 5, nthr = blockDim.x;
+
+    float* sScale = reinterpret_cast<float*>(sm + kOffScale);
+    float* sBias = reinterpret_cast<float*>(sm + kOffBias);
+    load_network<true>(params, sm + kOffW1, sm + kOffW2, sm + kOffW3, kWtapBytes, sm + kOffW4,
+                       sScale, sBias, inv_wscale, t, nthr);
+    // the copies (their zero rows and columns are never written), the
+    // feature planes' border and the stages
+    for (int i = t; i < kSlotsW * kSlotBytes / 16; i += nthr)
+        reinterpret_cast<uint4*>(sm + kOffCopies)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = t; i < (kSmemBytes - kOffFeat) / 16; i += nthr)
+        reinterpret_cast<uint4*>(sm + kOffFeat)[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (t == 0) {
+        for (int sl = 0; sl < kSlotsW; ++sl) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full_bar[sl]))
+                         : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(
+                             smem_u32(&ready_bar[sl]))
+                         : "memory");
+            issued_s[sl] = 0;
+            consumed_s[sl] = 0;
+        }
+        abort_s = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base_s)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_base_s;
+    const long long stride = (long long)kSlotsW * gridDim.x;  // tiles between a slot's tiles
+    auto first_tile = [&](int sl) { return (long long)blockIdx.x * kSlotsW + sl; };
+    auto fail = [&]() {
+        abort_s = 1;
+        if (status) atomicExch(status, 1);
+    };
+
+    if (warp >= kEpiGroups * 4) {
+        // ==== MMA-issuing warp ig (one per epilogue warpgroup, for its slots):
+        // lane 0 serves whichever slot's operand is ready; each slot runs
+        // layers 0..3 of its tiles in order ==================================
+        const int ig = warp - kEpiGroups * 4;
+        if ((t & 31) == 0) {
+            const uint32_t sW1a = smem_u32(sm + kOffW1), sW2a = smem_u32(sm + kOffW2);
+            const uint32_t sW3a = smem_u32(sm + kOffW3), sW4a = smem_u32(sm + kOffW4);
+            auto issue = [&](int sl, int ly) {
+                const uint32_t cp = smem_u32(sm + kOffCopies + sl * kSlotBytes);  // copy 0
+                const uint32_t td = tmem + (uint32_t)(sl * kSlotCols);
+                // copy 1's interior rows (the unshifted activations, or the im2col
+                // operand of layer 1) start at position 16
+                const uint64_t a_mid = sdesc(cp + kCopyBytes + 16 * 16, kChunk, 128);
+                if (ly == 0) {
+                    constexpr uint32_t id = idesc<true>(128, 32);
+                    const uint64_t b0 = sdesc(sW1a, 512, 128);
+#pragma unroll
+                    for (int b = 0; b < 2; ++b)
+                        mma<true>(td + b * 32, a_mid + ((128 * b * 16) >> 4), b0, id, 0u);
+                } else if (ly < 3) {
+                    constexpr uint32_t id = idesc<true>(128, 32);
+                    const uint64_t a0 = sdesc(cp, kChunk, 128);
+                    const uint64_t b0 = sdesc(ly == 1 ? sW2a : sW3a, 512, 128);
+#pragma unroll
+                    for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+                        for (int b = 0; b < 2; ++b) {
+                            // copy kx, window from row 8b + ky (position (8b + ky) 16)
+                            const int off = (tap % 3) * kCopyBytes + (8 * b + tap / 3) * 16 * 16;
+                            mma<true>(td + b * 32, a0 + (off >> 4),
+                                      b0 + ((tap * kWtapBytes) >> 4), id, tap != 0);
+                        }
+                } else {
+                    constexpr uint32_t id = idesc<true>(128, 16);
+                    const uint64_t b0 = sdesc(sW4a, 256, 128);
+#pragma unroll
+                    for (int b = 0; b < 2; ++b)
+                        mma<true>(td + b * 16, a_mid + ((128 * b * 16) >> 4), b0, id, 0u);
+                }
+                commit(smem_u32(&full_bar[sl]));
+                ++issued_s[sl];
+            };
+            // per-slot state (tile, layer, ready phase, slot) in registers,
+            // rotated so that the slot being polled is always the first
+            const long long n = src.n_tiles;
+            long long tA = first_tile(3 * ig), tB = first_tile(3 * ig + 1),
+                      tC = first_tile(3 * ig + 2);
+            int lA = 0, lB = 0, lC = 0, sA = 3 * ig, sB = 3 * ig + 1, sC = 3 * ig + 2;
+            uint32_t pA = 0, pB = 0, pC = 0;
+            int left = (tA < n) + (tB < n) + (tC < n);
+            int misses = 0;
+            long long idle_rounds = 0;
+            while (left > 0) {
+                if (tA < n && try_wait(smem_u32(&ready_bar[sA]), pA)) {
+                    pA ^= 1u;
+                    fence_after();
+                    issue(sA, lA);
+                    if (++lA == 4) {
+                        lA = 0;
+                        tA += stride;
+                        left -= tA >= n;
+                    }
+                    misses = 0;
+                    idle_rounds = 0;
+                } else if (++misses == kPerGroup) {
+                    // a round over the slots found no work: back off so the
+                    // epilogue warps sharing this scheduler get its issue slots
+                    misses = 0;
+                    if (abort_s) break;
+                    if (++idle_rounds > kIdlePolls) {
+                        fail();
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                const long long tt = tA;
+                const int ll = lA, ss = sA;
+                const uint32_t pp = pA;
+                tA = tB; lA = lB; sA = sB; pA = pB;
+                tB = tC; lB = lC; sB = sC; pB = pC;
+                tC = tt; lC = ll; sC = ss; pC = pp;
+            }
+        }
+    } else {
+        // ==== epilogue warpgroup g: slots 3g .. 3g + 2 ========================
+        const int g = warp >> 2, tg = t & 127, bar_id = 1 + g;
+        const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;  // this warp's TMEM lanes
+        float2* fplane = reinterpret_cast<float2*>(sm + kOffFeat + g * kFeatBytes);
+        float* stage = reinterpret_cast<float*>(sm + kOffStage + g * kStageW);
+        long long tile[kPerGroup];
+        int layer[kPerGroup];
+        uint32_t phase[kPerGroup];
+        float scale[kPerGroup], dv[kPerGroup][2], gv[kPerGroup][2];
+#pragma unroll
+        for (int k = 0; k < kPerGroup; ++k) {
+            layer[k] = 0;
+            phase[k] = 0u;
+            scale[k] = 1.0f;
+            dv[k][0] = dv[k][1] = gv[k][0] = gv[k][1] = 0.0f;
+        }
+
+        // features of slot k's tile from the gathered pixels (the warpgroup's
+        // zero-bordered plane), and the layer-1 im2col operand in copy 1's
+        // interior (whose previous reader, the slot's last layer, has completed)
+        auto build = [&](int k) {
+            const int sl = kPerGroup * g + k;
+            float* sD = reinterpret_cast<float*>(sm + kOffTile + sl * 2048);
+            float* sG = sD + 256;
+            float s1 = dv[k][0] + dv[k][1], s2 = dv[k][0] * dv[k][0] + dv[k][1] * dv[k][1];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            }
+            wg_sync(bar_id);  // earlier readers of red and of the feature plane are done
+            if ((t & 31) == 0) {
+                red[g][warp & 3] = s1;
+                red[g][4 + (warp & 3)] = s2;
+            }
+            wg_sync(bar_id);
+            const float mu = (red[g][0] + red[g][1] + red[g][2] + red[g][3]) * (1.0f / 256.0f);
+            const float sd = sqrtf(fmaxf((red[g][4] + red[g][5] + red[g][6] + red[g][7]) *
+                                             (1.0f / 256.0f) - mu * mu,
+                                         0.0f)) + 1.0f;
+            scale[k] = sd;
+            const float fs = f8_in_scale(0) / sd;  // the features carry layer 1's input scale
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int p = tg + 128 * h;
+                sD[p] = dv[k][h];
+                sG[p] = gv[k][h];
+                fplane[((p >> 4) + 1) * kPlane + (p & 15) + 2] =
+                    make_float2((dv[k][h] - mu) * fs,
+                                sqrtf(fmaxf(dv[k][h], 0.0f) + fmaxf(gv[k][h], 0.0f)) * fs);
+            }
+            wg_sync(bar_id);
+            unsigned char* c1 = sm + kOffCopies + sl * kSlotBytes + kCopyBytes;
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const int p = 128 * b + tg, r = p >> 4, c = p & 15;
+                float v[32];
+#pragma unroll
+                for (int tap = 0; tap < 9; ++tap) {
+                    // pixel (r + ky - 1, c + kx - 1) on the plane: index + 1
+                    const float2 x = fplane[(r + tap / 3) * kPlane + c + tap % 3 + 1];
+                    v[2 * tap] = x.x;
+                    v[2 * tap + 1] = x.y;
+                }
+#pragma unroll
+                for (int kk = 18; kk < 32; ++kk) v[kk] = 0.0f;
+                store_pos<true>(c1, kChunk, (r + 1) * 16 + c, v);
+            }
+        };
+
+        // the slot's operand writes (generic proxy) and tensor-memory reads
+        // are complete: hand the slot to the MMA warp
+        auto hand_over = [&](int k) {
+            fence_async_smem();
+            fence_before();
+            mbar_arrive(smem_u32(&ready_bar[kPerGroup * g + k]));
+        };
+
+        // epilogue of slot k's layer: this thread's accumulator row of both blocks
+        auto epilogue = [&](int k) {
+            const int sl = kPerGroup * g + k, ly = layer[k];
+            const uint32_t td = tmem + lane_off + (uint32_t)(sl * kSlotCols);
+            if (ly < 3) {
+                float sc[32], bias[32];
+                {
+                    const float4* sc4 = reinterpret_cast<const float4*>(sScale + 32 * ly);
+                    const float4* b4 = reinterpret_cast<const float4*>(sBias + 32 * ly);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const float4 a = sc4[i], bb = b4[i];
+                        sc[4 * i] = a.x; sc[4 * i + 1] = a.y; sc[4 * i + 2] = a.z; sc[4 * i + 3] = a.w;
+                        bias[4 * i] = bb.x; bias[4 * i + 1] = bb.y; bias[4 * i + 2] = bb.z;
+                        bias[4 * i + 3] = bb.w;
+                    }
+                }
+                unsigned char* cp = sm + kOffCopies + sl * kSlotBytes;
+                uint32_t ra[32], rb[32];
+                tmem_ld32_issue(td, ra);
+                tmem_ld32_issue(td + 32, rb);
+                tmem_wait32(ra);
+                after_wait32(rb);
+                // pixel p's activations into the three copies: copy 1 at (r, c),
+                // copy 0 at (r, c + 1), copy 2 at (r, c - 1) where inside the tile
+                auto finish = [&](int b, const uint32_t (&r32)[32]) {
+                    const int p = 128 * b + tg, r = p >> 4, c = p & 15;
+                    float v[32];
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) v[i] = fmaf(__uint_as_float(r32[i]), sc[i], bias[i]);
+                    uint4 w[2];
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk) {
+                        const float* cv = v + 16 * kk;
+                        uint32_t q[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            q[j] = __byte_perm(relu_e4m3x2(cv[4 * j], cv[4 * j + 1]),
+                                               relu_e4m3x2(cv[4 * j + 2], cv[4 * j + 3]), 0x5410);
+                        w[kk] = make_uint4(q[0], q[1], q[2], q[3]);
+                    }
+                    const int pos = (r + 1) * 16 + c;
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk) {
+                        *reinterpret_cast<uint4*>(cp + kCopyBytes + kk * kChunk + pos * 16) = w[kk];
+                        if (c < 15)
+                            *reinterpret_cast<uint4*>(cp + kk * kChunk + (pos + 1) * 16) = w[kk];
+                        if (c > 0)
+                            *reinterpret_cast<uint4*>(cp + 2 * kCopyBytes + kk * kChunk +
+                                                      (pos - 1) * 16) = w[kk];
+                    }
+                };
+                finish(0, ra);
+                finish(1, rb);
+            } else {
+                // D[p][tap] (= sum_ci a[p][ci] w[ci][tap]) -> stage[tap][p]
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    uint32_t r16[16];
+                    tmem_ld16(td + b * 16, r16);
+#pragma unroll
+                    for (int tap = 0; tap < 9; ++tap)
+                        stage[tap * 256 + 128 * b + tg] = __uint_as_float(r16[tap]);
+                }
+                wg_sync(bar_id);
+                // y(p) = sum over the taps inside the tile of D[p + (ky-1) 16 + (kx-1)][tap]
+                const float* sD = reinterpret_cast<const float*>(sm + kOffTile + sl * 2048);
+                const float* sG = sD + 256;
+                const float sdv = scale[k];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int p = tg + 128 * h, r = p >> 4, c = p & 15;
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int tap = 0; tap < 9; ++tap) {
+                        const int rr = r + tap / 3 - 1, cc = c + tap % 3 - 1;
+                        if (rr >= 0 && rr < 16 && cc >= 0 && cc < 16)
+                            acc += stage[tap * 256 + rr * 16 + cc];
+                    }
+                    const float y = fmaf(acc, sScale[96], sBias[96]);
+                    const float d = sD[p], gm = sG[p];
+                    const float lo = kStartFrac * fmaxf(d + gm, 1e-3f) - gm;
+                    u0[tile[k] * 256 + p] = fmaxf(fmaf(sdv, y, d), lo);
+                }
+            }
+        };
+
+        // ---- start: each slot's first tile ---------------------------------
+#pragma unroll
+        for (int k = 0; k < kPerGroup; ++k) {
+            tile[k] = first_tile(kPerGroup * g + k);
+            if (tile[k] < src.n_tiles) gather_pixels(src, tile[k], tg, dv[k], gv[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < kPerGroup; ++k) {
+            if (tile[k] >= src.n_tiles) continue;
+            build(k);
+            hand_over(k);
+            if (tile[k] + stride < src.n_tiles) gather_pixels(src, tile[k] + stride, tg, dv[k], gv[k]);
+        }
+
+        // ---- rotate over the slots until they run out of tiles ---------------
+        // (tile, layer and stop are uniform over the warpgroup: every branch
+        // below is taken by all 128 threads, as its named barriers require)
+        bool stop = false;
+        for (;;) {
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < kPerGroup; ++k) {
+                if (tile[k] >= src.n_tiles) continue;
+                any = true;
+                const int sl = kPerGroup * g + k;
+                bool ok = false;
+                for (long long i = 0; i < kWaitTries && !ok; ++i) {
+                    ok = try_wait(smem_u32(&full_bar[sl]), phase[k]);
+                    if (!ok && abort_s) break;
+                }
+                if (!wg_all(bar_id, ok)) {
+                    if (tg == 0) fail();
+                    stop = true;
+                    break;
+                }
+                phase[k] ^= 1u;
+                if (tg == 0) ++consumed_s[sl];
+                fence_after();
+                epilogue(k);
+                if (layer[k] < 3) {
+                    ++layer[k];
+                    hand_over(k);
+                } else {
+                    // tile done: its successor's pixels were gathered during its layers
+                    tile[k] += stride;
+                    layer[k] = 0;
+                    if (tile[k] < src.n_tiles) {
+                        build(k);
+                        hand_over(k);
+                        if (tile[k] + stride < src.n_tiles)
+                            gather_pixels(src, tile[k] + stride, tg, dv[k], gv[k]);
+                    }
+                }
+            }
+            if (!any || stop) break;
+        }
+    }
+
+    __syncwarp();
+    __syncthreads();
+    if (t == 0 && abort_s) {
+        // drain: give every slot's outstanding MMAs a bounded time to complete
+        for (int sl = 0; sl < kSlotsW; ++sl)
+            for (int c = consumed_s[sl]; c < issued_s[sl]; ++c)
+                wait_bounded(smem_u32(&full_bar[sl]), (uint32_t)(c & 1));
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+int launch_w16(const Src& src, const float* params, float* u0, int32_t* status, cudaStream_t s) {
+    if (cudaFuncSetAttribute(infer_tc_w16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             w16::kSmemBytes) != cudaSuccess)
+        return NCSB_ECUDA;
+    cudaFuncSetAttribute(infer_tc_w16, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    int dev = 0, sms = 1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NCSB_ECUDA;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // one persistent CTA per SM (its shared memory allows no second one)
+    long long grid = sms;
+    if (grid > (src.n_tiles + w16::kSlotsW - 1) / w16::kSlotsW)
+        grid = (src.n_tiles + w16::kSlotsW - 1) / w16::kSlotsW;
+    infer_tc_w16<<<(unsigned)grid, kCtaThreads, w16::kSmemBytes, s>>>(src, params, u0, status);
+    return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
+}
+
 template <bool F8>
 int launch_fmt(const Src& src, const float* params, float* u0, int32_t* status, cudaStream_t s) {
     // at least 120 KB, so that a second CTA never shares an SM: each CTA
@@ -897,7 +1362,7 @@ int launch_fmt(const Src& src, const float* params, float* u0, int32_t* status, 
 
 int launch(const Src& src, const float* params, float* u0, int32_t* status, bool fp8,
            cudaStream_t s) {
-    return fp8 ? launch_fmt<true>(src, params, u0, status, s)
+    return fp8 ? launch_w16(src, params, u0, status, s)
                : launch_fmt<false>(src, params, u0, status, s);
 }
 

@@ -915,14 +915,15 @@ __global__ void __launch_bounds__(kCtaThreads)
 // interior; layer 4's per-tap partial sums are summed over the taps' shifts
 // with the tile's edge tested per tap.
 namespace w16 {
-constexpr int kSlotsW = 6;                      // tiles in flight, three per warpgroup
-constexpr int kPerGroup = kSlotsW / kEpiGroups;
+constexpr int kGroups = 3;                     // epilogue warpgroups, each with an MMA warp
+constexpr int kThreadsW = 160 * kGroups;
+constexpr int kSlotsW = 6;                     // tiles in flight, two per warpgroup
+constexpr int kPerGroup = kSlotsW / kGroups;
 constexpr int kRowPos = 18 * 16;               // positions of one copy
 constexpr int kChunk = kRowPos * 16;           // bytes per 16-channel chunk (the LBO)
 constexpr int kCopyBytes = 2 * kChunk;         // 32 E4M3 channels
 constexpr int kSlotBytes = 3 * kCopyBytes;     // the copies for shifts -1, 0, +1
 constexpr int kSlotCols = 64;                  // tensor-memory columns per slot
-constexpr int kStageW = 9 * 256 * 4;       // per warpgroup: partial sums [tap][pixel]
 constexpr int kFeatBytes = kFeatPlane * 8;     // per warpgroup: the feature plane
 constexpr int kWtapBytes = 2 * 32 * 16;        // per tap K 32 x N 32, E4M3
 constexpr int kOffW1 = 0;
@@ -934,16 +935,17 @@ constexpr int kOffScale = kOffCopies + kSlotsW * kSlotBytes;
 constexpr int kOffBias = kOffScale + 128 * 4;
 constexpr int kOffTile = kOffBias + 128 * 4;   // per slot: d and gamma, 256 floats each
 constexpr int kOffFeat = kOffTile + kSlotsW * 2048;
-constexpr int kOffStage = kOffFeat + kEpiGroups * kFeatBytes;
-constexpr int kSmemBytes = kOffStage + kEpiGroups * kStageW;
+constexpr int kSmemBytes = kOffFeat + kGroups * kFeatBytes;
 static_assert(kOffCopies % 128 == 0 && kSlotBytes % 128 == 0 && kOffTile % 16 == 0 &&
-                  kOffFeat % 16 == 0 && kOffStage % 16 == 0,
+                  kOffFeat % 16 == 0,
               "operand and table alignment");
 static_assert(kSmemBytes + 2048 <= 227 * 1024, "one CTA per SM");
-static_assert(kSlotsW * kSlotCols <= (int)kTmemCols && kSlotsW % kEpiGroups == 0, "slots");
+static_assert(kSlotsW * kSlotCols <= (int)kTmemCols && kSlotsW == 2 * kGroups, "slots");
+// the last layer's partial sums [tap][pixel] are staged in the slot's copy 0
+static_assert(9 * 256 * 4 == kCopyBytes, "stage size");
 }  // namespace w16
 
-__global__ void __launch_bounds__(kCtaThreads)
+__global__ void __launch_bounds__(w16::kThreadsW)
     infer_tc_w16(const Src src, const float* __restrict__ params, float* __restrict__ u0,
                  int32_t* __restrict__ status) {
     using namespace w16;
@@ -951,7 +953,7 @@ __global__ void __launch_bounds__(kCtaThreads)
     __shared__ __align__(8) uint64_t full_bar[kSlotsW];   // a slot's layer MMAs completed
     __shared__ __align__(8) uint64_t ready_bar[kSlotsW];  // a slot's next operand written
     __shared__ uint32_t tmem_base_s;
-    __shared__ float red[kEpiGroups][8];
+    __shared__ float red[kGroups][8];
     __shared__ float inv_wscale[4 * kC];
     __shared__ int issued_s[kSlotsW], consumed_s[kSlotsW];
     __shared__ volatile int abort_s;
@@ -961,8 +963,8 @@ __global__ void __launch_bounds__(kCtaThreads)
     float* sBias = reinterpret_cast<float*>(sm + kOffBias);
     load_network<true>(params, sm + kOffW1, sm + kOffW2, sm + kOffW3, kWtapBytes, sm + kOffW4,
                        sScale, sBias, inv_wscale, t, nthr);
-    // the copies (their zero rows and columns are never written), the
-    // feature planes' border and the stages
+    // the copies (their zero rows and columns are never written but by the
+    // last layer's stage, which restores them) and the feature planes' border
     for (int i = t; i < kSlotsW * kSlotBytes / 16; i += nthr)
         reinterpret_cast<uint4*>(sm + kOffCopies)[i] = make_uint4(0u, 0u, 0u, 0u);
     for (int i = t; i < (kSmemBytes - kOffFeat) / 16; i += nthr)
@@ -997,11 +999,11 @@ __global__ void __launch_bounds__(kCtaThreads)
         if (status) atomicExch(status, 1);
     };
 
-    if (warp >= kEpiGroups * 4) {
+    if (warp >= kGroups * 4) {
         // ==== MMA-issuing warp ig (one per epilogue warpgroup, for its slots):
         // lane 0 serves whichever slot's operand is ready; each slot runs
         // layers 0..3 of its tiles in order ==================================
-        const int ig = warp - kEpiGroups * 4;
+        const int ig = warp - kGroups * 4;
         if ((t & 31) == 0) {
             const uint32_t sW1a = smem_u32(sm + kOffW1), sW2a = smem_u32(sm + kOffW2);
             const uint32_t sW3a = smem_u32(sm + kOffW3), sW4a = smem_u32(sm + kOffW4);
@@ -1043,11 +1045,10 @@ __global__ void __launch_bounds__(kCtaThreads)
             // per-slot state (tile, layer, ready phase, slot) in registers,
             // rotated so that the slot being polled is always the first
             const long long n = src.n_tiles;
-            long long tA = first_tile(3 * ig), tB = first_tile(3 * ig + 1),
-                      tC = first_tile(3 * ig + 2);
-            int lA = 0, lB = 0, lC = 0, sA = 3 * ig, sB = 3 * ig + 1, sC = 3 * ig + 2;
-            uint32_t pA = 0, pB = 0, pC = 0;
-            int left = (tA < n) + (tB < n) + (tC < n);
+            long long tA = first_tile(2 * ig), tB = first_tile(2 * ig + 1);
+            int lA = 0, lB = 0, sA = 2 * ig, sB = 2 * ig + 1;
+            uint32_t pA = 0, pB = 0;
+            int left = (tA < n) + (tB < n);
             int misses = 0;
             long long idle_rounds = 0;
             while (left > 0) {
@@ -1077,16 +1078,14 @@ __global__ void __launch_bounds__(kCtaThreads)
                 const int ll = lA, ss = sA;
                 const uint32_t pp = pA;
                 tA = tB; lA = lB; sA = sB; pA = pB;
-                tB = tC; lB = lC; sB = sC; pB = pC;
-                tC = tt; lC = ll; sC = ss; pC = pp;
+                tB = tt; lB = ll; sB = ss; pB = pp;
             }
         }
     } else {
-        // ==== epilogue warpgroup g: slots 3g .. 3g + 2 ========================
+        // ==== epilogue warpgroup g: slots 2g and 2g + 1 =======================
         const int g = warp >> 2, tg = t & 127, bar_id = 1 + g;
         const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;  // this warp's TMEM lanes
         float2* fplane = reinterpret_cast<float2*>(sm + kOffFeat + g * kFeatBytes);
-        float* stage = reinterpret_cast<float*>(sm + kOffStage + g * kStageW);
         long long tile[kPerGroup];
         int layer[kPerGroup];
         uint32_t phase[kPerGroup];
@@ -1165,40 +1164,32 @@ __global__ void __launch_bounds__(kCtaThreads)
             const int sl = kPerGroup * g + k, ly = layer[k];
             const uint32_t td = tmem + lane_off + (uint32_t)(sl * kSlotCols);
             if (ly < 3) {
-                float sc[32], bias[32];
-                {
-                    const float4* sc4 = reinterpret_cast<const float4*>(sScale + 32 * ly);
-                    const float4* b4 = reinterpret_cast<const float4*>(sBias + 32 * ly);
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const float4 a = sc4[i], bb = b4[i];
-                        sc[4 * i] = a.x; sc[4 * i + 1] = a.y; sc[4 * i + 2] = a.z; sc[4 * i + 3] = a.w;
-                        bias[4 * i] = bb.x; bias[4 * i + 1] = bb.y; bias[4 * i + 2] = bb.z;
-                        bias[4 * i + 3] = bb.w;
-                    }
-                }
+                const float4* sc4 = reinterpret_cast<const float4*>(sScale + 32 * ly);
+                const float4* b4 = reinterpret_cast<const float4*>(sBias + 32 * ly);
                 unsigned char* cp = sm + kOffCopies + sl * kSlotBytes;
-                uint32_t ra[32], rb[32];
-                tmem_ld32_issue(td, ra);
-                tmem_ld32_issue(td + 32, rb);
-                tmem_wait32(ra);
-                after_wait32(rb);
                 // pixel p's activations into the three copies: copy 1 at (r, c),
                 // copy 0 at (r, c + 1), copy 2 at (r, c - 1) where inside the tile
-                auto finish = [&](int b, const uint32_t (&r32)[32]) {
+#pragma unroll 1
+                for (int b = 0; b < 2; ++b) {
+                    uint32_t r32[32];
+                    tmem_ld32_issue(td + 32 * b, r32);
+                    tmem_wait32(r32);
                     const int p = 128 * b + tg, r = p >> 4, c = p & 15;
-                    float v[32];
-#pragma unroll
-                    for (int i = 0; i < 32; ++i) v[i] = fmaf(__uint_as_float(r32[i]), sc[i], bias[i]);
                     uint4 w[2];
 #pragma unroll
                     for (int kk = 0; kk < 2; ++kk) {
-                        const float* cv = v + 16 * kk;
                         uint32_t q[4];
 #pragma unroll
-                        for (int j = 0; j < 4; ++j)
-                            q[j] = __byte_perm(relu_e4m3x2(cv[4 * j], cv[4 * j + 1]),
-                                               relu_e4m3x2(cv[4 * j + 2], cv[4 * j + 3]), 0x5410);
+                        for (int j = 0; j < 4; ++j) {
+                            const int i0 = 16 * kk + 4 * j;
+                            const float4 s = sc4[i0 >> 2], o = b4[i0 >> 2];
+                            q[j] = __byte_perm(
+                                relu_e4m3x2(fmaf(__uint_as_float(r32[i0]), s.x, o.x),
+                                            fmaf(__uint_as_float(r32[i0 + 1]), s.y, o.y)),
+                                relu_e4m3x2(fmaf(__uint_as_float(r32[i0 + 2]), s.z, o.z),
+                                            fmaf(__uint_as_float(r32[i0 + 3]), s.w, o.w)),
+                                0x5410);
+                        }
                         w[kk] = make_uint4(q[0], q[1], q[2], q[3]);
                     }
                     const int pos = (r + 1) * 16 + c;
@@ -1211,11 +1202,12 @@ __global__ void __launch_bounds__(kCtaThreads)
                             *reinterpret_cast<uint4*>(cp + 2 * kCopyBytes + kk * kChunk +
                                                       (pos - 1) * 16) = w[kk];
                     }
-                };
-                finish(0, ra);
-                finish(1, rb);
+                }
             } else {
-                // D[p][tap] (= sum_ci a[p][ci] w[ci][tap]) -> stage[tap][p]
+                // D[p][tap] (= sum_ci a[p][ci] w[ci][tap]) -> stage[tap][p], in the
+                // slot's copy 0: the layer-4 MMAs read copy 1 only, and copy 0's
+                // next reader is the next tile's layer 2
+                float* stage = reinterpret_cast<float*>(sm + kOffCopies + sl * kSlotBytes);
 #pragma unroll
                 for (int b = 0; b < 2; ++b) {
                     uint32_t r16[16];
@@ -1243,6 +1235,15 @@ __global__ void __launch_bounds__(kCtaThreads)
                     const float d = sD[p], gm = sG[p];
                     const float lo = kStartFrac * fmaxf(d + gm, 1e-3f) - gm;
                     u0[tile[k] * 256 + p] = fmaxf(fmaf(sdv, y, d), lo);
+                }
+                // copy 0's zero positions again (rows 0 and 17, column 0): 48
+                // positions x 2 chunks, once every thread has read the stage
+                wg_sync(bar_id);
+                if (tg < 96) {
+                    const int z = tg >> 1, kk = tg & 1;
+                    const int pos = z < 16 ? z : (z < 32 ? 272 + (z - 16) : (z - 31) * 16);
+                    *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(stage) +
+                                              kk * kChunk + pos * 16) = make_uint4(0u, 0u, 0u, 0u);
                 }
             }
         };
@@ -1336,7 +1337,8 @@ int launch_w16(const Src& src, const float* params, float* u0, int32_t* status, 
     long long grid = sms;
     if (grid > (src.n_tiles + w16::kSlotsW - 1) / w16::kSlotsW)
         grid = (src.n_tiles + w16::kSlotsW - 1) / w16::kSlotsW;
-    infer_tc_w16<<<(unsigned)grid, kCtaThreads, w16::kSmemBytes, s>>>(src, params, u0, status);
+    infer_tc_w16<<<(unsigned)grid, w16::kThreadsW, w16::kSmemBytes, s>>>(src, params, u0,
+                                                                          status);
     return cudaGetLastError() == cudaSuccess ? NCSB_OK : NCSB_ECUDA;
 }
 

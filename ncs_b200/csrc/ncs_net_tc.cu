@@ -17,8 +17,8 @@
 // infer_tc_w16 (E4M3 operands, kind::f8f6f4, K = 32 per MMA: half the
 // operand bytes of BF16).  Each activation is stored as three column-shifted
 // copies on 16-wide rows, so that 2 M blocks cover exactly the 256 pixels
-// (40 MMAs per tile instead of 60) and a slot needs 64 tensor-memory
-// columns: six slots, three per warpgroup (the description at the kernel).
+// and a slot needs 64 tensor-memory columns: six slots, two per warpgroup
+// of three (the description at the kernel).
 // Each output channel's weights are scaled by max|w| / 448 before rounding,
 // and each layer's input by a fixed power of two (features x 8, hidden
 // activations x 4: 56 and 112 at E4M3's largest value, against 14 and 41
@@ -238,6 +238,13 @@ __device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t (&r)[32
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
 }
+// One accumulator column of this thread's lane.
+__device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r) : : "memory");
+    return __uint_as_float(r);
+}
 // Waits for this thread's tensor-memory loads; r (one load's registers) is
 // an operand so that no read of it moves above the wait.
 __device__ __forceinline__ void tmem_wait32(uint32_t (&r)[32]) {
@@ -418,7 +425,7 @@ template <bool F8>
 __device__ void load_network(const float* __restrict__ params, unsigned char* sW1,
                              unsigned char* sW2, unsigned char* sW3, int tap_bytes,
                              unsigned char* sW4, float* sScale, float* sBias, float* inv_wscale,
-                             int t, int nthr) {
+                             int t, int nthr, bool w4_per_tap = false) {
     const float* w1 = params;
     const float* b1 = w1 + 2 * 9 * kC;
     const float* w2 = b1 + kC;
@@ -455,9 +462,17 @@ __device__ void load_network(const float* __restrict__ params, unsigned char* sW
                            inv_wscale[32 * l + co]);
         }
     }
-    for (int i = t; i < 32 * 16; i += nthr) {
-        const int ci = i >> 4, n = i & 15;
-        put_weight<F8>(sW4, 16, ci, n, n < 9 ? weight(3, ci, n, 0) : 0.0f, inv_wscale[96]);
+    if (w4_per_tap) {  // per tap B[ci][n], the one output channel in column 0
+        for (int i = t; i < 9 * 32 * 16; i += nthr) {
+            const int tap = i / 512, rem = i - tap * 512, ci = rem >> 4, n = rem & 15;
+            put_weight<F8>(sW4 + tap * (tap_bytes / 2), 16, ci, n,
+                           n == 0 ? weight(3, ci, tap, 0) : 0.0f, inv_wscale[96]);
+        }
+    } else {
+        for (int i = t; i < 32 * 16; i += nthr) {
+            const int ci = i >> 4, n = i & 15;
+            put_weight<F8>(sW4, 16, ci, n, n < 9 ? weight(3, ci, n, 0) : 0.0f, inv_wscale[96]);
+        }
     }
     for (int i = t; i < 97; i += nthr) {
         const int l = i >> 5;
@@ -908,12 +923,12 @@ __global__ void __launch_bounds__(kCtaThreads)
 // (18 x 16 positions, [chunk][position][16 B]).  Tap (ky, kx) of the 128
 // pixels of block b (rows 8b .. 8b + 7) is then the window of copy kx that
 // starts at row 8b + ky: 2 M blocks per layer cover exactly the 256 pixels,
-// 40 MMAs per tile instead of 60, and a slot needs 64 tensor-memory columns,
-// so a CTA holds six slots, three per epilogue warpgroup.  The epilogue
+// a slot needs 64 tensor-memory columns, so a CTA holds six slots, two per
+// epilogue warpgroup.  The epilogue
 // writes each value three times (the copies' zero columns and rows are
 // never written and stay zero).  The layer-1 im2col operand lives in copy 1's
-// interior; layer 4's per-tap partial sums are summed over the taps' shifts
-// with the tile's edge tested per tap.
+// interior; layer 4 (one output channel, zero-padded to N = 16) runs like the
+// hidden layers, 18 more MMAs that leave the epilogue a single column.
 namespace w16 {
 constexpr int kGroups = 3;                     // epilogue warpgroups, each with an MMA warp
 constexpr int kThreadsW = 160 * kGroups;
@@ -930,7 +945,8 @@ constexpr int kOffW1 = 0;
 constexpr int kOffW2 = kOffW1 + 2 * 32 * 16;
 constexpr int kOffW3 = kOffW2 + 9 * kWtapBytes;
 constexpr int kOffW4 = kOffW3 + 9 * kWtapBytes;
-constexpr int kOffCopies = kOffW4 + 2 * 16 * 16;
+constexpr int kW4tapBytes = 2 * 16 * 16;      // layer 4: per tap K 32 x N 16
+constexpr int kOffCopies = kOffW4 + 9 * kW4tapBytes;
 constexpr int kOffScale = kOffCopies + kSlotsW * kSlotBytes;
 constexpr int kOffBias = kOffScale + 128 * 4;
 constexpr int kOffTile = kOffBias + 128 * 4;   // per slot: d and gamma, 256 floats each
@@ -941,8 +957,7 @@ static_assert(kOffCopies % 128 == 0 && kSlotBytes % 128 == 0 && kOffTile % 16 ==
               "operand and table alignment");
 static_assert(kSmemBytes + 2048 <= 227 * 1024, "one CTA per SM");
 static_assert(kSlotsW * kSlotCols <= (int)kTmemCols && kSlotsW == 2 * kGroups, "slots");
-// the last layer's partial sums [tap][pixel] are staged in the slot's copy 0
-static_assert(9 * 256 * 4 == kCopyBytes, "stage size");
+static_assert(kWtapBytes == 2 * kW4tapBytes, "load_network's per-tap layer-4 stride");
 }  // namespace w16
 
 __global__ void __launch_bounds__(w16::kThreadsW)
@@ -962,9 +977,9 @@ __global__ void __launch_bounds__(w16::kThreadsW)
     float* sScale = reinterpret_cast<float*>(sm + kOffScale);
     float* sBias = reinterpret_cast<float*>(sm + kOffBias);
     load_network<true>(params, sm + kOffW1, sm + kOffW2, sm + kOffW3, kWtapBytes, sm + kOffW4,
-                       sScale, sBias, inv_wscale, t, nthr);
-    // the copies (their zero rows and columns are never written but by the
-    // last layer's stage, which restores them) and the feature planes' border
+                       sScale, sBias, inv_wscale, t, nthr, true);
+    // the copies (their zero rows and columns are never written) and the
+    // feature planes' border
     for (int i = t; i < kSlotsW * kSlotBytes / 16; i += nthr)
         reinterpret_cast<uint4*>(sm + kOffCopies)[i] = make_uint4(0u, 0u, 0u, 0u);
     for (int i = t; i < (kSmemBytes - kOffFeat) / 16; i += nthr)
@@ -1034,10 +1049,16 @@ __global__ void __launch_bounds__(w16::kThreadsW)
                         }
                 } else {
                     constexpr uint32_t id = idesc<true>(128, 16);
+                    const uint64_t a0 = sdesc(cp, kChunk, 128);
                     const uint64_t b0 = sdesc(sW4a, 256, 128);
 #pragma unroll
-                    for (int b = 0; b < 2; ++b)
-                        mma<true>(td + b * 16, a_mid + ((128 * b * 16) >> 4), b0, id, 0u);
+                    for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+                        for (int b = 0; b < 2; ++b) {
+                            const int off = (tap % 3) * kCopyBytes + (8 * b + tap / 3) * 16 * 16;
+                            mma<true>(td + b * 16, a0 + (off >> 4),
+                                      b0 + ((tap * kW4tapBytes) >> 4), id, tap != 0);
+                        }
                 }
                 commit(smem_u32(&full_bar[sl]));
                 ++issued_s[sl];
@@ -1204,46 +1225,17 @@ __global__ void __launch_bounds__(w16::kThreadsW)
                     }
                 }
             } else {
-                // D[p][tap] (= sum_ci a[p][ci] w[ci][tap]) -> stage[tap][p], in the
-                // slot's copy 0: the layer-4 MMAs read copy 1 only, and copy 0's
-                // next reader is the next tile's layer 2
-                float* stage = reinterpret_cast<float*>(sm + kOffCopies + sl * kSlotBytes);
-#pragma unroll
-                for (int b = 0; b < 2; ++b) {
-                    uint32_t r16[16];
-                    tmem_ld16(td + b * 16, r16);
-#pragma unroll
-                    for (int tap = 0; tap < 9; ++tap)
-                        stage[tap * 256 + 128 * b + tg] = __uint_as_float(r16[tap]);
-                }
-                wg_sync(bar_id);
-                // y(p) = sum over the taps inside the tile of D[p + (ky-1) 16 + (kx-1)][tap]
+                // the one output channel: column 0 of both blocks
                 const float* sD = reinterpret_cast<const float*>(sm + kOffTile + sl * 2048);
                 const float* sG = sD + 256;
                 const float sdv = scale[k];
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int p = tg + 128 * h, r = p >> 4, c = p & 15;
-                    float acc = 0.0f;
-#pragma unroll
-                    for (int tap = 0; tap < 9; ++tap) {
-                        const int rr = r + tap / 3 - 1, cc = c + tap % 3 - 1;
-                        if (rr >= 0 && rr < 16 && cc >= 0 && cc < 16)
-                            acc += stage[tap * 256 + rr * 16 + cc];
-                    }
-                    const float y = fmaf(acc, sScale[96], sBias[96]);
+                for (int b = 0; b < 2; ++b) {
+                    const int p = 128 * b + tg;
+                    const float y = fmaf(tmem_ld1(td + b * 16), sScale[96], sBias[96]);
                     const float d = sD[p], gm = sG[p];
                     const float lo = kStartFrac * fmaxf(d + gm, 1e-3f) - gm;
                     u0[tile[k] * 256 + p] = fmaxf(fmaf(sdv, y, d), lo);
-                }
-                // copy 0's zero positions again (rows 0 and 17, column 0): 48
-                // positions x 2 chunks, once every thread has read the stage
-                wg_sync(bar_id);
-                if (tg < 96) {
-                    const int z = tg >> 1, kk = tg & 1;
-                    const int pos = z < 16 ? z : (z < 32 ? 272 + (z - 16) : (z - 31) * 16);
-                    *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(stage) +
-                                              kk * kChunk + pos * 16) = make_uint4(0u, 0u, 0u, 0u);
                 }
             }
         };

@@ -68,7 +68,9 @@ constexpr int kM = 16 * kTiles;
 constexpr int kTcWarps = kTiles;
 constexpr int kTcThreads = 32 * kTcWarps;
 constexpr int kMinBlocks = 16 / kTiles;  // 128 registers a thread fill the register file
-constexpr uint32_t kTmemCols = 128;        // D of stages 1..4 at columns 0, 32, 64, 96
+// D of stages 1 and 3 at column 0, of stages 2 and 4 at column 32: a stage's
+// accumulators are read before the MMAs of the stage after next are issued
+constexpr uint32_t kTmemCols = 64;
 constexpr long long kWaitTries = 1ll << 17;  // mbarrier polls of <= 20 us before giving up
 constexpr long long kSpinTries = 1ll << 26;  // mbarrier polls without suspending (seconds)
 
@@ -240,7 +242,7 @@ __device__ __forceinline__ void issue_stage(int stage, uint32_t tmem, uint32_t s
                                                                             : PL::B1 + 2 * PL::B2));
     const uint32_t a = stage == 1 ? sa1 : sa2;
     const uint32_t apart = stage == 1 ? PL::A1 : PL::A2;
-    const uint32_t col = (uint32_t)(stage - 1) * 32;
+    const uint32_t col = (uint32_t)((stage - 1) & 1) * 32;
     // K steps of 2 chunks (TF32: K 8; BF16: K 16) -- stage 4 only up to K 24 / 32
     const int steps = BF ? (stage == 1 ? 1 : 2) : (stage == 1 ? 2 : (stage == 4 ? 3 : 4));
     for (int s = 0; s < steps; ++s) {
@@ -572,7 +574,7 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
         if (!run_stage(3)) break;
         if (has_tile) {
             float e[16];
-            tc::tmem_ld_16x256b_x4(tlane + 64, e);
+            tc::tmem_ld_16x256b_x4(tlane + 0, e);
             tc::tmem_wait_ld();
             // (Re, Im) of W[r][kc] for r = 4 q + Qd, kc = P (and 8): stage-4 row r, K = 2 kc
 #pragma unroll
@@ -585,7 +587,7 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
         if (!run_stage(4)) break;
         if (has_tile) {
             float e[8];
-            tc::tmem_ld_16x256b_x2(tlane + 96, e);
+            tc::tmem_ld_16x256b_x2(tlane + 32, e);
             tc::tmem_wait_ld();
             p[0] = e[0]; p[1] = e[2]; p[2] = e[1]; p[3] = e[3];
             p[4] = e[4]; p[5] = e[6]; p[6] = e[5]; p[7] = e[7];

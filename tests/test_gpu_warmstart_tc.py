@@ -107,3 +107,24 @@ def test_tc_stack_equals_tiles_and_solve_gain(ws, fp8):
     assert it1.float().mean().item() <= it0.float().mean().item() - 0.5
     rel = ((c1 - c0).abs() / c0.abs().clamp(min=1.0)).max().item()
     assert rel <= 1e-6   # both converge to the same per-tile optimum
+
+
+def test_fp8_many_tiles_per_slot(ws):
+    """Each slot of the E4M3 kernel processes several tiles in turn (20 frames
+    of 256 x 256: about eight per slot), so its activation copies are reused
+    with their zero rows and columns: sampled tiles match the oracle's E4M3
+    restatement at every position in the order they ran."""
+    from ncs_b200 import sim
+    w = sim.make_stack("frame256", T=20, seed=9)
+    net = ws.WarmStartNet.load()
+    u, st = net.propose_stack_tc(w["images"], w["gamma"], fp8=True)
+    assert int(st.item()) == 0
+    d, g = ws.cut_tiles(w["images"], w["gamma"])
+    n = d.shape[0]
+    idx = numpy.unique(numpy.concatenate([numpy.arange(0, n, 97), [n - 1]]))
+    dn = d.cpu().numpy()[idx].astype(numpy.float64)
+    gn = g.cpu().numpy()[idx].astype(numpy.float64)
+    ref = wr.propose_fp8(net.params.cpu().numpy().astype(numpy.float64), dn, gn)
+    _, _, sd = wr.features(dn, gn)
+    e8 = numpy.abs(u.cpu().numpy()[idx] - ref) / sd[:, None, None]
+    assert e8.max() <= 0.1 and e8.mean() <= 1e-4, (e8.max(), e8.mean())

@@ -765,7 +765,9 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                         const float gn = 1.0f - r + v[i];
                         s[i] = un - u[i];
                         y[i] = gn - g[i];
-                        mv += (s[i] != 0.0f) ? 1.0f : 0.0f;
+                        // mv = s's squared norm: zero when no pixel moved (steps below about
+                        // 1e-22, whose squares underflow, count as none)
+                        mv = fmaf(s[i], s[i], mv);
                         u[i] = un;
                         g[i] = gn;
                         sy = fmaf(s[i], y[i], sy);

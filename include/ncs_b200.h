@@ -457,14 +457,16 @@ int ncsb_net_infer_tiles_tc(const float *params, const float *d, const float *ga
                             int64_t n_tiles, float *u0, int32_t *status, void *stream);
 
 /* The three tensor-core inferences above with E4M3 (FP8) operands
- * (tcgen05 kind::f8f6f4, K = 32 per MMA): half the MMAs and half the
- * operand bytes of the BF16 form.  Each output channel's weights are divided
+ * (tcgen05 kind::f8f6f4, K = 32 per MMA; activations stored as three
+ * column-shifted copies so that each layer is 2 M blocks x 9 taps): about
+ * twice the speed of the BF16 form.  Each output channel's weights are divided
  * by (its largest |w|) / 448 before rounding, the network's input features
  * are multiplied by 8 and the hidden activations by 4 (exact powers of two;
  * values beyond E4M3's range saturate at +-448), and the epilogue undoes
  * both scales in FP32.  Proposals differ from the FP32 network's by about
- * 0.1-0.2 of the tile's scale s at most; the solve from them is unchanged
- * in its stopping rule and fallback, and takes about the same iterations. */
+ * 0.03-0.05 of the tile's scale s on average (single pixels up to about s);
+ * the solve from them is unchanged in its stopping rule and fallback, and
+ * takes the same iterations. */
 int ncsb_net_infer_stack_tc_fp8(const float *params, const float *images, int n_frames,
                                 int height, int width, const float *gamma, int gamma_per_frame,
                                 float *u0_tiles, int32_t *status, void *stream);

@@ -128,3 +128,41 @@ def test_fp8_many_tiles_per_slot(ws):
     _, _, sd = wr.features(dn, gn)
     e8 = numpy.abs(u.cpu().numpy()[idx] - ref) / sd[:, None, None]
     assert e8.max() <= 0.1 and e8.mean() <= 1e-4, (e8.max(), e8.mean())
+
+
+def test_fp8_saturating_inputs_stay_finite_and_feasible(ws):
+    """Tiles far outside the training range (a hot pixel at 1e5 photons, a
+    near-empty tile, a huge gamma, a tile of 1e4..5e4 photons) push features
+    and activations beyond E4M3's range: the kernel saturates them as the
+    oracle's restatement does, the proposals stay finite and feasible, and the
+    solve from them ends at the photon-image solve's cost."""
+    import ncs_b200
+    from oracle import numpy_ref as nr
+    rng = numpy.random.default_rng(21)
+    d = rng.uniform(5.0, 30.0, size=(6, 16, 16)).astype(numpy.float32)
+    g = rng.exponential(10.0, size=(6, 16, 16)).astype(numpy.float32)
+    d[0, 7, 7] = 1.0e5                                 # one hot pixel
+    d[1] = 1.0e-6                                      # an empty tile
+    g[2] *= 1.0e4                                      # a huge read-noise variance
+    d[3] = rng.uniform(1.0e4, 5.0e4, size=(16, 16))    # a tile of bright pixels
+    net = ws.WarmStartNet.load()
+    dt, gt = torch.from_numpy(d).cuda(), torch.from_numpy(g).cuda()
+    u0, st = net.propose_tiles_tc(dt, gt, fp8=True)
+    assert int(st.item()) == 0
+    u = u0.cpu().numpy().astype(numpy.float64)
+    dd, gg = d.astype(numpy.float64), g.astype(numpy.float64)
+    assert numpy.isfinite(u).all()
+    floor = wr.START_FRAC * numpy.maximum(dd + gg, 1e-3)
+    assert (u + gg >= floor * (1.0 - 1e-5) - 1e-6 * (1.0 + gg)).all()
+    ref = wr.propose_fp8(net.params.cpu().numpy().astype(numpy.float64), dd, gg)
+    _, _, sd = wr.features(dd, gg)
+    assert (numpy.abs(u - ref) / sd[:, None, None]).mean() <= 1e-3
+    mask = numpy.fft.fftshift(numpy.full((16, 16), 0.5))
+    s = ncs_b200.Solver(alpha=0.2)
+    s.set_otf_mask(mask)
+    u_cold, _, _, _ = s.solve_tiles(dt, gt)
+    u_warm, _, _, _ = s.solve_tiles(dt, gt, u0=u0)
+    ms = numpy.fft.ifftshift(mask)
+    f_cold = nr.cost(u_cold.cpu().numpy().astype(numpy.float64), dd, gg, ms, 0.2)
+    f_warm = nr.cost(u_warm.cpu().numpy().astype(numpy.float64), dd, gg, ms, 0.2)
+    assert (numpy.abs(f_warm - f_cold) / numpy.maximum(numpy.abs(f_cold), 1.0) <= 1e-5).all()

@@ -1188,32 +1188,41 @@ __global__ void __launch_bounds__(w16::kThreadsW)
                 const float4* sc4 = reinterpret_cast<const float4*>(sScale + 32 * ly);
                 const float4* b4 = reinterpret_cast<const float4*>(sBias + 32 * ly);
                 unsigned char* cp = sm + kOffCopies + sl * kSlotBytes;
+                // both blocks' accumulator rows (pixels tg and 128 + tg), each
+                // scale and bias loaded once for the two
+                uint32_t ra[32], rb[32];
+                tmem_ld32_issue(td, ra);
+                tmem_ld32_issue(td + 32, rb);
+                tmem_wait32(ra);
+                after_wait32(rb);
+                uint4 wa[2], wb[2];
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    uint32_t qa[4], qb[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int i0 = 16 * kk + 4 * j;
+                        const float4 sv = sc4[i0 >> 2], o = b4[i0 >> 2];
+                        qa[j] = __byte_perm(
+                            relu_e4m3x2(fmaf(__uint_as_float(ra[i0]), sv.x, o.x),
+                                        fmaf(__uint_as_float(ra[i0 + 1]), sv.y, o.y)),
+                            relu_e4m3x2(fmaf(__uint_as_float(ra[i0 + 2]), sv.z, o.z),
+                                        fmaf(__uint_as_float(ra[i0 + 3]), sv.w, o.w)),
+                            0x5410);
+                        qb[j] = __byte_perm(
+                            relu_e4m3x2(fmaf(__uint_as_float(rb[i0]), sv.x, o.x),
+                                        fmaf(__uint_as_float(rb[i0 + 1]), sv.y, o.y)),
+                            relu_e4m3x2(fmaf(__uint_as_float(rb[i0 + 2]), sv.z, o.z),
+                                        fmaf(__uint_as_float(rb[i0 + 3]), sv.w, o.w)),
+                            0x5410);
+                    }
+                    wa[kk] = make_uint4(qa[0], qa[1], qa[2], qa[3]);
+                    wb[kk] = make_uint4(qb[0], qb[1], qb[2], qb[3]);
+                }
                 // pixel p's activations into the three copies: copy 1 at (r, c),
                 // copy 0 at (r, c + 1), copy 2 at (r, c - 1) where inside the tile
-#pragma unroll 1
-                for (int b = 0; b < 2; ++b) {
-                    uint32_t r32[32];
-                    tmem_ld32_issue(td + 32 * b, r32);
-                    tmem_wait32(r32);
-                    const int p = 128 * b + tg, r = p >> 4, c = p & 15;
-                    uint4 w[2];
-#pragma unroll
-                    for (int kk = 0; kk < 2; ++kk) {
-                        uint32_t q[4];
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int i0 = 16 * kk + 4 * j;
-                            const float4 s = sc4[i0 >> 2], o = b4[i0 >> 2];
-                            q[j] = __byte_perm(
-                                relu_e4m3x2(fmaf(__uint_as_float(r32[i0]), s.x, o.x),
-                                            fmaf(__uint_as_float(r32[i0 + 1]), s.y, o.y)),
-                                relu_e4m3x2(fmaf(__uint_as_float(r32[i0 + 2]), s.z, o.z),
-                                            fmaf(__uint_as_float(r32[i0 + 3]), s.w, o.w)),
-                                0x5410);
-                        }
-                        w[kk] = make_uint4(q[0], q[1], q[2], q[3]);
-                    }
-                    const int pos = (r + 1) * 16 + c;
+                auto put = [&](int p, const uint4 (&w)[2]) {
+                    const int r = p >> 4, c = p & 15, pos = (r + 1) * 16 + c;
 #pragma unroll
                     for (int kk = 0; kk < 2; ++kk) {
                         *reinterpret_cast<uint4*>(cp + kCopyBytes + kk * kChunk + pos * 16) = w[kk];
@@ -1223,7 +1232,9 @@ __global__ void __launch_bounds__(w16::kThreadsW)
                             *reinterpret_cast<uint4*>(cp + 2 * kCopyBytes + kk * kChunk +
                                                       (pos - 1) * 16) = w[kk];
                     }
-                }
+                };
+                put(tg, wa);
+                put(128 + tg, wb);
             } else {
                 // the one output channel: column 0 of both blocks
                 const float* sD = reinterpret_cast<const float*>(sm + kOffTile + sl * 2048);

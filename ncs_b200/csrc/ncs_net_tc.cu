@@ -1158,7 +1158,7 @@ __global__ void __launch_bounds__(w16::kThreadsW)
 #pragma unroll
             for (int b = 0; b < 2; ++b) {
                 const int p = 128 * b + tg, r = p >> 4, c = p & 15;
-                float v[32];
+                float v[18];
 #pragma unroll
                 for (int tap = 0; tap < 9; ++tap) {
                     // pixel (r + ky - 1, c + kx - 1) on the plane: index + 1
@@ -1166,9 +1166,17 @@ __global__ void __launch_bounds__(w16::kThreadsW)
                     v[2 * tap] = x.x;
                     v[2 * tap + 1] = x.y;
                 }
+                // K = 18 values, E4M3, in the two 16-byte chunks of the row;
+                // the padding to K = 32 is zero
+                uint32_t q[5];
 #pragma unroll
-                for (int kk = 18; kk < 32; ++kk) v[kk] = 0.0f;
-                store_pos<true>(c1, kChunk, (r + 1) * 16 + c, v);
+                for (int j = 0; j < 4; ++j)
+                    q[j] = __byte_perm(pack2_f8(v[4 * j], v[4 * j + 1]),
+                                       pack2_f8(v[4 * j + 2], v[4 * j + 3]), 0x5410);
+                q[4] = pack2_f8(v[16], v[17]);
+                const int pos = (r + 1) * 16 + c;
+                *reinterpret_cast<uint4*>(c1 + pos * 16) = make_uint4(q[0], q[1], q[2], q[3]);
+                *reinterpret_cast<uint4*>(c1 + kChunk + pos * 16) = make_uint4(q[4], 0u, 0u, 0u);
             }
         };
 

@@ -29,9 +29,11 @@
 // and the solves from them take the same iterations.
 //
 // In both, the first layer (2 input channels) is one GEMM per block with an
-// im2col operand, K = 18 taps x channels padded to 32, and the last layer
-// (one output channel) is one GEMM per block with the 9 taps as the N = 16
-// columns: per-tap partial sums, added over the taps' shifts in the epilogue.
+// im2col operand, K = 18 taps x channels padded to 32.  The last layer (one
+// output channel) is, in the BF16 kernel, one GEMM per block with the 9 taps
+// as the N = 16 columns (per-tap partial sums, added over the taps' shifts in
+// the epilogue), and in the E4M3 kernel a tap convolution like the hidden
+// layers with its output zero-padded to N = 16.
 //
 // Shared-memory operands are K-major without swizzle: 8 consecutive
 // positions x 16 bytes (8 BF16 or 16 E4M3 channels) form a core matrix, so an
@@ -922,13 +924,14 @@ __global__ void __launch_bounds__(kCtaThreads)
 // (zero outside the tile) on 16-wide rows with a zero row above and below
 // (18 x 16 positions, [chunk][position][16 B]).  Tap (ky, kx) of the 128
 // pixels of block b (rows 8b .. 8b + 7) is then the window of copy kx that
-// starts at row 8b + ky: 2 M blocks per layer cover exactly the 256 pixels,
-// a slot needs 64 tensor-memory columns, so a CTA holds six slots, two per
-// epilogue warpgroup.  The epilogue
-// writes each value three times (the copies' zero columns and rows are
-// never written and stay zero).  The layer-1 im2col operand lives in copy 1's
-// interior; layer 4 (one output channel, zero-padded to N = 16) runs like the
-// hidden layers, 18 more MMAs that leave the epilogue a single column.
+// starts at row 8b + ky: 2 M blocks per layer cover exactly the 256 pixels
+// (2 MMAs for layer 1, 18 for each of layers 2-4: 56 per tile), and a slot
+// needs 64 tensor-memory columns, so a CTA holds six slots, two per epilogue
+// warpgroup.  The epilogue writes each value three times (the copies' zero
+// columns and rows are never written and stay zero).  The layer-1 im2col
+// operand lives in copy 1's interior; layer 4 (one output channel, zero-
+// padded to N = 16) runs like the hidden layers and leaves the epilogue a
+// single column to read.
 namespace w16 {
 constexpr int kGroups = 3;                     // epilogue warpgroups, each with an MMA warp
 constexpr int kThreadsW = 160 * kGroups;

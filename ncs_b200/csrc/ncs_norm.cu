@@ -10,8 +10,10 @@
 // One thread per pixel: 9 unknowns, FP64 iterate, gradient and costs (the
 // cost is a sum of terms of order 100 whose differences near convergence are
 // of order 1e-5), BFGS with a dense 9 x 9 inverse-Hessian approximation kept
-// in shared memory (45 packed FP64 entries per thread), backtracking Armijo
-// line search with the fraction-to-barrier rule of the main solver.  The
+// in shared memory (45 packed FP32 entries per thread; the direction and the
+// update in FP32 as the main solver's L-BFGS, the update's scalars in FP64),
+// backtracking Armijo line search on the FP64 cost with the fraction-to-
+// barrier rule of the main solver.  The
 // reference minimises with MATLAB's fminunc quasi-Newton; the stopping rule
 // here is fminunc's first-order optimality test, ||g||_inf <= tol *
 // max(1, ||g_0||_inf), with its iteration cap.  Q (9 x 9, symmetric) is the
@@ -27,9 +29,8 @@
 namespace ncsb {
 namespace norm {
 
-// 64 threads: the FP64 inverse Hessians (45 x 8 B a thread) and segment
-// constants fit the 48 KB of static shared memory, and at 255 registers a
-// thread the SM holds 4 such blocks either way
+// 64 threads a block: the inverse Hessians (45 x 4 B a thread) and segment
+// constants take 20 KB of static shared memory
 constexpr int kThreads = 64;
 constexpr int kPacked = 45;  // upper triangle of a symmetric 9 x 9
 
@@ -97,7 +98,7 @@ __device__ double evaluate(const Args& a, const double (&u)[9], const Seg& sg, d
 }
 
 __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
-    __shared__ double Hm[kPacked][kThreads];  // inverse-Hessian approximation, per thread
+    __shared__ float Hm[kPacked][kThreads];  // inverse-Hessian approximation, per thread
     __shared__ double Cs[9][kThreads], Gs[9][kThreads];
     const long long HW = (long long)a.H * a.W;
     const long long idx = (long long)blockIdx.x * kThreads + threadIdx.x;
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
 #pragma unroll
     for (int i = 0; i < 9; ++i)
 #pragma unroll
-        for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0 : 0.0;
+        for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0f : 0.0f;
 
     double fu = evaluate(a, u, sg, g, true);
     double g0 = 0.0;
@@ -139,27 +140,33 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
 #pragma unroll
         for (int i = 0; i < 9; ++i) gmax = fmax(gmax, fabs(g[i]));
         if (gmax <= a.tol * fmax(1.0, g0)) { status = NCSB_SUCCESS; break; }
-        // direction p = -H g
-        double d[9], gd = 0.0;
+        // direction p = -H g (FP32), its slope g'p in FP64
+        float d[9];
+        double gd = 0.0;
+        {
+            float gf[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            double acc = 0.0;
+            for (int j = 0; j < 9; ++j) gf[j] = (float)g[j];
 #pragma unroll
-            for (int j = 0; j < 9; ++j)
-                acc = fma(Hm[i <= j ? pk(i, j) : pk(j, i)][t], g[j], acc);
-            d[i] = -acc;
-            gd = fma(g[i], d[i], gd);
+            for (int i = 0; i < 9; ++i) {
+                float acc = 0.0f;
+#pragma unroll
+                for (int j = 0; j < 9; ++j)
+                    acc = fmaf(Hm[i <= j ? pk(i, j) : pk(j, i)][t], gf[j], acc);
+                d[i] = -acc;
+                gd = fma(g[i], (double)d[i], gd);
+            }
         }
         if (!(gd < 0.0)) {  // lost positive definiteness: restart from steepest descent
 #pragma unroll
             for (int i = 0; i < 9; ++i)
 #pragma unroll
-                for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0 : 0.0;
+                for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0f : 0.0f;
             gd = 0.0;
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
-                d[i] = -g[i];
-                gd = fma(g[i], d[i], gd);
+                d[i] = -(float)g[i];
+                gd = fma(g[i], (double)d[i], gd);
             }
         }
         // backtracking Armijo; trials keep u + gamma >= 1% of its value
@@ -169,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
             bool feas = true;
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
-                un[i] = fma(step, d[i], u[i]);
+                un[i] = fma(step, (double)d[i], u[i]);
                 feas = feas && (un[i] + sg.G(i) >= 0.01 * (u[i] + sg.G(i)));
             }
             if (feas) {
@@ -182,38 +189,51 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
             if (!(step >= a.min_step)) break;
         }
         if (!ok) { status = NCSB_MINIMUM_STEP; break; }
-        // BFGS update of the inverse Hessian with s = un - u, y = gn - g
-        double s[9], yv[9], sy = 0.0, yy = 0.0;
+        // BFGS update of the inverse Hessian with s = un - u, y = gn - g:
+        // H <- H - rho (v s' + s v') + (rho^2 y'Hy + rho) s s', v = H y.  The
+        // differences and the scalars in FP64, the 45 entries in FP32 from
+        // pre-scaled vectors (no FP32 product of rho or rho^2 alone).
+        float s[9], yv[9];
+        double sy = 0.0, yy = 0.0;
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
-            s[i] = un[i] - u[i];
-            yv[i] = gn[i] - g[i];
-            sy = fma(s[i], yv[i], sy);
-            yy = fma(yv[i], yv[i], yy);
+            const double sd = un[i] - u[i], yd = gn[i] - g[i];
+            s[i] = (float)sd;
+            yv[i] = (float)yd;
+            sy = fma(sd, yd, sy);
+            yy = fma(yd, yd, yy);
         }
         if (sy > 1e-300) {
             if (it == 0) {  // scale the identity before the first update
-                const double sc = sy / yy;
+                const float sc = (float)(sy / yy);
 #pragma unroll
                 for (int i = 0; i < 9; ++i) Hm[pk(i, i)][t] = sc;
             }
-            double v[9], yHy = 0.0;
+            float v[9];
+            double yHy = 0.0;
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
-                double acc = 0.0;
+                float acc = 0.0f;
 #pragma unroll
                 for (int j = 0; j < 9; ++j)
-                    acc = fma(Hm[i <= j ? pk(i, j) : pk(j, i)][t], yv[j], acc);
+                    acc = fmaf(Hm[i <= j ? pk(i, j) : pk(j, i)][t], yv[j], acc);
                 v[i] = acc;
-                yHy = fma(yv[i], acc, yHy);
+                yHy = fma((double)yv[i], (double)acc, yHy);
             }
             const double rho = 1.0 / sy, k2 = rho * rho * yHy + rho;
+            float rv[9], ks[9];  // rho v and (rho^2 y'Hy + rho) s
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                rv[i] = (float)(rho * (double)v[i]);
+                ks[i] = (float)(k2 * (double)s[i]);
+            }
 #pragma unroll
             for (int i = 0; i < 9; ++i)
 #pragma unroll
                 for (int j = i; j < 9; ++j) {
-                    const double h = Hm[pk(i, j)][t];
-                    Hm[pk(i, j)][t] = h - rho * (v[i] * s[j] + s[i] * v[j]) + k2 * s[i] * s[j];
+                    const float h = Hm[pk(i, j)][t];
+                    Hm[pk(i, j)][t] =
+                        fmaf(ks[i], s[j], fmaf(-rv[i], s[j], fmaf(-s[i], rv[j], h)));
                 }
         }
         bool moved = false;

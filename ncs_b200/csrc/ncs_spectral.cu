@@ -131,7 +131,10 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
         }
 
         // ---- gather the tile (segmentation, ncs.c:66-113) ---------------------
-        float d[8], gam[8], u[8];
+        // Pixel pairs: element j of a float2[4] holds rows P and P + 8 at column
+        // Qd + 4j, the packing of the transforms' complex rows, so that the
+        // per-pixel updates run as packed FP32 pairs.
+        float d[8], gam[8], u0[8];
         int f = 0, ox = 0, oy = 0, own_r = 0, own_c = 0;
         if (a.tile_mode) {
             const long long base = tile * kPix;
@@ -142,7 +145,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     const int off = (G.P + 8 * s) * kTile + G.Qd + 4 * j;
                     d[2 * j + s] = __ldg(a.data + base + off);
                     gam[2 * j + s] = __ldg(a.gamma + base + off);
-                    u[2 * j + s] = Warm ? __ldg(a.u0 + base + off) : d[2 * j + s];
+                    u0[2 * j + s] = Warm ? __ldg(a.u0 + base + off) : d[2 * j + s];
                 }
         } else {
             const Geo sg = geo_of<Batch>(a, sdesc[wid]);
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     const int col = clampi(oy + G.Qd + 4 * j - 1, 0, sg.W - 1);
                     d[2 * j + s] = __ldg(img + row * sg.W + col);
                     gam[2 * j + s] = __ldg(gmap + row * sg.W + col);
-                    u[2 * j + s] = d[2 * j + s];
+                    u0[2 * j + s] = d[2 * j + s];
                 }
             }
             if (Warm) {
@@ -173,41 +176,46 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 for (int j = 0; j < 4; ++j)
 #pragma unroll
                     for (int s = 0; s < 2; ++s)
-                        u[2 * j + s] = __ldg(ut + (G.P + 8 * s) * kTile + G.Qd + 4 * j);
+                        u0[2 * j + s] = __ldg(ut + (G.P + 8 * s) * kTile + G.Qd + 4 * j);
             }
         }
+        float2 u[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) u[j] = make_float2(u0[2 * j], u0[2 * j + 1]);
         // the photon image again, for the start passes of a proposed start
         // (re-read rather than kept in registers through the solve)
-        auto load_d = [&](float (&dst)[8]) {
+        auto load_d = [&](float2 (&dst)[4]) {
             if (a.tile_mode) {
                 const float* dt = a.data + tile * kPix;
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-#pragma unroll
-                    for (int s = 0; s < 2; ++s)
-                        dst[2 * j + s] = __ldg(dt + (G.P + 8 * s) * kTile + G.Qd + 4 * j);
+                    dst[j] = make_float2(__ldg(dt + G.P * kTile + G.Qd + 4 * j),
+                                         __ldg(dt + (G.P + 8) * kTile + G.Qd + 4 * j));
             } else {
                 const Geo sg = geo_of<Batch>(a, sdesc[wid]);
                 const float* img = sg.data + (long long)f * sg.H * sg.W;
+                const long long r0 = clampi(ox + G.P - 1, 0, sg.H - 1);
+                const long long r1 = clampi(ox + G.P + 7, 0, sg.H - 1);
 #pragma unroll
-                for (int s = 0; s < 2; ++s) {
-                    const long long row = clampi(ox + G.P + 8 * s - 1, 0, sg.H - 1);
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        dst[2 * j + s] =
-                            __ldg(img + row * sg.W + clampi(oy + G.Qd + 4 * j - 1, 0, sg.W - 1));
+                for (int j = 0; j < 4; ++j) {
+                    const int col = clampi(oy + G.Qd + 4 * j - 1, 0, sg.W - 1);
+                    dst[j] = make_float2(__ldg(img + r0 * sg.W + col), __ldg(img + r1 * sg.W + col));
                 }
             }
         };
         __syncwarp();  // the previous tile's terms are no longer read
-        store_terms(terms, lane, d, gam);
+        store_terms_neg(terms, lane, d, gam);
         __syncwarp();
 
         // ---- preconditioned L-BFGS ---------------------------------------------
         // Pass 0 transforms u (v = 2 alpha Q u, initial gradient); later passes
-        // transform the two-loop vector q.  One call site for each FFT half.
-        // v = 2 alpha Q u and w = 2 alpha Q p carry the factor 2 alpha.
-        float v[8], g[8], p[8], w[8];
+        // transform the two-loop vector.  One call site for each FFT half.
+        // v = 2 alpha Q u carries the factor 2 alpha.  Signs chosen so that the
+        // packed updates need no negation: the transformed vector is nq = -q =
+        // g + sum a_i y_i (its spectral weights are negated instead), and the
+        // solver keeps wn = -w = -2 alpha Q p and the history -Q s; the pixel
+        // terms are read as -c (load_terms_neg).
+        float2 v[4], g[4], p[4], wn[4];
         float rho[MaxM], al[MaxM];
         // s'g of the newest pair at the gradient it was stored with: the first
         // two-loop dot of the next iteration, s'(-g), without a reduction
@@ -222,46 +230,47 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 
         for (;;) {
             if (!first && iters >= a.max_iters) { status = kReachedMaxIters; break; }
-            float q[8];
+            float2 nq[4];
             if (first) {
                 if (start_pass == 1) {
-                    load_d(q);
+                    load_d(nq);
                 } else {
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) q[i] = u[i];
+                    for (int j = 0; j < 4; ++j) nq[j] = u[j];
                 }
             } else {
-                // two-loop, first half (newest pair first)
+                // two-loop, first half (newest pair first), on nq = -q
 #pragma unroll
-                for (int i = 0; i < 8; ++i) q[i] = -g[i];
+                for (int j = 0; j < 4; ++j) nq[j] = g[j];
 #pragma unroll
                 for (int i = 0; i < MaxM; ++i) {
                     if (i < k) {
                         int slot = newest - i;
                         if (slot < 0) slot += mcap;
-                        float hv[8];
-                        float dot;
+                        float2 hv[4];
+                        float dot;  // s'q
                         if (i == 0 && sg_fresh) {
                             dot = -sg_newest;  // q = -g here
                         } else {
                             load_hist(hs + slot * 64, lane, hv);
-                            float acc = 0.0f;
+                            float2 acc = hv[0] * nq[0];
 #pragma unroll
-                            for (int e = 0; e < 8; ++e) acc = fmaf(hv[e], q[e], acc);
-                            dot = warp_sum_f(acc);
+                            for (int e = 1; e < 4; ++e) acc = fma2(hv[e], nq[e], acc);
+                            dot = -warp_sum_f(acc.x + acc.y);
                         }
                         const float ai = rho[i] * dot;
                         al[i] = ai;
                         load_hist(hy + slot * 64, lane, hv);
+                        const float2 a2 = splat(ai);
 #pragma unroll
-                        for (int e = 0; e < 8; ++e) q[e] = fmaf(-ai, hv[e], q[e]);
+                        for (int e = 0; e < 4; ++e) nq[e] = fma2(a2, hv[e], nq[e]);
                     }
                 }
             }
             // spectral step: p = H0 q (pass 0: 2 alpha Q u) by one forward and
             // one inverse transform; the weights are real and symmetric in k.
             float2 spec[8];
-            warp_fft_fwd<false>(q, spec, ws, with_twiddles(G, s_tw));  // 2 F q: the weights hold the 1/2
+            warp_fft_fwd<false>(nq, spec, ws, with_twiddles(G, s_tw));  // 2 F nq: the weights hold the 1/2
             float mk[8];
             {
                 const float4 m0 = Batch ? __ldg(mkp) : mkp[0];
@@ -271,20 +280,21 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             }
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                // (1/512) / (lam + 512 alpha mk) = 1 / (512 lam + 512^2 alpha mk): the
-                // power-of-two factor moves inside exactly
+                // -(1/512) / (lam + 512 alpha mk) = 1 / (-512 lam - 512^2 alpha mk): the
+                // power-of-two factor moves inside exactly; the sign turns nq into q
                 const float wgt = first ? alpha * mk[i]
-                                        : rcp_fast(fmaf(512.0f * two_alpha_256, mk[i], 512.0f * lam));
+                                        : rcp_fast(fmaf(-512.0f * two_alpha_256, mk[i], -512.0f * lam));
                 spec[i] = make_float2(spec[i].x * wgt, spec[i].y * wgt);
             }
             warp_fft_inv(spec, p, ws, with_twiddles(G, s_tw));
-            if (!first) {  // w = 2 alpha Q H0 q = q - lambda H0 q
+            if (!first) {  // -w = -2 alpha Q H0 q = lambda H0 q - q
                 if (two_alpha > 0.0f) {
+                    const float2 l2 = splat(lam);
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) w[i] = fmaf(-lam, p[i], q[i]);
+                    for (int j = 0; j < 4; ++j) wn[j] = fma2(l2, p[j], nq[j]);
                 } else {
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) w[i] = 0.0f;
+                    for (int j = 0; j < 4; ++j) wn[j] = make_float2(0.0f, 0.0f);
                 }
             }
             if (first) {
@@ -294,25 +304,30 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     //              >= alpha u0'Q u0 - delta'v0,
                     // so f(u0) - f(d) <= LL(u0) - LL(d) + delta'v0: when that
                     // bound is <= 0 the proposal is accepted at once, without
-                    // transforming d.  Otherwise keep v0 and transform d next
-                    // for the exact comparison.
-                    float dd[8], c[8], gm[8];
+                    // transforming d.  Otherwise keep v0 (in wn) and transform d
+                    // next for the exact comparison.
+                    float2 dd[4], nc[4], gm[4];
                     load_d(dd);
-                    load_terms(terms, lane, c, gm);
+                    load_terms_neg(terms, lane, nc, gm);
                     float dl = 0.0f, dq = 0.0f;
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const float lr = __fsub_rn(__logf(fmaxf(u[i] + gm[i], kFitMin)),
-                                                   __logf(fmaxf(dd[i] + gm[i], kFitMin)));
-                        dl += fmaf(-c[i], lr, u[i] - dd[i]);
-                        dq += __fmul_rn(__fsub_rn(u[i], dd[i]), p[i]);
-                    }
+                    for (int j = 0; j < 4; ++j)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const float ui = h ? u[j].y : u[j].x, di = h ? dd[j].y : dd[j].x;
+                            const float gi = h ? gm[j].y : gm[j].x, ci = h ? nc[j].y : nc[j].x;
+                            const float pi = h ? p[j].y : p[j].x;
+                            const float lr = __fsub_rn(__logf(fmaxf(ui + gi, kFitMin)),
+                                                       __logf(fmaxf(di + gi, kFitMin)));
+                            dl += fmaf(ci, lr, ui - di);
+                            dq += __fmul_rn(__fsub_rn(ui, di), pi);
+                        }
                     const double bound = warp_sum_d((double)dl + (double)dq);
                     if (bound <= 0.0) {
                         start_pass = 0;  // accepted: v = v0 below
                     } else {
 #pragma unroll
-                        for (int i = 0; i < 8; ++i) w[i] = p[i];
+                        for (int j = 0; j < 4; ++j) wn[j] = p[j];
                         start_pass = 1;
                         continue;
                     }
@@ -320,82 +335,90 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 if (start_pass == 1) {
                     // f(u0) - f(d) = sum[(u0 - d) - c (log(u0 + gamma) - log(d + gamma))]
                     //                + alpha (u0'Q u0 - d'Q d);  p = 2 alpha Q d,
-                    //                w = 2 alpha Q u0
-                    float dd[8], c[8], gm[8];
+                    //                wn = 2 alpha Q u0 here
+                    float2 dd[4], nc[4], gm[4];
                     load_d(dd);
-                    load_terms(terms, lane, c, gm);
+                    load_terms_neg(terms, lane, nc, gm);
                     float dl = 0.0f, dq = 0.0f;
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        // explicitly rounded operations: an FMA contraction of
-                        // the two logs' scalings, or of the two products, would
-                        // leave a rounding residue instead of 0 when u0 = d
-                        const float lr = __fsub_rn(__logf(fmaxf(u[i] + gm[i], kFitMin)),
-                                                   __logf(fmaxf(dd[i] + gm[i], kFitMin)));
-                        dl += fmaf(-c[i], lr, u[i] - dd[i]);
-                        dq += __fsub_rn(__fmul_rn(u[i], w[i]), __fmul_rn(dd[i], p[i]));
-                    }
+                    for (int j = 0; j < 4; ++j)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const float ui = h ? u[j].y : u[j].x, di = h ? dd[j].y : dd[j].x;
+                            const float gi = h ? gm[j].y : gm[j].x, ci = h ? nc[j].y : nc[j].x;
+                            const float pi = h ? p[j].y : p[j].x, wi = h ? wn[j].y : wn[j].x;
+                            // explicitly rounded operations: an FMA contraction of
+                            // the two logs' scalings, or of the two products, would
+                            // leave a rounding residue instead of 0 when u0 = d
+                            const float lr = __fsub_rn(__logf(fmaxf(ui + gi, kFitMin)),
+                                                       __logf(fmaxf(di + gi, kFitMin)));
+                            dl += fmaf(ci, lr, ui - di);
+                            dq += __fsub_rn(__fmul_rn(ui, wi), __fmul_rn(di, pi));
+                        }
                     const double delta = warp_sum_d((double)dl + 0.5 * (double)dq);
                     if (delta <= 0.0) {
 #pragma unroll
-                        for (int i = 0; i < 8; ++i) p[i] = w[i];
+                        for (int j = 0; j < 4; ++j) p[j] = wn[j];
                     } else {
                         fell_back = 1;
 #pragma unroll
-                        for (int i = 0; i < 8; ++i) u[i] = dd[i];
+                        for (int j = 0; j < 4; ++j) u[j] = dd[j];
                     }
                     start_pass = 0;
                 }
                 first = false;
-                float c[8], gm[8];
-                load_terms(terms, lane, c, gm);
-                float uu = 0.0f, gg = 0.0f, ll = 0.0f;
+                float2 nc[4], gm[4];
+                load_terms_neg(terms, lane, nc, gm);
+                float2 uu2 = make_float2(0.0f, 0.0f), gg2 = uu2, ll2 = uu2;
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    v[i] = p[i];
-                    const float ia = rcp_fast(fmaxf(u[i] + gm[i], kFitMin));
-                    const float r = c[i] * ia;
-                    g[i] = 1.0f - r + v[i];
-                    uu = fmaf(u[i], u[i], uu);
-                    gg = fmaf(g[i], g[i], gg);
-                    ll = fmaf(r, ia, ll);
+                for (int j = 0; j < 4; ++j) {
+                    v[j] = p[j];
+                    const float2 A = u[j] + gm[j];
+                    const float2 ia = make_float2(rcp_fast(fmaxf(A.x, kFitMin)), rcp_fast(fmaxf(A.y, kFitMin)));
+                    const float2 r = nc[j] * ia;  // -c / (u + gamma)
+                    g[j] = (r + splat(1.0f)) + v[j];
+                    uu2 = fma2(u[j], u[j], uu2);
+                    gg2 = fma2(g[j], g[j], gg2);
+                    ll2 = fma2(r, ia, ll2);
                 }
-                uu = warp_sum_f(uu);
-                gg = warp_sum_f(gg);
-                lam = warp_sum_f(ll) * (1.0f / 256.0f);
+                const float uu = warp_sum_f(uu2.x + uu2.y);
+                const float gg = warp_sum_f(gg2.x + gg2.y);
+                lam = warp_sum_f(ll2.x + ll2.y) * (-1.0f / 256.0f);
                 if (gg <= eps2 * fmaxf(uu, 1.0f)) { status = kSuccess; break; }
                 continue;
             }
-            // two-loop, second half (oldest pair first): p += coef s, w += coef Q s
+            // two-loop, second half (oldest pair first): p += coef s, wn += coef (-Q s)
 #pragma unroll
             for (int i = MaxM - 1; i >= 0; --i) {
                 if (i < k) {
                     int slot = newest - i;
                     if (slot < 0) slot += mcap;
-                    float hv[8];
+                    float2 hv[4];
                     load_hist(hy + slot * 64, lane, hv);
-                    float acc = 0.0f;
+                    float2 acc = hv[0] * p[0];
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) acc = fmaf(hv[e], p[e], acc);
-                    const float coef = al[i] - rho[i] * warp_sum_f(acc);
+                    for (int e = 1; e < 4; ++e) acc = fma2(hv[e], p[e], acc);
+                    const float2 cf = splat(al[i] - rho[i] * warp_sum_f(acc.x + acc.y));
                     load_hist(hs + slot * 64, lane, hv);
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) p[e] = fmaf(coef, hv[e], p[e]);
+                    for (int e = 0; e < 4; ++e) p[e] = fma2(cf, hv[e], p[e]);
                     load_hist(hq + slot * 64, lane, hv);
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) w[e] = fmaf(coef, hv[e], w[e]);
+                    for (int e = 0; e < 4; ++e) wn[e] = fma2(cf, hv[e], wn[e]);
                 }
             }
 
-            float gp = 0.0f, pv = 0.0f, pw = 0.0f;
+            float2 gp2 = g[0] * p[0], pv2 = p[0] * v[0], pw2 = p[0] * wn[0];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                gp = fmaf(g[i], p[i], gp);
-                pv = fmaf(p[i], v[i], pv);
-                pw = fmaf(p[i], w[i], pw);
+            for (int j = 1; j < 4; ++j) {
+                gp2 = fma2(g[j], p[j], gp2);
+                pv2 = fma2(p[j], v[j], pv2);
+                pw2 = fma2(p[j], wn[j], pw2);
             }
-            double gd = (double)gp, dpv = (double)pv, dpw = (double)pw;
+            double gd = (double)(gp2.x + gp2.y), dpv = (double)(pv2.x + pv2.y),
+                   dpw = (double)(pw2.x + pw2.y);
             warp_sum3_d(gd, dpv, dpw, lane);
+            dpw = -dpw;  // p'w = -p'wn
             if (!(gd < 0.0)) {
                 // not a descent direction: drop the history (H0 alone is positive
                 // definite); fail only if even that does not descend
@@ -410,26 +433,35 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             float t = 1.0f;
             bool ok = false;
             for (int trial = 0; trial < 64; ++trial) {
-                float c[8], gm[8];
-                load_terms(terms, lane, c, gm);
-                float term = 0.0f;
+                float2 nc[4], gm[4];
+                load_terms_neg(terms, lane, nc, gm);
+                const float2 t2 = splat(t);
+                float2 term = make_float2(0.0f, 0.0f);
                 bool cross = false;
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
+                for (int j = 0; j < 4; ++j) {
                     // log(max(ni, F)) - log(max(ai, F)) = log1p((max(ni, F) - A) / A),
                     // A = max(ai, F); above the floor the numerator is the exact
                     // step tp (branch free: one select instead of a branch)
-                    const float ai = u[i] + gm[i];
-                    const float tp = t * p[i];
-                    const float ni = ai + tp;
-                    const bool in_dom = ai >= kFitMin && ni >= kFitMin;
-                    const float A = fmaxf(ai, kFitMin);
-                    const float l = log1p_ls((in_dom ? tp : fmaxf(ni, kFitMin) - A) * rcp_fast(A));
-                    cross |= (ai >= kFitMin) && (ni < kBarrierFrac * ai);
-                    term += fmaf(-c[i], l, tp);
+                    const float2 ai = u[j] + gm[j];
+                    const float2 tp = t2 * p[j];
+                    const float2 ni = ai + tp;
+                    const float2 bar = splat(kBarrierFrac) * ai;
+                    float2 num, rA;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const float a1 = h ? ai.y : ai.x, n1 = h ? ni.y : ni.x;
+                        const bool in_dom = a1 >= kFitMin && n1 >= kFitMin;
+                        const float A = fmaxf(a1, kFitMin);
+                        const float nm = in_dom ? (h ? tp.y : tp.x) : fmaxf(n1, kFitMin) - A;
+                        (h ? num.y : num.x) = nm;
+                        (h ? rA.y : rA.x) = rcp_fast(A);
+                        cross |= (a1 >= kFitMin) && (n1 < (h ? bar.y : bar.x));
+                    }
+                    term = term + fma2(nc[j], log1p_ls(num * rA), tp);
                 }
                 const bool any_cross = __any_sync(kFull, cross);
-                const double dl = warp_sum_d((double)term);
+                const double dl = warp_sum_d((double)(term.x + term.y));
                 ++evals;
                 const double td = (double)t;
                 const double delta = any_cross ? CUDART_INF
@@ -440,33 +472,37 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             }
             if (!ok) { status = kMinimumStep; break; }
 
-            // accept; new pair (s, y, Q s = t w)
-            float s[8], y[8], c[8], gm[8];
-            load_terms(terms, lane, c, gm);
-            float sy = 0.0f, uu = 0.0f, gg = 0.0f, ll = 0.0f, mv = 0.0f, sg = 0.0f;
+            // accept; new pair (s, y, -Q s = t wn)
+            float2 s[4], y[4], nc[4], gm[4];
+            load_terms_neg(terms, lane, nc, gm);
+            const float2 t2 = splat(t), z2 = make_float2(0.0f, 0.0f);
+            float2 sy2 = z2, uu2 = z2, gg2 = z2, ll2 = z2, mv2 = z2, sg2 = z2;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const float un = fmaf(t, p[i], u[i]);
-                w[i] *= t;
-                v[i] += w[i];
-                const float ia = rcp_fast(fmaxf(un + gm[i], kFitMin));
-                const float r = c[i] * ia;
-                const float gn = 1.0f - r + v[i];
-                s[i] = un - u[i];
-                y[i] = gn - g[i];
+            for (int j = 0; j < 4; ++j) {
+                const float2 un = fma2(t2, p[j], u[j]);
+                wn[j] = wn[j] * t2;
+                v[j] = v[j] - wn[j];  // v += t w
+                const float2 A = un + gm[j];
+                const float2 ia = make_float2(rcp_fast(fmaxf(A.x, kFitMin)), rcp_fast(fmaxf(A.y, kFitMin)));
+                const float2 r = nc[j] * ia;  // -c / (u + gamma)
+                const float2 gn = (r + splat(1.0f)) + v[j];
+                s[j] = un - u[j];
+                y[j] = gn - g[j];
                 // mv = s's squared norm: zero when no pixel moved (steps below about
                 // 1e-22, whose squares underflow, count as none)
-                mv = fmaf(s[i], s[i], mv);
-                u[i] = un;
-                g[i] = gn;
-                sy = fmaf(s[i], y[i], sy);
-                sg = fmaf(s[i], gn, sg);
-                uu = fmaf(un, un, uu);
-                gg = fmaf(gn, gn, gg);
-                ll = fmaf(r, ia, ll);
+                mv2 = fma2(s[j], s[j], mv2);
+                u[j] = un;
+                g[j] = gn;
+                sy2 = fma2(s[j], y[j], sy2);
+                sg2 = fma2(s[j], gn, sg2);
+                uu2 = fma2(un, un, uu2);
+                gg2 = fma2(gn, gn, gg2);
+                ll2 = fma2(r, ia, ll2);
             }
+            float sy, uu, gg, ll, mv, sg;
             {
-                float vals[8] = {sy, uu, gg, ll, mv, sg};
+                float vals[8] = {sy2.x + sy2.y, uu2.x + uu2.y, gg2.x + gg2.y,
+                                 ll2.x + ll2.y, mv2.x + mv2.y, sg2.x + sg2.y};
                 const float tot = warp_transpose_sum<8>(vals, lane);
                 sy = __shfl_sync(kFull, tot, 0);
                 uu = __shfl_sync(kFull, tot, 1);
@@ -476,7 +512,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 sg = __shfl_sync(kFull, tot, 5);
             }
             ++iters;
-            lam = ll * (1.0f / 256.0f);
+            lam = ll * (-1.0f / 256.0f);
             if (gg <= eps2 * fmaxf(uu, 1.0f)) { status = kSuccess; break; }
             if (mv == 0.0f) { status = kReachedMaxPrecision; break; }
             sg_fresh = sy > 0.0f;
@@ -485,7 +521,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 newest = newest + 1 == mcap ? 0 : newest + 1;
                 store_hist(hs + newest * 64, lane, s);
                 store_hist(hy + newest * 64, lane, y);
-                store_hist(hq + newest * 64, lane, w);
+                store_hist(hq + newest * 64, lane, wn);
 #pragma unroll
                 for (int i = MaxM - 1; i > 0; --i) rho[i] = rho[i - 1];
                 rho[0] = rcp_fast(sy);
@@ -495,14 +531,17 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 
         // ---- outputs -----------------------------------------------------------
         if (a.cost) {
-            float c[8], gm[8];
-            load_terms(terms, lane, c, gm);
+            float2 nc[4], gm[4];
+            load_terms_neg(terms, lane, nc, gm);
             double e0 = 0.0, e1 = 0.0;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                e0 += (double)u[i] - (double)c[i] * log(fmax((double)u[i] + gm[i], 1.0e-6));
-                e1 += (double)u[i] * v[i];
-            }
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const double ui = h ? u[j].y : u[j].x, gi = h ? gm[j].y : gm[j].x;
+                    e0 += ui + (double)(h ? nc[j].y : nc[j].x) * log(fmax(ui + gi, 1.0e-6));
+                    e1 += ui * (h ? v[j].y : v[j].x);
+                }
             e0 = warp_sum_d(e0);
             e1 = warp_sum_d(e1);
             if (lane == 0) a.cost[tile] = e0 + 0.5 * e1;  // v = 2 alpha Q u
@@ -516,10 +555,10 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
         if (a.tile_mode) {
             const long long base = tile * kPix;
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-#pragma unroll
-                for (int s = 0; s < 2; ++s)
-                    a.out[base + (G.P + 8 * s) * kTile + G.Qd + 4 * j] = u[2 * j + s];
+            for (int j = 0; j < 4; ++j) {
+                a.out[base + G.P * kTile + G.Qd + 4 * j] = u[j].x;
+                a.out[base + (G.P + 8) * kTile + G.Qd + 4 * j] = u[j].y;
+            }
         } else {
             const Geo sg = geo_of<Batch>(a, sdesc[wid]);
             float* o = sg.out + (long long)f * sg.H * sg.W;
@@ -531,7 +570,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 for (int s = 0; s < 2; ++s) {
                     const int rr = G.P + 8 * s;
                     if (rr >= 1 && rr <= own_r)
-                        o[(long long)(ox + rr - 1) * sg.W + oy + cc - 1] = u[2 * j + s];
+                        o[(long long)(ox + rr - 1) * sg.W + oy + cc - 1] = s ? u[j].y : u[j].x;
                 }
             }
         }

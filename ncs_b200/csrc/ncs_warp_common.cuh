@@ -35,10 +35,22 @@ __device__ __forceinline__ int bitrev3(int i) {
     return ((i & 1) << 2) | (i & 2) | ((i & 4) >> 2);
 }
 
-__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Packed FP32 pairs: sm_100's FADD2 / FMUL2 / FFMA2 issue both components as
+// one instruction, each rounded as its scalar operation.  Complex values and
+// the warp solvers' pixel pairs are such pairs.  Products with i swap the
+// components, so the butterflies that take one (add_ib, sub_ib) stay scalar.
+__device__ __forceinline__ float2 splat(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b exactly: the product b (-1) is exact and the sum rounds once
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 mul_i(float2 a) { return make_float2(-a.y, a.x); }      // i a
 __device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }     // -i a
+__device__ __forceinline__ float2 add_ib(float2 a, float2 b) { return make_float2(a.x - b.y, a.y + b.x); }  // a + i b
+__device__ __forceinline__ float2 sub_ib(float2 a, float2 b) { return make_float2(a.x + b.y, a.y - b.x); }  // a - i b
 __device__ __forceinline__ float2 conjmul(float2 a, float2 w) {                            // a conj(w)
     return make_float2(fmaf(a.x, w.x, a.y * w.y), fmaf(a.y, w.x, -a.x * w.y));
 }
@@ -56,65 +68,52 @@ __device__ __forceinline__ float2 w16(int p) {
 }
 
 // In-place 8-point DFT, decimation in frequency: natural order in, output
-// position i holds frequency bitrev3(i).  Unnormalised.
+// position i holds frequency bitrev3(i).  Unnormalised.  The butterflies
+// whose partner carries a factor -i are written as sub_ib / add_ib.
 __device__ __forceinline__ void fft8_fwd(float2 (&e)[8]) {
+    float2 a[4], b[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const float2 a = e[r] + e[r + 4], b = e[r] - e[r + 4];
-        e[r] = a;
-        if (r == 0) e[r + 4] = b;
-        else if (r == 1) e[r + 4] = make_float2(kS2 * (b.x + b.y), kS2 * (b.y - b.x));
-        else if (r == 2) e[r + 4] = mul_mi(b);
-        else e[r + 4] = make_float2(kS2 * (b.y - b.x), -kS2 * (b.x + b.y));
+        a[r] = e[r] + e[r + 4];
+        b[r] = e[r] - e[r + 4];
     }
-#pragma unroll
-    for (int base = 0; base < 8; base += 4) {
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const float2 a = e[base + r] + e[base + r + 2], b = e[base + r] - e[base + r + 2];
-            e[base + r] = a;
-            e[base + r + 2] = r == 0 ? b : mul_mi(b);
-        }
-    }
-#pragma unroll
-    for (int base = 0; base < 8; base += 2) {
-        const float2 a = e[base] + e[base + 1], b = e[base] - e[base + 1];
-        e[base] = a;
-        e[base + 1] = b;
-    }
+    // twiddles W8^1 and W8^3 (W8^2 = -i is taken by the butterflies below)
+    const float2 t1 = make_float2(kS2 * (b[1].x + b[1].y), kS2 * (b[1].y - b[1].x));
+    const float2 t3 = make_float2(kS2 * (b[3].y - b[3].x), -kS2 * (b[3].x + b[3].y));
+    const float2 A0 = a[0] + a[2], A2 = a[0] - a[2], A1 = a[1] + a[3], A3 = a[1] - a[3];
+    const float2 B0 = sub_ib(b[0], b[2]), B2 = add_ib(b[0], b[2]), B1 = t1 + t3, B3 = t1 - t3;
+    e[0] = A0 + A1;
+    e[1] = A0 - A1;
+    e[2] = sub_ib(A2, A3);
+    e[3] = add_ib(A2, A3);
+    e[4] = B0 + B1;
+    e[5] = B0 - B1;
+    e[6] = sub_ib(B2, B3);
+    e[7] = add_ib(B2, B3);
 }
 
 // Inverse of fft8_fwd up to the factor 8: bit-reversed in, natural out,
 // conjugate twiddles (unnormalised inverse DFT).
 __device__ __forceinline__ void fft8_inv(float2 (&e)[8]) {
+    float2 a[8];
 #pragma unroll
     for (int base = 0; base < 8; base += 2) {
-        const float2 a = e[base], b = e[base + 1];
-        e[base] = a + b;
-        e[base + 1] = a - b;
+        a[base] = e[base] + e[base + 1];
+        a[base + 1] = e[base] - e[base + 1];
     }
-#pragma unroll
-    for (int base = 0; base < 8; base += 4) {
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const float2 t = r == 0 ? e[base + r + 2] : mul_i(e[base + r + 2]);
-            const float2 a = e[base + r];
-            e[base + r] = a + t;
-            e[base + r + 2] = a - t;
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const float2 b = e[r + 4];
-        float2 t;
-        if (r == 0) t = b;
-        else if (r == 1) t = make_float2(kS2 * (b.x - b.y), kS2 * (b.x + b.y));
-        else if (r == 2) t = mul_i(b);
-        else t = make_float2(-kS2 * (b.x + b.y), kS2 * (b.x - b.y));
-        const float2 a = e[r];
-        e[r] = a + t;
-        e[r + 4] = a - t;
-    }
+    const float2 c0 = a[0] + a[2], c2 = a[0] - a[2], c1 = add_ib(a[1], a[3]), c3 = sub_ib(a[1], a[3]);
+    const float2 c4 = a[4] + a[6], c6 = a[4] - a[6], c5 = add_ib(a[5], a[7]), c7 = sub_ib(a[5], a[7]);
+    // conjugate twiddles W8^-1 and W8^-3 (W8^-2 = i is taken by the butterflies)
+    const float2 t1 = make_float2(kS2 * (c5.x - c5.y), kS2 * (c5.x + c5.y));
+    const float2 t3 = make_float2(-kS2 * (c7.x + c7.y), kS2 * (c7.x - c7.y));
+    e[0] = c0 + c4;
+    e[4] = c0 - c4;
+    e[1] = c1 + t1;
+    e[5] = c1 - t1;
+    e[2] = add_ib(c2, c6);
+    e[6] = sub_ib(c2, c6);
+    e[3] = c3 + t3;
+    e[7] = c3 - t3;
 }
 
 struct LaneGeo {
@@ -169,6 +168,19 @@ __device__ __forceinline__ void store_hist(float4* h, int lane, const float (&x)
     h[32 + lane] = make_float4(x[4], x[5], x[6], x[7]);
 }
 
+// The same as pixel pairs z[j] = (row P, row P + 8) at column Qd + 4j.
+__device__ __forceinline__ void load_hist(const float4* h, int lane, float2 (&z)[4]) {
+    const float4 a = h[lane], b = h[32 + lane];
+    z[0] = make_float2(a.x, a.y);
+    z[1] = make_float2(a.z, a.w);
+    z[2] = make_float2(b.x, b.y);
+    z[3] = make_float2(b.z, b.w);
+}
+__device__ __forceinline__ void store_hist(float4* h, int lane, const float2 (&z)[4]) {
+    h[lane] = make_float4(z[0].x, z[0].y, z[1].x, z[1].y);
+    h[32 + lane] = make_float4(z[2].x, z[2].y, z[3].x, z[3].y);
+}
+
 // The pixel terms c = d + gamma and gamma of a lane's 8 pixels, kept in the
 // warp's shared memory as [c low, c high, gamma low, gamma high][lane]
 // float4s (each access is 32 consecutive 16-byte words) and re-read at
@@ -192,6 +204,29 @@ __device__ __forceinline__ void load_terms(const float4* t, int lane, float (&c)
     c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
     gm[0] = g0.x; gm[1] = g0.y; gm[2] = g0.z; gm[3] = g0.w;
     gm[4] = g1.x; gm[5] = g1.y; gm[6] = g1.z; gm[7] = g1.w;
+}
+
+// The spectral solver's form of the pixel terms: -c and gamma as pixel pairs
+// (the same layout), so that its packed updates take -c without negating.
+__device__ __forceinline__ void store_terms_neg(float4* t, int lane, const float (&d)[8],
+                                                const float (&gm)[8]) {
+    t[lane] = make_float4(-(d[0] + gm[0]), -(d[1] + gm[1]), -(d[2] + gm[2]), -(d[3] + gm[3]));
+    t[32 + lane] = make_float4(-(d[4] + gm[4]), -(d[5] + gm[5]), -(d[6] + gm[6]), -(d[7] + gm[7]));
+    t[64 + lane] = make_float4(gm[0], gm[1], gm[2], gm[3]);
+    t[96 + lane] = make_float4(gm[4], gm[5], gm[6], gm[7]);
+}
+__device__ __forceinline__ void load_terms_neg(const float4* t, int lane, float2 (&nc)[4],
+                                               float2 (&gm)[4]) {
+    const float4 c0 = lds_v4_volatile(t + lane), c1 = lds_v4_volatile(t + 32 + lane);
+    const float4 g0 = lds_v4_volatile(t + 64 + lane), g1 = lds_v4_volatile(t + 96 + lane);
+    nc[0] = make_float2(c0.x, c0.y);
+    nc[1] = make_float2(c0.z, c0.w);
+    nc[2] = make_float2(c1.x, c1.y);
+    nc[3] = make_float2(c1.z, c1.w);
+    gm[0] = make_float2(g0.x, g0.y);
+    gm[1] = make_float2(g0.z, g0.w);
+    gm[2] = make_float2(g1.x, g1.y);
+    gm[3] = make_float2(g1.z, g1.w);
 }
 
 // The row-stage twiddles of the four lane classes Qd, for kernels that re-read
@@ -223,34 +258,29 @@ __device__ __forceinline__ LaneGeo with_twiddles(const LaneGeo& g, const Twiddle
 // Forward half of the 16x16 transform: lane (KC = L>>1, H = L&1) ends with
 // the spectrum X[2 bitrev3(i) + H][KC] of its 8 pixels' tile in e[i]
 // (unnormalised; with Halve = false, 2 X, for callers that fold the factor
-// 1/2 of the row-pair separation into a later scaling).  Input: x[2j] = row
-// P, x[2j+1] = row P+8, column Qd + 4j.
+// 1/2 of the row-pair separation into a later scaling).  Input: z[j] = rows
+// P and P + 8 at column Qd + 4j, one complex row value.
 template <bool Halve = true>
-__device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8], WarpSmem& ws,
+__device__ __forceinline__ void warp_fft_fwd(const float2 (&z)[4], float2 (&e)[8], WarpSmem& ws,
                                              const LaneGeo& L) {
     // rows: 4-point DFT over j in the lane, twiddle, 4-point DFT across lanes
     float2 V[4];
     {
-        const float2 z0 = make_float2(x[0], x[1]), z1 = make_float2(x[2], x[3]);
-        const float2 z2 = make_float2(x[4], x[5]), z3 = make_float2(x[6], x[7]);
-        const float2 s02 = z0 + z2, d02 = z0 - z2, s13 = z1 + z3, d13 = z1 - z3;
+        const float2 s02 = z[0] + z[2], d02 = z[0] - z[2], s13 = z[1] + z[3], d13 = z[1] - z[3];
         V[0] = s02 + s13;
         V[2] = cmul(s02 - s13, L.tw2);
-        V[1] = cmul(d02 + mul_mi(d13), L.tw1);
-        V[3] = cmul(d02 + mul_i(d13), L.tw3);
+        V[1] = cmul(sub_ib(d02, d13), L.tw1);
+        V[3] = cmul(add_ib(d02, d13), L.tw3);
     }
     const bool q3 = L.Qd == 3;
+    const float2 sA = splat(L.sA), sB = splat(L.sB);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const float2 p = shfl_xor2(V[k], 2);
-        float2 t = make_float2(fmaf(L.sA, V[k].x, p.x), fmaf(L.sA, V[k].y, p.y));
+        const float2 t = fma2(sA, V[k], shfl_xor2(V[k], 2));
         V[k] = q3 ? mul_mi(t) : t;
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float2 p = shfl_xor2(V[k], 1);
-        V[k] = make_float2(fmaf(L.sB, V[k].x, p.x), fmaf(L.sB, V[k].y, p.y));
-    }
+    for (int k = 0; k < 4; ++k) V[k] = fma2(sB, V[k], shfl_xor2(V[k], 1));
     __syncwarp();  // previous users of the transpose buffer are done
 #pragma unroll
     for (int k = 0; k < 4; ++k) ws.fb[L.P][L.k0 + k] = V[k];
@@ -263,15 +293,24 @@ __device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8]
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
         const float2 Z = ws.fb[p][L.KC], Zm = ws.fb[p][kneg];
-        const float sx = Z.x + Zm.x, dx = Z.x - Zm.x, sy = Z.y + Zm.y, dy = Z.y - Zm.y;
-        float2 ev = make_float2(fmaf(L.sH, sy, sx), fmaf(-L.sH, dx, dy));
-        if (Halve) ev = make_float2(0.5f * ev.x, 0.5f * ev.y);
+        const float2 S = Z + Zm, D = Z - Zm;
+        float2 ev = make_float2(fmaf(L.sH, S.y, S.x), fmaf(-L.sH, D.x, D.y));
+        if (Halve) ev = ev * splat(0.5f);
         // odd half: twiddle W16^p (p = 0: 1; p = 4: -i, exact)
         if (p == 0) e[p] = ev;
         else if (p == 4) e[p] = L.H ? mul_mi(ev) : ev;
         else e[p] = L.H ? cmul(ev, w16(p)) : ev;
     }
     fft8_fwd(e);
+}
+
+// The same from 8 real pixels: x[2j] = row P, x[2j+1] = row P+8, column Qd + 4j.
+template <bool Halve = true>
+__device__ __forceinline__ void warp_fft_fwd(const float (&x)[8], float2 (&e)[8], WarpSmem& ws,
+                                             const LaneGeo& L) {
+    const float2 z[4] = {make_float2(x[0], x[1]), make_float2(x[2], x[3]),
+                         make_float2(x[4], x[5]), make_float2(x[6], x[7])};
+    warp_fft_fwd<Halve>(z, e, ws, L);
 }
 
 // Column stage of the inverse: from a spectrum in the layout warp_fft_fwd
@@ -294,11 +333,9 @@ __device__ __forceinline__ void warp_ifft_cols(float2 (&e)[8], WarpSmem& ws, con
 // Row stage of the inverse: V[k] = one row's spectrum at frequencies k0 + k
 // (this lane's four); z[j] = that row at column Qd + 4j (unnormalised).
 __device__ __forceinline__ void warp_ifft_row(float2 (&V)[4], float2 (&z)[4], const LaneGeo& L) {
+    const float2 sA = splat(L.sA), sB = splat(L.sB);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float2 p = shfl_xor2(V[k], 1);
-        V[k] = make_float2(fmaf(L.sB, V[k].x, p.x), fmaf(L.sB, V[k].y, p.y));
-    }
+    for (int k = 0; k < 4; ++k) V[k] = fma2(sB, V[k], shfl_xor2(V[k], 1));
     // butterfly of lanes Qd and Qd ^ 2: lower = own + i^odd partner, upper =
     // partner - i^odd own.  The upper lane twiddles its own value before the
     // exchange, so each lane adds sA times its (twiddled) value to what it
@@ -307,8 +344,7 @@ __device__ __forceinline__ void warp_ifft_row(float2 (&V)[4], float2 (&z)[4], co
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float2 y = upper_odd ? mul_i(V[k]) : V[k];
-        const float2 p = shfl_xor2(y, 2);
-        V[k] = make_float2(fmaf(L.sA, y.x, p.x), fmaf(L.sA, y.y, p.y));
+        V[k] = fma2(sA, y, shfl_xor2(y, 2));
     }
     V[1] = conjmul(V[1], L.tw1);
     V[2] = conjmul(V[2], L.tw2);
@@ -316,25 +352,32 @@ __device__ __forceinline__ void warp_ifft_row(float2 (&V)[4], float2 (&z)[4], co
     const float2 s02 = V[0] + V[2], d02 = V[0] - V[2], s13 = V[1] + V[3], d13 = V[1] - V[3];
     z[0] = s02 + s13;
     z[2] = s02 - s13;
-    z[1] = d02 + mul_i(d13);
-    z[3] = d02 + mul_mi(d13);
+    z[1] = add_ib(d02, d13);
+    z[3] = sub_ib(d02, d13);
 }
 
 // Inverse half: from a spectrum in the layout warp_fft_fwd leaves, the real
-// tile back in this lane's 8 pixels (unnormalised inverse: x 256).  The two
-// real rows P and P + 8 share one complex row transform.
-__device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float (&y)[8], WarpSmem& ws,
+// tile back in this lane's pixel pairs (unnormalised inverse: x 256): z[j] =
+// rows P and P + 8 at column Qd + 4j.  The two real rows share one complex
+// row transform.
+__device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float2 (&z)[4], WarpSmem& ws,
                                              const LaneGeo& L) {
     warp_ifft_cols(e, ws, L);
-    float2 V[4], z[4];
+    float2 V[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         // rows P = E + O and P + 8 = E - O, packed as one complex row
         const float2 ev = ws.fb[L.P][L.k0 + k], od = ws.fb[L.P + 8][L.k0 + k];
-        const float2 a = ev + od, b = ev - od;
-        V[k] = make_float2(a.x - b.y, a.y + b.x);
+        V[k] = add_ib(ev + od, ev - od);
     }
     warp_ifft_row(V, z, L);
+}
+
+// The same into 8 real pixels: y[2j] = row P, y[2j+1] = row P+8.
+__device__ __forceinline__ void warp_fft_inv(float2 (&e)[8], float (&y)[8], WarpSmem& ws,
+                                             const LaneGeo& L) {
+    float2 z[4];
+    warp_fft_inv(e, z, ws, L);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         y[2 * j] = z[j].x;
@@ -393,6 +436,25 @@ __device__ __forceinline__ float log1p_ls(float x) {
     s = fmaf(y2, s, 1.0f);
     const float small = 2.0f * y * s;
     return fabsf(x) <= 0.5f ? small : log_fast(1.0f + x);
+}
+
+// log1p_ls of a pair: the arithmetic packed, the reciprocals, the log2s and
+// the choice of branch per component.
+__device__ __forceinline__ float2 log1p_ls(float2 x) {
+    const float2 den = x + splat(2.0f);
+    const float2 y = x * make_float2(rcp_fast(den.x), rcp_fast(den.y));
+    const float2 y2 = y * y;
+    float2 s = fma2(y2, splat(1.0f / 9.0f), splat(1.0f / 7.0f));
+    s = fma2(y2, s, splat(1.0f / 5.0f));
+    s = fma2(y2, s, splat(1.0f / 3.0f));
+    s = fma2(y2, s, splat(1.0f));
+    const float2 small = (splat(2.0f) * y) * s;
+    const float2 x1 = x + splat(1.0f);
+    float2 l2;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l2.x) : "f"(x1.x));
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l2.y) : "f"(x1.y));
+    const float2 big = l2 * splat(0.69314718055994531f);  // ln 2
+    return make_float2(fabsf(x.x) <= 0.5f ? small.x : big.x, fabsf(x.y) <= 0.5f ? small.y : big.y);
 }
 
 __device__ __forceinline__ double warp_sum_d(double v) {

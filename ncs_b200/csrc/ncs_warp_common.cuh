@@ -430,11 +430,12 @@ __device__ __forceinline__ float log_fast(float x) {
 __device__ __forceinline__ float log1p_ls(float x) {
     const float y = x * rcp_fast(2.0f + x);
     const float y2 = y * y;
-    float s = fmaf(y2, 1.0f / 9.0f, 1.0f / 7.0f);
-    s = fmaf(y2, s, 1.0f / 5.0f);
-    s = fmaf(y2, s, 1.0f / 3.0f);
-    s = fmaf(y2, s, 1.0f);
-    const float small = 2.0f * y * s;
+    // Horner on the doubled coefficients: exactly 2 s, so y (2 s) = (2 y) s
+    float s = fmaf(y2, 2.0f / 9.0f, 2.0f / 7.0f);
+    s = fmaf(y2, s, 2.0f / 5.0f);
+    s = fmaf(y2, s, 2.0f / 3.0f);
+    s = fmaf(y2, s, 2.0f);
+    const float small = y * s;
     return fabsf(x) <= 0.5f ? small : log_fast(1.0f + x);
 }
 
@@ -444,11 +445,11 @@ __device__ __forceinline__ float2 log1p_ls(float2 x) {
     const float2 den = x + splat(2.0f);
     const float2 y = x * make_float2(rcp_fast(den.x), rcp_fast(den.y));
     const float2 y2 = y * y;
-    float2 s = fma2(y2, splat(1.0f / 9.0f), splat(1.0f / 7.0f));
-    s = fma2(y2, s, splat(1.0f / 5.0f));
-    s = fma2(y2, s, splat(1.0f / 3.0f));
-    s = fma2(y2, s, splat(1.0f));
-    const float2 small = (splat(2.0f) * y) * s;
+    float2 s = fma2(y2, splat(2.0f / 9.0f), splat(2.0f / 7.0f));
+    s = fma2(y2, s, splat(2.0f / 5.0f));
+    s = fma2(y2, s, splat(2.0f / 3.0f));
+    s = fma2(y2, s, splat(2.0f));
+    const float2 small = y * s;
     const float2 x1 = x + splat(1.0f);
     float2 l2;
     asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l2.x) : "f"(x1.x));

@@ -781,8 +781,13 @@ __global__ void __launch_bounds__(kCtaThreads)
                     if (q < 288 && Cc >= 1 && Cc <= 16) {
                         float v[32];
 #pragma unroll
-                        for (int i = 0; i < 32; ++i)
-                            v[i] = fmaf(__uint_as_float(r[i]), sc[i], bias[i]);
+                        for (int i = 0; i < 32; i += 2) {  // FFMA2 on channel pairs
+                            const float2 y = __ffma2_rn(
+                                make_float2(__uint_as_float(r[i]), __uint_as_float(r[i + 1])),
+                                make_float2(sc[i], sc[i + 1]), make_float2(bias[i], bias[i + 1]));
+                            v[i] = y.x;
+                            v[i + 1] = y.y;
+                        }
                         store_pos_relu<F8>(dst, kChunkA, P + 1, v);
                     } else {
                         store_pos_zero<F8>(dst, kChunkA, P + 1);  // border columns: padding
@@ -1212,20 +1217,23 @@ __global__ void __launch_bounds__(w16::kThreadsW)
                     uint32_t qa[4], qb[4];
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
+                        // scale and bias of adjacent channels as packed FP32 pairs
+                        // (FFMA2: one instruction, each half rounded as fmaf)
                         const int i0 = 16 * kk + 4 * j;
                         const float4 sv = sc4[i0 >> 2], o = b4[i0 >> 2];
-                        qa[j] = __byte_perm(
-                            relu_e4m3x2(fmaf(__uint_as_float(ra[i0]), sv.x, o.x),
-                                        fmaf(__uint_as_float(ra[i0 + 1]), sv.y, o.y)),
-                            relu_e4m3x2(fmaf(__uint_as_float(ra[i0 + 2]), sv.z, o.z),
-                                        fmaf(__uint_as_float(ra[i0 + 3]), sv.w, o.w)),
-                            0x5410);
-                        qb[j] = __byte_perm(
-                            relu_e4m3x2(fmaf(__uint_as_float(rb[i0]), sv.x, o.x),
-                                        fmaf(__uint_as_float(rb[i0 + 1]), sv.y, o.y)),
-                            relu_e4m3x2(fmaf(__uint_as_float(rb[i0 + 2]), sv.z, o.z),
-                                        fmaf(__uint_as_float(rb[i0 + 3]), sv.w, o.w)),
-                            0x5410);
+                        const float2 s01 = make_float2(sv.x, sv.y), s23 = make_float2(sv.z, sv.w);
+                        const float2 o01 = make_float2(o.x, o.y), o23 = make_float2(o.z, o.w);
+                        auto pair = [&](const uint32_t (&r)[32], int i) {
+                            return make_float2(__uint_as_float(r[i]), __uint_as_float(r[i + 1]));
+                        };
+                        const float2 a01 = __ffma2_rn(pair(ra, i0), s01, o01);
+                        const float2 a23 = __ffma2_rn(pair(ra, i0 + 2), s23, o23);
+                        const float2 b01 = __ffma2_rn(pair(rb, i0), s01, o01);
+                        const float2 b23 = __ffma2_rn(pair(rb, i0 + 2), s23, o23);
+                        qa[j] = __byte_perm(relu_e4m3x2(a01.x, a01.y), relu_e4m3x2(a23.x, a23.y),
+                                            0x5410);
+                        qb[j] = __byte_perm(relu_e4m3x2(b01.x, b01.y), relu_e4m3x2(b23.x, b23.y),
+                                            0x5410);
                     }
                     wa[kk] = make_uint4(qa[0], qa[1], qa[2], qa[3]);
                     wb[kk] = make_uint4(qb[0], qb[1], qb[2], qb[3]);

@@ -408,36 +408,14 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 }
             }
 
-            float2 gp2 = g[0] * p[0], pv2 = p[0] * v[0], pw2 = p[0] * wn[0];
-#pragma unroll
-            for (int j = 1; j < 4; ++j) {
-                gp2 = fma2(g[j], p[j], gp2);
-                pv2 = fma2(p[j], v[j], pv2);
-                pw2 = fma2(p[j], wn[j], pw2);
-            }
-            double gd = (double)(gp2.x + gp2.y), dpv = (double)(pv2.x + pv2.y),
-                   dpw = (double)(pw2.x + pw2.y);
-            warp_sum3_d(gd, dpv, dpw, lane);
-            dpw = -dpw;  // p'w = -p'wn
-            if (!(gd < 0.0)) {
-                // not a descent direction: drop the history (H0 alone is positive
-                // definite); fail only if even that does not descend
-                if (k == 0) { status = kIncreasingGradient; break; }
-                k = 0;
-                newest = -1;
-                sg_fresh = false;
-                continue;
-            }
-
-            // Armijo backtracking on the exact cost difference, FP64 across lanes
-            float t = 1.0f;
-            bool ok = false;
-            for (int trial = 0; trial < 64; ++trial) {
+            // this lane's part of the cost change at step t: sum tp - c log1p(tp / A)
+            // over its pixels, and whether a pixel crosses the barrier fraction
+            auto trial_part = [&](float t, float& part, bool& cross) {
                 float2 nc[4], gm[4];
                 load_terms_neg(terms, lane, nc, gm);
                 const float2 t2 = splat(t);
                 float2 term = make_float2(0.0f, 0.0f);
-                bool cross = false;
+                cross = false;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     // log(max(ni, F)) - log(max(ai, F)) = log1p((max(ni, F) - A) / A),
@@ -460,8 +438,50 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     }
                     term = term + fma2(nc[j], log1p_ls(num * rA), tp);
                 }
-                const bool any_cross = __any_sync(kFull, cross);
-                const double dl = warp_sum_d((double)(term.x + term.y));
+                part = term.x + term.y;
+            };
+
+            // The slopes g'p, p'v, p'w and the first trial's (t = 1) cost change
+            // in one FP64 reduction: the trial depends on p alone, and it is
+            // accepted in almost every iteration.
+            float2 gp2 = g[0] * p[0], pv2 = p[0] * v[0], pw2 = p[0] * wn[0];
+#pragma unroll
+            for (int j = 1; j < 4; ++j) {
+                gp2 = fma2(g[j], p[j], gp2);
+                pv2 = fma2(p[j], v[j], pv2);
+                pw2 = fma2(p[j], wn[j], pw2);
+            }
+            float part0;
+            bool cross0;
+            trial_part(1.0f, part0, cross0);
+            const bool any_cross0 = __any_sync(kFull, cross0);
+            double gd = (double)(gp2.x + gp2.y), dpv = (double)(pv2.x + pv2.y),
+                   dpw = (double)(pw2.x + pw2.y), dl0 = (double)part0;
+            warp_sum4_d(gd, dpv, dpw, dl0, lane);
+            dpw = -dpw;  // p'w = -p'wn
+            if (!(gd < 0.0)) {
+                // not a descent direction: drop the history (H0 alone is positive
+                // definite); fail only if even that does not descend
+                if (k == 0) { status = kIncreasingGradient; break; }
+                k = 0;
+                newest = -1;
+                sg_fresh = false;
+                continue;
+            }
+
+            // Armijo backtracking on the exact cost difference, FP64 across lanes
+            float t = 1.0f;
+            bool ok = false;
+            for (int trial = 0; trial < 64; ++trial) {
+                double dl = dl0;
+                bool any_cross = any_cross0;
+                if (trial > 0) {
+                    float part;
+                    bool cross;
+                    trial_part(t, part, cross);
+                    any_cross = __any_sync(kFull, cross);
+                    dl = warp_sum_d((double)part);
+                }
                 ++evals;
                 const double td = (double)t;
                 const double delta = any_cross ? CUDART_INF

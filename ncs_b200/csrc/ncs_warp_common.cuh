@@ -464,9 +464,24 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
-// Warp totals of three FP64 values: the first two levels exchange halves of
-// a 4-slot vector (slot 3 empty), so lane L & 3 = j ends with total j after
-// 6 double shuffles; 3 more broadcast them (15 for three plain sums).
+// Warp totals of four FP64 values: the first two levels exchange halves of
+// the 4-slot vector, so lane L & 3 = j ends with total j after 6 double
+// shuffles; 4 more broadcast them (20 for four plain sums).
+__device__ __forceinline__ void warp_sum4_d(double& a, double& b, double& c, double& d, int lane) {
+    const bool up2 = (lane & 2) != 0, up1 = (lane & 1) != 0;
+    double v0 = (up2 ? c : a) + __shfl_xor_sync(kFull, up2 ? a : c, 2);
+    double v1 = (up2 ? d : b) + __shfl_xor_sync(kFull, up2 ? b : d, 2);
+    v0 = (up1 ? v1 : v0) + __shfl_xor_sync(kFull, up1 ? v0 : v1, 1);
+#pragma unroll
+    for (int o = 4; o < 32; o <<= 1) v0 += __shfl_xor_sync(kFull, v0, o);
+    a = __shfl_sync(kFull, v0, 0);
+    b = __shfl_sync(kFull, v0, 1);
+    c = __shfl_sync(kFull, v0, 2);
+    d = __shfl_sync(kFull, v0, 3);
+}
+
+// Warp totals of three FP64 values: warp_sum4_d with slot 3 empty (6 double
+// shuffles and 3 broadcasts; 15 for three plain sums).
 __device__ __forceinline__ void warp_sum3_d(double& a, double& b, double& c, int lane) {
     const bool up2 = (lane & 2) != 0, up1 = (lane & 1) != 0;
     const double s0 = up2 ? a : c, s1 = up2 ? b : 0.0;

@@ -216,7 +216,9 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
         // solver keeps wn = -w = -2 alpha Q p and the history -Q s; the pixel
         // terms are read as -c (load_terms_neg).
         float2 v[4], g[4], p[4], wn[4];
-        float rho[MaxM], al[MaxM];
+        // step of each stored pair: its -Q s is kept as t (-Q s) / t = wn, unscaled
+        // (t is a power of two, so the scaling is exact either way)
+        float rho[MaxM], al[MaxM], tq[MaxM];
         // s'g of the newest pair at the gradient it was stored with: the first
         // two-loop dot of the next iteration, s'(-g), without a reduction
         float sg_newest = 0.0f;
@@ -398,13 +400,14 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     float2 acc = hv[0] * p[0];
 #pragma unroll
                     for (int e = 1; e < 4; ++e) acc = fma2(hv[e], p[e], acc);
-                    const float2 cf = splat(al[i] - rho[i] * warp_sum_f(acc.x + acc.y));
+                    const float coef = al[i] - rho[i] * warp_sum_f(acc.x + acc.y);
+                    const float2 cf = splat(coef), cq = splat(coef * tq[i]);
                     load_hist(hs + slot * 64, lane, hv);
 #pragma unroll
                     for (int e = 0; e < 4; ++e) p[e] = fma2(cf, hv[e], p[e]);
                     load_hist(hq + slot * 64, lane, hv);
 #pragma unroll
-                    for (int e = 0; e < 4; ++e) wn[e] = fma2(cf, hv[e], wn[e]);
+                    for (int e = 0; e < 4; ++e) wn[e] = fma2(cq, hv[e], wn[e]);
                 }
             }
 
@@ -492,7 +495,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             }
             if (!ok) { status = kMinimumStep; break; }
 
-            // accept; new pair (s, y, -Q s = t wn)
+            // accept; new pair (s, y, -Q s = t wn, stored as wn and t)
             float2 s[4], y[4], nc[4], gm[4];
             load_terms_neg(terms, lane, nc, gm);
             const float2 t2 = splat(t), z2 = make_float2(0.0f, 0.0f);
@@ -500,8 +503,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const float2 un = fma2(t2, p[j], u[j]);
-                wn[j] = wn[j] * t2;
-                v[j] = v[j] - wn[j];  // v += t w
+                v[j] = fma2(splat(-t), wn[j], v[j]);  // v += t w
                 const float2 A = un + gm[j];
                 const float2 ia = make_float2(rcp_fast(fmaxf(A.x, kFitMin)), rcp_fast(fmaxf(A.y, kFitMin)));
                 const float2 r = nc[j] * ia;  // -c / (u + gamma)
@@ -543,8 +545,12 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 store_hist(hy + newest * 64, lane, y);
                 store_hist(hq + newest * 64, lane, wn);
 #pragma unroll
-                for (int i = MaxM - 1; i > 0; --i) rho[i] = rho[i - 1];
+                for (int i = MaxM - 1; i > 0; --i) {
+                    rho[i] = rho[i - 1];
+                    tq[i] = tq[i - 1];
+                }
                 rho[0] = rcp_fast(sy);
+                tq[0] = t;
                 if (k < mcap) ++k;
             }
         }

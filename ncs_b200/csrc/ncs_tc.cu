@@ -694,6 +694,31 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
 #pragma unroll
                 for (int e2 = 0; e2 < 8; ++e2) w[e2] = fmaf(coef, hv[e2], w[e2]);
             }
+            // this lane's part of the cost change at step t, and whether a pixel
+            // crosses the barrier fraction
+            auto trial_part = [&](float t, float& part, bool& cross) {
+                float c[8], gm[8];
+                load_terms(terms, lane, c, gm);
+                float term = 0.0f;
+                cross = false;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    // log(max(ni, F)) - log(max(ai, F)) = log1p((max(ni, F) - A) / A),
+                    // A = max(ai, F); above the floor the numerator is the exact
+                    // step tp (branch free: one select instead of a branch)
+                    const float ai = u[i] + gm[i];
+                    const float tp = t * p[i];
+                    const float ni = ai + tp;
+                    const bool in_dom = ai >= kFitMin && ni >= kFitMin;
+                    const float A = fmaxf(ai, kFitMin);
+                    const float l = log1p_ls((in_dom ? tp : fmaxf(ni, kFitMin) - A) * rcp_fast(A));
+                    cross |= (ai >= kFitMin) && (ni < kBarrierFrac * ai);
+                    term += fmaf(-c[i], l, tp);
+                }
+                part = term;
+            };
+            // the slopes and the first trial's (t = 1) cost change in one FP64
+            // reduction: the trial depends on p alone and is almost always accepted
             float gp = 0.0f, pv = 0.0f, pw = 0.0f;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
@@ -701,8 +726,12 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                 pv = fmaf(p[i], v[i], pv);
                 pw = fmaf(p[i], w[i], pw);
             }
-            double gd = (double)gp, dpv = (double)pv, dpw = (double)pw;
-            warp_sum3_d(gd, dpv, dpw, lane);
+            float part0;
+            bool cross0;
+            trial_part(1.0f, part0, cross0);
+            const bool any_cross0 = __any_sync(kFull, cross0);
+            double gd = (double)gp, dpv = (double)pv, dpw = (double)pw, dl0 = (double)part0;
+            warp_sum4_d(gd, dpv, dpw, dl0, lane);
             if (!(gd < 0.0)) {
                 // not a descent direction: drop the history, or fail without one
                 if (k == 0) {
@@ -716,26 +745,15 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                 float t = 1.0f;
                 bool ok = false;
                 for (int trial = 0; trial < 64; ++trial) {
-                    float c[8], gm[8];
-                    load_terms(terms, lane, c, gm);
-                    float term = 0.0f;
-                    bool cross = false;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        // log(max(ni, F)) - log(max(ai, F)) = log1p((max(ni, F) - A) / A),
-                        // A = max(ai, F); above the floor the numerator is the exact
-                        // step tp (branch free: one select instead of a branch)
-                        const float ai = u[i] + gm[i];
-                        const float tp = t * p[i];
-                        const float ni = ai + tp;
-                        const bool in_dom = ai >= kFitMin && ni >= kFitMin;
-                        const float A = fmaxf(ai, kFitMin);
-                        const float l = log1p_ls((in_dom ? tp : fmaxf(ni, kFitMin) - A) * rcp_fast(A));
-                        cross |= (ai >= kFitMin) && (ni < kBarrierFrac * ai);
-                        term += fmaf(-c[i], l, tp);
+                    double dl = dl0;
+                    bool any_cross = any_cross0;
+                    if (trial > 0) {
+                        float part;
+                        bool cross;
+                        trial_part(t, part, cross);
+                        any_cross = __any_sync(kFull, cross);
+                        dl = warp_sum_d((double)part);
                     }
-                    const bool any_cross = __any_sync(kFull, cross);
-                    const double dl = warp_sum_d((double)term);
                     ++evals;
                     const double td = (double)t;
                     const double delta =

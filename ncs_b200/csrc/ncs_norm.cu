@@ -12,8 +12,9 @@
 // of order 1e-5), BFGS with a dense 9 x 9 inverse-Hessian approximation kept
 // in shared memory (45 packed FP32 entries per thread; the direction and the
 // update in FP32 as the main solver's L-BFGS, the update's scalars in FP64),
-// backtracking Armijo line search on the FP64 cost with the fraction-to-
-// barrier rule of the main solver.  The
+// backtracking Armijo line search on the FP64 cost change (in difference
+// form, see the trial loop) with the fraction-to-barrier rule of the main
+// solver.  The
 // reference minimises with MATLAB's fminunc quasi-Newton; the stopping rule
 // here is fminunc's first-order optimality test, ||g||_inf <= tol *
 // max(1, ||g_0||_inf), with its iteration cap.  Q (9 x 9, symmetric) is the
@@ -63,10 +64,11 @@ struct Seg {
     __device__ double G(int i) const { return gm[i][t]; }
 };
 
-// cost and (optionally) gradient; returns +inf outside the domain
-__device__ double evaluate(const Args& a, const double (&u)[9], const Seg& sg, double (&g)[9],
-                           bool want_grad) {
-    double S = 0.0, ll = 0.0, Qu[9];
+// Q u, S = sum u and P = u'Q u at a point (the noise term is alpha P / S).
+__device__ void noise_parts(const Args& a, const double (&u)[9], double (&Qu)[9], double& S,
+                            double& P) {
+    S = 0.0;
+    P = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
         S += u[i];
@@ -76,30 +78,58 @@ __device__ double evaluate(const Args& a, const double (&u)[9], const Seg& sg, d
             acc = fma(a.qk[((i / 3 - j / 3 + 3) % 3) * 3 + (i % 3 - j % 3 + 3) % 3], u[j], acc);
         Qu[i] = acc;
     }
-    double P = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) P = fma(u[i], Qu[i], P);
-    bool ok = S > 0.0;
+}
+
+// 1/x for x > 0 in the normal FP32 range: the hardware FP32 reciprocal (PTX
+// rcp.approx.ftz.f32, relative error about 2^-23) refined by one Newton step
+// in FP64, r (2 - x r), which squares the error (about 2^-46).
+__device__ __forceinline__ double recip(double x) {
+    float r0;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"((float)x));
+    const double r = (double)r0;
+    return r * fma(-x, r, 2.0);
+}
+
+// log1p(x) for |x| <= kSeriesMax: 2 atanh(y), y = x / (2 + x), |y| < 0.18, by
+// the odd series 2y (1 + y^2/3 + ... + y^14/15); the first omitted term,
+// y^16/17, is below 6e-14 relative, and y carries the reciprocal's 2^-46.
+constexpr double kSeriesMax = 0.3;
+__device__ __forceinline__ double log1p_series(double x) {
+    const double y = x * recip(2.0 + x), y2 = y * y;
+    double s = fma(y2, 1.0 / 15.0, 1.0 / 13.0);
+    s = fma(y2, s, 1.0 / 11.0);
+    s = fma(y2, s, 1.0 / 9.0);
+    s = fma(y2, s, 1.0 / 7.0);
+    s = fma(y2, s, 1.0 / 5.0);
+    s = fma(y2, s, 1.0 / 3.0);
+    s = fma(y2, s, 1.0);
+    return 2.0 * y * s;
+}
+
+// the cost at u (FP64 logs; once per pixel, for the reported cost)
+__device__ double full_cost(const Args& a, const double (&u)[9], const Seg& sg) {
+    double Qu[9], S, P, ll = 0.0;
+    noise_parts(a, u, Qu, S, P);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        const double ai = u[i] + sg.G(i);
-        ok = ok && ai > 0.0;
-        ll += u[i] - sg.C(i) * log(ai > 0.0 ? ai : 1.0);
-    }
-    if (!ok) return CUDART_INF;
-    if (want_grad) {
-        const double is = 1.0 / S, is2 = is * is;
-#pragma unroll
-        for (int i = 0; i < 9; ++i)
-            g[i] = (2.0 / 9.0) * (1.0 - sg.C(i) / (u[i] + sg.G(i))) +
-                   a.alpha * (2.0 * Qu[i] * S - P) * is2;
-    }
+    for (int i = 0; i < 9; ++i) ll += u[i] - sg.C(i) * log(u[i] + sg.G(i));
     return (2.0 / 9.0) * ll + a.alpha * P / S;
+}
+
+// gradient at u from its noise parts and r_i = 1 / (u_i + gamma_i)
+__device__ void gradient(const Args& a, const double (&Qu)[9], double S, double P,
+                         const double (&r)[9], const Seg& sg, double (&g)[9]) {
+    const double is = 1.0 / S, is2 = is * is;
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        g[i] = (2.0 / 9.0) * (1.0 - sg.C(i) * r[i]) + a.alpha * (2.0 * Qu[i] * S - P) * is2;
 }
 
 __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
     __shared__ float Hm[kPacked][kThreads];  // inverse-Hessian approximation, per thread
     __shared__ double Cs[9][kThreads], Gs[9][kThreads];
+    __shared__ double Rs[9][kThreads];  // 1 / (u + gamma) at the current iterate
     const long long HW = (long long)a.H * a.W;
     const long long idx = (long long)blockIdx.x * kThreads + threadIdx.x;
     if (idx >= (long long)a.T * HW) return;
@@ -129,12 +159,26 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
 #pragma unroll
         for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0f : 0.0f;
 
-    double fu = evaluate(a, u, sg, g, true);
+    double Qu[9], S, P;
+    noise_parts(a, u, Qu, S, P);
+    bool feasible = S > 0.0;
+    {
+        double r[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const double A = u[i] + sg.G(i);
+            feasible = feasible && A > 0.0;
+            r[i] = recip(A > 0.0 ? A : 1.0);
+            Rs[i][t] = r[i];
+        }
+        gradient(a, Qu, S, P, r, sg, g);
+    }
+    double fq = feasible ? P / S : 0.0;  // P / S at the current iterate
     double g0 = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) g0 = fmax(g0, fabs(g[i]));
     int status = NCSB_REACHED_MAXITERS, it = 0;
-    if (!(fu < CUDART_INF)) status = NCSB_INCREASING_GRADIENT;  // infeasible start
+    if (!feasible) status = NCSB_INCREASING_GRADIENT;  // infeasible start
     for (; it < a.max_iters && status == NCSB_REACHED_MAXITERS; ++it) {
         double gmax = 0.0;
 #pragma unroll
@@ -169,8 +213,13 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
                 gd = fma(g[i], (double)d[i], gd);
             }
         }
-        // backtracking Armijo; trials keep u + gamma >= 1% of its value
-        double step = 1.0, un[9], gn[9], fn = CUDART_INF;
+        // backtracking Armijo on the cost change in difference form:
+        //   f(un) - f(u) = (2/9) sum_i [s_i - c_i log1p(s_i / (u_i + gamma_i))]
+        //                  + alpha (P(un) / S(un) - P(u) / S(u)),  s = un - u,
+        // whose log terms are of the order of the step rather than of the costs
+        // (about 100), so a series log1p at 1e-13 replaces the FP64 logs of two
+        // full costs; trials keep u + gamma >= 1% of its value
+        double step = 1.0, un[9], gn[9], Qn[9], Sn = 0.0, Pn = 0.0, fqn = 0.0;
         bool ok = false;
         for (int trial = 0; trial < 64; ++trial) {
             bool feas = true;
@@ -180,15 +229,37 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
                 feas = feas && (un[i] + sg.G(i) >= 0.01 * (u[i] + sg.G(i)));
             }
             if (feas) {
-                // with the gradient: nearly every first trial is accepted, and
-                // evaluating again after acceptance would repeat the logs and Q u
-                fn = evaluate(a, un, sg, gn, true);
-                if (fn <= fu + a.c1 * step * gd) { ok = true; break; }
+                noise_parts(a, un, Qn, Sn, Pn);
+                if (Sn > 0.0) {
+                    double dll = 0.0;
+                    bool big = false;
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) {
+                        const double si = un[i] - u[i], x = si * Rs[i][t];
+                        big = big || !(fabs(x) <= kSeriesMax);
+                        dll += fma(-sg.C(i), log1p_series(x), si);
+                    }
+                    if (big) {  // a relative step beyond the series' range
+                        dll = 0.0;
+#pragma unroll
+                        for (int i = 0; i < 9; ++i) {
+                            const double si = un[i] - u[i];
+                            dll += fma(-sg.C(i), log1p(si * Rs[i][t]), si);
+                        }
+                    }
+                    fqn = Pn / Sn;
+                    const double df = (2.0 / 9.0) * dll + a.alpha * (fqn - fq);
+                    if (df <= a.c1 * step * gd) { ok = true; break; }
+                }
             }
             step *= 0.5;
             if (!(step >= a.min_step)) break;
         }
         if (!ok) { status = NCSB_MINIMUM_STEP; break; }
+        double rn[9];  // un + gamma >= 1% of u + gamma > 0
+#pragma unroll
+        for (int i = 0; i < 9; ++i) rn[i] = recip(un[i] + sg.G(i));
+        gradient(a, Qn, Sn, Pn, rn, sg, gn);
         // BFGS update of the inverse Hessian with s = un - u, y = gn - g:
         // H <- H - rho (v s' + s v') + (rho^2 y'Hy + rho) s s', v = H y.  The
         // differences and the scalars in FP64, the 45 entries in FP32 from
@@ -242,15 +313,16 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
             moved = moved || (un[i] != u[i]);
             u[i] = un[i];
             g[i] = gn[i];
+            Rs[i][t] = rn[i];
         }
-        fu = fn;
+        fq = fqn;
         if (!moved) { status = NCSB_REACHED_MAXPRECISION; ++it; break; }
     }
     const float centre = (float)u[4];
     a.out[idx] = centre < 0.0f ? 1.0e-6f : centre;
     if (a.iters) a.iters[idx] = it;
     if (a.status) a.status[idx] = status;
-    if (a.cost) a.cost[idx] = fu;
+    if (a.cost) a.cost[idx] = feasible ? full_cost(a, u, sg) : CUDART_INF;
 }
 
 }  // namespace norm

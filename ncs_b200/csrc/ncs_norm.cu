@@ -82,13 +82,14 @@ __device__ void noise_parts(const Args& a, const double (&u)[9], double (&Qu)[9]
     for (int i = 0; i < 9; ++i) P = fma(u[i], Qu[i], P);
 }
 
-// 1/x for x > 0 in the normal FP32 range: the hardware FP32 reciprocal (PTX
-// rcp.approx.ftz.f32, relative error about 2^-23) refined by one Newton step
-// in FP64, r (2 - x r), which squares the error (about 2^-46).
+// 1/x for x > 0: the hardware's gross FP64 reciprocal (PTX rcp.approx.ftz.f64,
+// from the operand's upper 32 bits) refined by two Newton steps r (2 - x r),
+// each of which squares the relative error, to FP64 rounding.  No FP32
+// round trip: conversions share the pipe with the reciprocal itself.
 __device__ __forceinline__ double recip(double x) {
-    float r0;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"((float)x));
-    const double r = (double)r0;
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    r = r * fma(-x, r, 2.0);
     return r * fma(-x, r, 2.0);
 }
 
@@ -184,11 +185,13 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
 #pragma unroll
         for (int i = 0; i < 9; ++i) gmax = fmax(gmax, fabs(g[i]));
         if (gmax <= a.tol * fmax(1.0, g0)) { status = NCSB_SUCCESS; break; }
-        // direction p = -H g (FP32), its slope g'p in FP64
+        // direction p = -H g and its slope g'p = -g'H g, both FP32 (a quadratic
+        // form: no cancellation; the Armijo threshold needs it to 1e-4 at most)
         float d[9];
-        double gd = 0.0;
+        double gd;
+        float gf[9];
         {
-            float gf[9];
+            float gdf = 0.0f;
 #pragma unroll
             for (int j = 0; j < 9; ++j) gf[j] = (float)g[j];
 #pragma unroll
@@ -198,20 +201,22 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
                 for (int j = 0; j < 9; ++j)
                     acc = fmaf(Hm[i <= j ? pk(i, j) : pk(j, i)][t], gf[j], acc);
                 d[i] = -acc;
-                gd = fma(g[i], (double)d[i], gd);
+                gdf = fmaf(gf[i], d[i], gdf);
             }
+            gd = (double)gdf;
         }
         if (!(gd < 0.0)) {  // lost positive definiteness: restart from steepest descent
 #pragma unroll
             for (int i = 0; i < 9; ++i)
 #pragma unroll
                 for (int j = i; j < 9; ++j) Hm[pk(i, j)][t] = i == j ? 1.0f : 0.0f;
-            gd = 0.0;
+            float gdf = 0.0f;
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
-                d[i] = -(float)g[i];
-                gd = fma(g[i], (double)d[i], gd);
+                d[i] = -gf[i];
+                gdf = fmaf(gf[i], d[i], gdf);
             }
+            gd = (double)gdf;
         }
         // backtracking Armijo on the cost change in difference form:
         //   f(un) - f(u) = (2/9) sum_i [s_i - c_i log1p(s_i / (u_i + gamma_i))]
@@ -274,14 +279,13 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
             sy = fma(sd, yd, sy);
             yy = fma(yd, yd, yy);
         }
-        if (sy > 1e-300) {
+        if (sy > 1e-30) {  // rho = 1 / sy within FP32 range
             if (it == 0) {  // scale the identity before the first update
                 const float sc = (float)(sy / yy);
 #pragma unroll
                 for (int i = 0; i < 9; ++i) Hm[pk(i, i)][t] = sc;
             }
-            float v[9];
-            double yHy = 0.0;
+            float v[9], yHyf = 0.0f;
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
                 float acc = 0.0f;
@@ -289,13 +293,14 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
                 for (int j = 0; j < 9; ++j)
                     acc = fmaf(Hm[i <= j ? pk(i, j) : pk(j, i)][t], yv[j], acc);
                 v[i] = acc;
-                yHy = fma((double)yv[i], (double)acc, yHy);
+                yHyf = fmaf(yv[i], acc, yHyf);
             }
-            const double rho = 1.0 / sy, k2 = rho * rho * yHy + rho;
-            float rv[9], ks[9];  // rho v and (rho^2 y'Hy + rho) s
+            const double rho = 1.0 / sy, k2 = rho * rho * (double)yHyf + rho;
+            const float rhof = (float)rho;
+            float rv[9], ks[9];  // rho v and (rho^2 y'Hy + rho) s (k2 may pass FP32's range)
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
-                rv[i] = (float)(rho * (double)v[i]);
+                rv[i] = rhof * v[i];
                 ks[i] = (float)(k2 * (double)s[i]);
             }
 #pragma unroll

@@ -81,8 +81,8 @@ typedef struct {
                           libLBFGS m = 6; default 1: NCS tiles need the same number of
                           iterations for every m measured, 1..8 in the plain form and
                           1..4 in the spectral one, and fewer pairs cost less -- the
-                          spectral solve of the 512 x 512 x 200 stack takes 4.01 ms at
-                          m = 1 and 4.24 ms at m = 2) */
+                          spectral solve measured about 6 % slower at m = 2 than at
+                          m = 1) */
     double epsilon;    /* stop when ||g|| <= epsilon * max(1, ||u||)
                           (ncs.cu EPSILON = 1e-4; libLBFGS epsilon = 1e-5) */
     double c1;         /* Armijo constant (ncs.cu C_1 = 1e-4) */

@@ -43,9 +43,20 @@ using namespace warp;
 namespace {
 
 // Per-warp shared memory: the common block, the s, y and Q s history, then
-// the tile's pixel terms c = d + gamma and gamma.
-__host__ __device__ constexpr size_t spec_warp_bytes(int m) {
-    return ((sizeof(WarpSmem) + 15) / 16) * 16 + (3 * (size_t)m + 2) * 32 * 2 * sizeof(float4);
+// the tile's pixel terms c = d + gamma and gamma, then (vg) the vectors v and g.
+__host__ __device__ constexpr size_t spec_warp_bytes(int m, bool vg) {
+    return ((sizeof(WarpSmem) + 15) / 16) * 16 +
+           (3 * (size_t)m + (vg ? 4 : 2)) * 32 * 2 * sizeof(float4);
+}
+
+// The 5-CTA launch of the plain single-stack solve keeps v = 2 alpha Q u and
+// g in the warp's shared memory instead of registers: at the 96 registers that
+// 5 CTAs (20 warps) per SM allow, the solve then runs without spills and
+// 0.7 % faster than 4 CTAs with them in registers; at 4 CTAs the extra loads
+// measured 0.6 % slower.
+template <int MinBlocks, bool Warm, bool Batch>
+__host__ __device__ constexpr bool vg_shared() {
+    return MinBlocks >= 5 && !Warm && !Batch;
 }
 
 // Per-stack pointers and geometry: the kernel parameters of a single-stack
@@ -81,13 +92,16 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
     // stopping rule ||g|| <= eps max(||u||, 1), compared squared
     const float eps2 = a.eps * a.eps;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    constexpr bool kVg = vg_shared<MinBlocks, Warm, Batch>();
     float* mtab = reinterpret_cast<float*>(dsm);
-    unsigned char* wbase = dsm + kTableBytes + (size_t)wid * spec_warp_bytes(mcap);
+    unsigned char* wbase = dsm + kTableBytes + (size_t)wid * spec_warp_bytes(mcap, kVg);
     WarpSmem& ws = *reinterpret_cast<WarpSmem*>(wbase);
     float4* hs = reinterpret_cast<float4*>(wbase + ((sizeof(WarpSmem) + 15) / 16) * 16);
     float4* hy = hs + (size_t)mcap * 64;
     float4* hq = hy + (size_t)mcap * 64;
     float4* terms = hq + (size_t)mcap * 64;  // c and gamma, see load_terms
+    float4* vbuf = terms + 128;  // kVg: v and g as pixel pairs
+    float4* gbuf = terms + 192;
 
     __shared__ StackDesc sdesc[kWarps];  // Batch: each warp's current stack
     __shared__ TwiddleTable s_tw;
@@ -242,6 +256,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 }
             } else {
                 // two-loop, first half (newest pair first), on nq = -q
+                if constexpr (kVg) load_hist_volatile(gbuf, lane, g);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) nq[j] = g[j];
 #pragma unroll
@@ -383,6 +398,10 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                     gg2 = fma2(g[j], g[j], gg2);
                     ll2 = fma2(r, ia, ll2);
                 }
+                if constexpr (kVg) {
+                    store_hist(vbuf, lane, v);
+                    store_hist(gbuf, lane, g);
+                }
                 const float uu = warp_sum_f(uu2.x + uu2.y);
                 const float gg = warp_sum_f(gg2.x + gg2.y);
                 lam = warp_sum_f(ll2.x + ll2.y) * (-1.0f / 256.0f);
@@ -447,6 +466,10 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             // The slopes g'p, p'v, p'w and the first trial's (t = 1) cost change
             // in one FP64 reduction: the trial depends on p alone, and it is
             // accepted in almost every iteration.
+            if constexpr (kVg) {
+                load_hist_volatile(vbuf, lane, v);
+                load_hist_volatile(gbuf, lane, g);
+            }
             float2 gp2 = g[0] * p[0], pv2 = p[0] * v[0], pw2 = p[0] * wn[0];
 #pragma unroll
             for (int j = 1; j < 4; ++j) {
@@ -498,6 +521,10 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             // accept; new pair (s, y, -Q s = t wn, stored as wn and t)
             float2 s[4], y[4], nc[4], gm[4];
             load_terms_neg(terms, lane, nc, gm);
+            if constexpr (kVg) {
+                load_hist_volatile(vbuf, lane, v);
+                load_hist_volatile(gbuf, lane, g);
+            }
             const float2 t2 = splat(t), z2 = make_float2(0.0f, 0.0f);
             float2 sy2 = z2, uu2 = z2, gg2 = z2, ll2 = z2, mv2 = z2, sg2 = z2;
 #pragma unroll
@@ -520,6 +547,10 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
                 uu2 = fma2(un, un, uu2);
                 gg2 = fma2(gn, gn, gg2);
                 ll2 = fma2(r, ia, ll2);
+            }
+            if constexpr (kVg) {
+                store_hist(vbuf, lane, v);
+                store_hist(gbuf, lane, g);
             }
             float sy, uu, gg, ll, mv, sg;
             {
@@ -560,6 +591,7 @@ __global__ void __launch_bounds__(kWarpCtaThreads, MinBlocks) ncs_spectral_kerne
             float2 nc[4], gm[4];
             load_terms_neg(terms, lane, nc, gm);
             double e0 = 0.0, e1 = 0.0;
+            if constexpr (kVg) load_hist_volatile(vbuf, lane, v);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
 #pragma unroll
@@ -607,9 +639,15 @@ namespace {
 
 using KernelFn = void (*)(SolveArgs);
 
-size_t spectral_smem_bytes(int m) {
+size_t spectral_smem_bytes(int m, bool vg) {
     const int mc = m < 1 ? 1 : (m > 4 ? 4 : m);
-    return kTableBytes + (size_t)kWarps * spec_warp_bytes(mc);
+    return kTableBytes + (size_t)kWarps * spec_warp_bytes(mc, vg);
+}
+
+// whether the instance spectral_variant picks for this launch keeps v and g
+// in shared memory (vg_shared above)
+bool variant_vg(int blocks, bool warm, bool batch) {
+    return blocks >= 5 && !warm && !batch;
 }
 
 template <int B, int MaxM>
@@ -638,24 +676,30 @@ KernelFn spectral_variant(int blocks, int m, bool warm, bool batch) {
                             : spectral_variant_m<4>(blocks, warm, batch));
 }
 
-int spectral_default_blocks(int m) {
+int spectral_default_blocks(int m, bool warm, bool batch) {
     int dev = 0, per_sm = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
         cudaSuccess)
         per_sm = 228 * 1024;
-    // 4 CTAs (16 warps, 128 registers, at most a few words spilled) measured
-    // fastest; the 5-CTA budget (96 registers) spills heavily
-    const int b = (int)(per_sm / (spectral_smem_bytes(m) + 1024));
+    // Plain single-stack solves at m = 1: 5 CTAs (20 warps, 96 registers, v and
+    // g in shared memory) measured fastest.  Otherwise 4 CTAs (16 warps, 128
+    // registers): with more history, proposals or a batch the 5-CTA budget
+    // spills.
+    if (m <= 1 && !warm && !batch &&
+        (int)(per_sm / (spectral_smem_bytes(m, true) + 1024)) >= 5)
+        return 5;
+    const int b = (int)(per_sm / (spectral_smem_bytes(m, false) + 1024));
     return b < 4 ? b : 4;
 }
 
 }  // namespace
 
 cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStream_t stream) {
-    const size_t smem = spectral_smem_bytes(args.m);
-    const KernelFn fn = spectral_variant(blocks > 0 ? blocks : spectral_default_blocks(args.m), args.m,
-                                         args.u0 != nullptr, args.stacks != nullptr);
+    const bool warm = args.u0 != nullptr, batch = args.stacks != nullptr;
+    const int b = blocks > 0 ? blocks : spectral_default_blocks(args.m, warm, batch);
+    const size_t smem = spectral_smem_bytes(args.m, variant_vg(b, warm, batch));
+    const KernelFn fn = spectral_variant(b, args.m, warm, batch);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     fn<<<grid, kWarpCtaThreads, smem, stream>>>(args);
@@ -663,9 +707,9 @@ cudaError_t launch_spectral(const SolveArgs& args, int grid, int blocks, cudaStr
 }
 
 int spectral_max_ctas_per_sm(int m, int blocks, bool warm, bool batch) {
-    const size_t smem = spectral_smem_bytes(m);
-    const KernelFn fn =
-        spectral_variant(blocks > 0 ? blocks : spectral_default_blocks(m), m, warm, batch);
+    const int b = blocks > 0 ? blocks : spectral_default_blocks(m, warm, batch);
+    const size_t smem = spectral_smem_bytes(m, variant_vg(b, warm, batch));
+    const KernelFn fn = spectral_variant(b, m, warm, batch);
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return 1;

@@ -181,6 +181,15 @@ __device__ __forceinline__ void store_hist(float4* h, int lane, const float2 (&z
     h[32 + lane] = make_float4(z[2].x, z[2].y, z[3].x, z[3].y);
 }
 
+// The same, re-read at each use (not hoisted into registers across a loop).
+__device__ __forceinline__ void load_hist_volatile(const float4* h, int lane, float2 (&z)[4]) {
+    const float4 a = lds_v4_volatile(h + lane), b = lds_v4_volatile(h + 32 + lane);
+    z[0] = make_float2(a.x, a.y);
+    z[1] = make_float2(a.z, a.w);
+    z[2] = make_float2(b.x, b.y);
+    z[3] = make_float2(b.z, b.w);
+}
+
 // The pixel terms c = d + gamma and gamma of a lane's 8 pixels, kept in the
 // warp's shared memory as [c low, c high, gamma low, gamma high][lane]
 // float4s (each access is 32 consecutive 16-byte words) and re-read at

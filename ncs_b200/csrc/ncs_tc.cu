@@ -696,24 +696,35 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
             }
             // this lane's part of the cost change at step t, and whether a pixel
             // crosses the barrier fraction
+            // (pixels 2j and 2j + 1, rows P and P + 8, as packed FP32 pairs)
             auto trial_part = [&](float t, float& part, bool& cross) {
                 float c[8], gm[8];
                 load_terms(terms, lane, c, gm);
+                const float2 t2 = splat(t);
                 float term = 0.0f;
                 cross = false;
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
+                for (int j = 0; j < 4; ++j) {
                     // log(max(ni, F)) - log(max(ai, F)) = log1p((max(ni, F) - A) / A),
                     // A = max(ai, F); above the floor the numerator is the exact
                     // step tp (branch free: one select instead of a branch)
-                    const float ai = u[i] + gm[i];
-                    const float tp = t * p[i];
-                    const float ni = ai + tp;
-                    const bool in_dom = ai >= kFitMin && ni >= kFitMin;
-                    const float A = fmaxf(ai, kFitMin);
-                    const float l = log1p_ls((in_dom ? tp : fmaxf(ni, kFitMin) - A) * rcp_fast(A));
-                    cross |= (ai >= kFitMin) && (ni < kBarrierFrac * ai);
-                    term += fmaf(-c[i], l, tp);
+                    const float2 ai = pair(u, j) + pair(gm, j);
+                    const float2 tp = t2 * pair(p, j);
+                    const float2 ni = ai + tp;
+                    const float2 bar = splat(kBarrierFrac) * ai;
+                    float2 num, rA;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const float a1 = h ? ai.y : ai.x, n1 = h ? ni.y : ni.x;
+                        const bool in_dom = a1 >= kFitMin && n1 >= kFitMin;
+                        const float A = fmaxf(a1, kFitMin);
+                        (h ? num.y : num.x) = in_dom ? (h ? tp.y : tp.x) : fmaxf(n1, kFitMin) - A;
+                        (h ? rA.y : rA.x) = rcp_fast(A);
+                        cross |= (a1 >= kFitMin) && (n1 < (h ? bar.y : bar.x));
+                    }
+                    const float2 l = log1p_ls(num * rA);
+                    term += fmaf(-c[2 * j], l.x, tp.x);
+                    term += fmaf(-c[2 * j + 1], l.y, tp.y);
                 }
                 part = term;
             };
@@ -772,28 +783,37 @@ __global__ void __launch_bounds__(kTcThreads, kMinBlocks) ncs_tc_kernel(const So
                     // accept; new pair (s, y, Q s = t w)
                     float s[8], y[8], c[8], gm[8];
                     load_terms(terms, lane, c, gm);
-                    float sy = 0.0f, uu = 0.0f, gg = 0.0f, ll = 0.0f, mv = 0.0f, sgv = 0.0f;
+                    const float2 t2 = splat(t), z2 = make_float2(0.0f, 0.0f);
+                    float2 sy2 = z2, uu2 = z2, gg2 = z2, ll2 = z2, mv2 = z2, sg2 = z2;
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const float un = fmaf(t, p[i], u[i]);
-                        w[i] *= t;
-                        v[i] += w[i];
-                        const float ia = rcp_fast(fmaxf(un + gm[i], kFitMin));
-                        const float r = c[i] * ia;
-                        const float gn = 1.0f - r + v[i];
-                        s[i] = un - u[i];
-                        y[i] = gn - g[i];
+                    for (int j = 0; j < 4; ++j) {  // pixel pairs, packed FP32
+                        const float2 uj = pair(u, j);
+                        const float2 un = fma2(t2, pair(p, j), uj);
+                        const float2 wj = pair(w, j) * t2;
+                        const float2 vj = pair(v, j) + wj;
+                        const float2 A = un + pair(gm, j);
+                        const float2 ia = make_float2(rcp_fast(fmaxf(A.x, kFitMin)),
+                                                      rcp_fast(fmaxf(A.y, kFitMin)));
+                        const float2 r = pair(c, j) * ia;
+                        const float2 gn = (splat(1.0f) - r) + vj;
+                        const float2 sj = un - uj, yj = gn - pair(g, j);
                         // mv = s's squared norm: zero when no pixel moved (steps below about
                         // 1e-22, whose squares underflow, count as none)
-                        mv = fmaf(s[i], s[i], mv);
-                        u[i] = un;
-                        g[i] = gn;
-                        sy = fmaf(s[i], y[i], sy);
-                        sgv = fmaf(s[i], gn, sgv);
-                        uu = fmaf(un, un, uu);
-                        gg = fmaf(gn, gn, gg);
-                        ll = fmaf(r, ia, ll);
+                        mv2 = fma2(sj, sj, mv2);
+                        sy2 = fma2(sj, yj, sy2);
+                        sg2 = fma2(sj, gn, sg2);
+                        uu2 = fma2(un, un, uu2);
+                        gg2 = fma2(gn, gn, gg2);
+                        ll2 = fma2(r, ia, ll2);
+                        set_pair(w, j, wj);
+                        set_pair(v, j, vj);
+                        set_pair(s, j, sj);
+                        set_pair(y, j, yj);
+                        set_pair(u, j, un);
+                        set_pair(g, j, gn);
                     }
+                    float sy = sy2.x + sy2.y, uu = uu2.x + uu2.y, gg = gg2.x + gg2.y;
+                    float ll = ll2.x + ll2.y, mv = mv2.x + mv2.y, sgv = sg2.x + sg2.y;
                     {
                         float vals[8] = {sy, uu, gg, ll, mv, sgv};
                         const float tot = warp_transpose_sum<8>(vals, lane);

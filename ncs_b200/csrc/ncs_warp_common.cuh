@@ -47,6 +47,14 @@ __device__ __forceinline__ float2 operator-(float2 a, float2 b) {
 }
 __device__ __forceinline__ float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// pixels 2j and 2j + 1 of a lane's 8 (rows P and P + 8 at column Qd + 4j) as a pair
+__device__ __forceinline__ float2 pair(const float (&x)[8], int j) {
+    return make_float2(x[2 * j], x[2 * j + 1]);
+}
+__device__ __forceinline__ void set_pair(float (&x)[8], int j, float2 z) {
+    x[2 * j] = z.x;
+    x[2 * j + 1] = z.y;
+}
 __device__ __forceinline__ float2 mul_i(float2 a) { return make_float2(-a.y, a.x); }      // i a
 __device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }     // -i a
 __device__ __forceinline__ float2 add_ib(float2 a, float2 b) { return make_float2(a.x - b.y, a.y + b.x); }  // a + i b

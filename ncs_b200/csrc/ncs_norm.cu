@@ -121,7 +121,7 @@ __device__ double full_cost(const Args& a, const double (&u)[9], const Seg& sg) 
 // gradient at u from its noise parts and r_i = 1 / (u_i + gamma_i)
 __device__ void gradient(const Args& a, const double (&Qu)[9], double S, double P,
                          const double (&r)[9], const Seg& sg, double (&g)[9]) {
-    const double is = 1.0 / S, is2 = is * is;
+    const double is = recip(S), is2 = is * is;
 #pragma unroll
     for (int i = 0; i < 9; ++i)
         g[i] = (2.0 / 9.0) * (1.0 - sg.C(i) * r[i]) + a.alpha * (2.0 * Qu[i] * S - P) * is2;
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
         }
         gradient(a, Qu, S, P, r, sg, g);
     }
-    double fq = feasible ? P / S : 0.0;  // P / S at the current iterate
+    double fq = feasible ? P * recip(S) : 0.0;  // P / S at the current iterate
     double g0 = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) g0 = fmax(g0, fabs(g[i]));
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
                             dll += fma(-sg.C(i), log1p(si * Rs[i][t]), si);
                         }
                     }
-                    fqn = Pn / Sn;
+                    fqn = Pn * recip(Sn);  // the same rounding as fq's
                     const double df = (2.0 / 9.0) * dll + a.alpha * (fqn - fq);
                     if (df <= a.c1 * step * gd) { ok = true; break; }
                 }
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
                 v[i] = acc;
                 yHyf = fmaf(yv[i], acc, yHyf);
             }
-            const double rho = 1.0 / sy, k2 = rho * rho * (double)yHyf + rho;
+            const double rho = recip(sy), k2 = rho * rho * (double)yHyf + rho;
             const float rhof = (float)rho;
             float rv[9], ks[9];  // rho v and (rho^2 y'Hy + rho) s (k2 may pass FP32's range)
 #pragma unroll

@@ -175,6 +175,23 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
         gradient(a, Qu, S, P, r, sg, g);
     }
     double fq = feasible ? P * recip(S) : 0.0;  // P / S at the current iterate
+    // A trial whose cost change is below the cost's FP64 resolution is accepted,
+    // as when two full costs compare equal: near the optimum the gradient still
+    // steers the steps (its test can need changes far below that resolution),
+    // and a step that moves no pixel ends the solve.  The resolution is taken
+    // as 2^-52 of a bound on |f|, (2/9) sum (|u| + c |log(u + gamma)|) +
+    // alpha |P / S|, from the start (FP32 hardware log2: only its scale matters)
+    double res_f = 0.0;
+    if (feasible) {
+        float bound = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            float l2;
+            asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l2) : "f"((float)(u[i] + sg.G(i))));
+            bound += fabsf((float)u[i]) + (float)sg.C(i) * fabsf(l2 * 0.69314718f);
+        }
+        res_f = 0x1p-52 * ((2.0 / 9.0) * (double)bound + a.alpha * fabs(fq));
+    }
     double g0 = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) g0 = fmax(g0, fabs(g[i]));
@@ -224,7 +241,7 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
         // whose log terms are of the order of the step rather than of the costs
         // (about 100), so a series log1p at 1e-13 replaces the FP64 logs of two
         // full costs; trials keep u + gamma >= 1% of its value
-        double step = 1.0, un[9], gn[9], Qn[9], Sn = 0.0, Pn = 0.0, fqn = 0.0;
+        double step = 1.0, un[9], gn[9], Qn[9], Sn = 0.0, Pn = 0.0, fqn = 0.0, df = 0.0;
         bool ok = false;
         for (int trial = 0; trial < 64; ++trial) {
             bool feas = true;
@@ -253,8 +270,11 @@ __global__ void __launch_bounds__(kThreads) normalized_kernel(const Args a) {
                         }
                     }
                     fqn = Pn * recip(Sn);  // the same rounding as fq's
-                    const double df = (2.0 / 9.0) * dll + a.alpha * (fqn - fq);
-                    if (df <= a.c1 * step * gd) { ok = true; break; }
+                    df = (2.0 / 9.0) * dll + a.alpha * (fqn - fq);
+                    if (df <= a.c1 * step * gd || fabs(df) <= res_f) {
+                        ok = true;
+                        break;
+                    }
                 }
             }
             step *= 0.5;

@@ -51,6 +51,30 @@ def test_converged_pixels_match_the_fp64_optimum(ncs, per_frame):
         assert numpy.abs(out[f] - ref).max() <= 1e-4 * max(1.0, numpy.abs(ref).max())
 
 
+def test_large_relative_steps_match_the_fp64_optimum(ncs):
+    # dead pixels (1e-6) beside bright ones, and hot pixels, with a small gamma:
+    # the first steps move u + gamma by far more than the 30 % the line search's
+    # series log1p covers, so the library log1p branch runs as well
+    from ncs_b200 import otf
+    from oracle import normalized_ref as nr
+    H, W = 8, 10
+    rng = numpy.random.default_rng(11)
+    im = rng.poisson(80.0, size=(1, H, W)).astype(numpy.float64)
+    im[0, ::3, ::2] = 1e-6
+    im[0, 1::4, 1::3] *= 6.0
+    im = im.astype(numpy.float32)
+    gam = numpy.full((H, W), 0.3, numpy.float32)
+    mask = otf.normalized_mask(0.1, 1.4, 0.7).astype(numpy.float32)
+    out, it, st, cost = ncs.reduce_noise_normalized(
+        torch.from_numpy(im).cuda(), torch.from_numpy(gam).cuda(), mask, alpha=1.0,
+        max_iters=500, tol=1e-9, stats=True)
+    st, cost = st.cpu().numpy(), cost.cpu().numpy()
+    assert numpy.isin(st, (0, -5)).all(), numpy.unique(st, return_counts=True)
+    _, fstar = nr.reduce_noise(im[0], gam, mask.astype(numpy.float64), 1.0)
+    gap = (cost[0].ravel() - fstar) / numpy.maximum(numpy.abs(fstar), 1.0)
+    assert gap.max() <= 1e-9 and gap.min() >= -1e-9
+
+
 def test_iteration_cap_of_the_reference_demos(ncs):
     from ncs_b200 import otf
     im, gam = data(1, 16, 16, 5)
